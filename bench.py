@@ -1,0 +1,343 @@
+"""Benchmark of the Kino-PAX tree-expansion iteration on one B200 (or N independent replicas).
+
+Metric: valid expansions/s (children that passed every RK4-step validity and collision check),
+the reference's own counter (sum of d_validCounterArray_, src/planners/KPAX.cu:393).
+
+  value  one planner iteration per step (frontier scan, fused expansion, region scores) on the
+         12D-quadrotor configuration (building scene, 1000 AABBs, 2^16 expansions/iteration,
+         25 RK4 steps of 0.02 s), inputs resident on the device, L2 flushed before every timed
+         iteration, kernels timed with CUDA events on the planner stream;
+  e2e    whole plans through the C ABI (kpax_plan_host) from host buffers: obstacles, start and
+         goal copied in and the path read back inside the timed region (host wall clock);
+  roofline  the expansion kernel: executed RK4 steps x FP32 FLOP per step / kernel time;
+  cpu_baseline  the reference's own propagation + collision + region routines compiled for the
+         host (oracle/_ref, OpenMP over all cores) on a bounded sample of the same children.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path[:0] = [str(ROOT / "kino-pax-fork_b200")]
+
+import kpax  # noqa: E402
+import kpax_envs as E  # noqa: E402
+
+METRIC = "valid expansions/s"
+UNIT = "expansions/s"
+# Algorithmic FP32 work per RK4 step (FMA = 2), counted from a CSE'd restatement of the models.
+FLOP_PER_STEP = {kpax.MODEL_DOUBLE_INTEGRATOR: 18, kpax.MODEL_DUBINS_AIRPLANE: 51, kpax.MODEL_QUADROTOR: 498}
+WORKLOADS = {
+    "quad": (kpax.PRESET_QUAD, E.quad_scene, "12D quadrotor, building scene (1000 AABBs incl. windowed wall), "
+             "2^16 expansions/iteration, 25 RK4 steps of 0.02 s"),
+    "dubins": (kpax.PRESET_DUBINS, E.dubins_scene, "Dubins airplane, forest of 200 columns, 2^16 expansions/iteration, "
+               "20 RK4 steps of 0.05 s"),
+    "di": (kpax.PRESET_DI, E.di_scene, "6D double integrator, 20 AABBs, 2^14 expansions/iteration, U{1..10} steps of 0.1 s"),
+}
+FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+def load_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0, "fallback": True}
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(prefix="kpax_clocks_", suffix=".csv")[1])
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader",
+                                          "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self) -> dict | None:
+        if not self.proc:
+            return None
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1].split()[0]))
+                mx.append(float(f[2].split()[0]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        self.path.unlink(missing_ok=True)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def frontier_parents(cfg, obs, start, goal, n_parents: int = 2048):
+    """States of late frontier nodes from a short CPU plan (the oracle; CPU-baseline inputs only)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    small = cfg.copy()
+    small.expansions_per_iter = min(cfg.expansions_per_iter, 1 << 13)
+    r = O.plan(small, start, goal, obs, plan_idx=7, max_iters=6, stop_at_goal=False)
+    rows = r["rows"][-n_parents:, : cfg.state_dim]
+    return np.ascontiguousarray(rows, np.float32)
+
+
+def cpu_reference_rate(cfg, obs, parents, budget_s: float, per_parent: int = 32, max_children: int = 1 << 16):
+    """The reference's own per-child expansion body (oracle/_ref, OpenMP, all host threads)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    ref = O.RefLib(cfg.model)
+    ref.set_obstacles(obs)
+    threads = ref.L.kref_max_threads()
+    n1, P = ref.num_r1, ref.r2_per_r1
+    n = min(max_children, parents.shape[0] * per_parent)
+    draws = E.uniform_draws(n, 99)
+    if cfg.fixed_steps:
+        N = cfg.max_propagation_duration
+        draws[:, 4] = np.float32((N - 0.5) / N)
+    scores = np.zeros(n1, np.float32)
+    valid_total, t_total, batches = 0, 0.0, 0
+    # size the sample to the budget: shrink the batch if one batch takes too long
+    while t_total < budget_s:
+        flags = np.zeros(n1 * P, np.int32)
+        counter = np.zeros(n1, np.int32)
+        vc = np.zeros(n1, np.int32)
+        t0 = time.perf_counter()
+        nv, _, _ = ref.expand(parents, per_parent, draws[:n], scores, flags, counter, vc, threads)
+        dt = time.perf_counter() - t0
+        valid_total += nv
+        t_total += dt
+        batches += 1
+        if batches == 1 and dt > budget_s / 3 and n > 4096:
+            n //= 4
+    return valid_total / t_total, threads, f"{batches} batches of <= {n} children (32 per frontier parent), {t_total:.1f} s"
+
+
+def dist_setup(n_gpus: int):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def run_reference(args) -> None:
+    ws, rank, _ = dist_setup(args.gpus)
+    if rank != 0:
+        return
+    pre, scene, desc = WORKLOADS[args.workload]
+    cfg = kpax.preset(pre)
+    obs, start, goal = scene()
+    parents = frontier_parents(cfg, obs, start, goal)
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    ref = O.RefLib(cfg.model)
+    ref.set_obstacles(obs)
+    threads = ref.L.kref_max_threads()
+    n1, P = ref.num_r1, ref.r2_per_r1
+    n = min(cfg.expansions_per_iter, parents.shape[0] * 32)
+    draws = E.uniform_draws(n, 98)
+    if cfg.fixed_steps:
+        draws[:, 4] = np.float32((cfg.max_propagation_duration - 0.5) / cfg.max_propagation_duration)
+    scores = np.zeros(n1, np.float32)
+
+    def step(m):
+        flags = np.zeros(n1 * P, np.int32)
+        c = np.zeros(n1, np.int32)
+        v = np.zeros(n1, np.int32)
+        t0 = time.perf_counter()
+        nv, _, _ = ref.expand(parents, 32, draws[:m], scores, flags, c, v, threads)
+        return nv, time.perf_counter() - t0
+
+    m = n
+    for i in range(max(args.warmup, 1)):
+        _, dt = step(m)
+        if i == 0 and dt * args.steps > 120 and m > 4096:  # keep the whole run within a few minutes
+            m = max(4096, int(m * 120 / (dt * args.steps)))
+    tot_v, tot_t = 0, 0.0
+    for _ in range(args.steps):
+        nv, dt = step(m)
+        tot_v += nv
+        tot_t += dt
+    value = tot_v / tot_t
+    sample = f"{m} children of frontier parents per step (reference per-child body, KPAX.cu:381-396)"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000 * tot_t / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": desc, "expansions_per_step": m, "parallelism": "host OpenMP"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args) -> None:
+    import torch
+
+    ws, rank, local = dist_setup(args.gpus)
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device (no CPU fallback)")
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    pre, scene, desc = WORKLOADS[args.workload]
+    cfg = kpax.preset(pre)
+    cfg.seed = cfg.seed + 1000003 * rank
+    obs, start, goal = scene()
+    d_obs = torch.from_numpy(obs).cuda()
+    pl = kpax.KPAX(cfg)
+    stream = torch.cuda.ExternalStream(pl.stream)
+    pl.begin(start, goal, d_obs.data_ptr(), obs.shape[0])
+    pl.iterate_timed(8, 0)  # grow the frontier until every iteration uses the full budget
+    pl.iterate_timed(max(args.warmup, 3), FLUSH_BYTES)
+    launches0 = kpax.kernel_launches()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        times, tot = pl.iterate_timed(args.steps, FLUSH_BYTES)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches = kpax.kernel_launches() - launches0
+    t_s = float(times[:, 0].sum()) / 1000.0
+    t_exp = float(times[:, 2].sum()) / 1000.0
+    valid = tot["valid"]
+    if dist:
+        tt = torch.tensor([t_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        vv = torch.tensor([valid], dtype=torch.float64, device="cuda")
+        dist.all_reduce(vv, op=dist.ReduceOp.SUM)
+        t_s, valid_all = float(tt.item()), float(vv.item())
+    else:
+        valid_all = float(valid)
+    value = valid_all / t_s
+
+    # roofline of the expansion kernel: FP32 issue bound
+    peaks = load_peaks()
+    flops = tot["steps"] * FLOP_PER_STEP[cfg.model]
+    achieved = flops / t_exp / 1e12
+    sm_mhz = peaks.get("sm_max_mhz", 1965.0)
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                "traffic": None, "kernel": "k_expand",
+                "peak_note": "nominal FP32: 148 SM x 128 lanes x 2 FLOP x clocks.max.sm (no measured FP32 peak in "
+                             "MEASURED_PEAKS.json)",
+                "work": f"{tot['steps']} RK4 steps x {FLOP_PER_STEP[cfg.model]} FLOP over {args.steps} launches",
+                "expand_ms_per_launch": 1000 * t_exp / args.steps}
+
+    # end to end: whole plans from host buffers through the C ABI
+    e2e_v, e2e_t, tts, found = 0, 0.0, [], 0
+    plans = args.plans
+    h2d = obs.nbytes + 2 * 4 * cfg.sample_dim
+    d2h = 0
+    for i in range(plans):
+        t0 = time.perf_counter()
+        r = pl.plan_host(start, goal, obs)
+        dt = time.perf_counter() - t0
+        e2e_v += r.valid_expansions
+        e2e_t += dt
+        d2h += 4 * cfg.sample_dim * r.path_len + 128
+        if r.found:
+            found += 1
+            tts.append(1000 * dt)
+    e2e = {"value": e2e_v / e2e_t, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h // max(plans, 1),
+           "plans": plans, "success_rate": found / max(plans, 1),
+           "tts_ms_p50": float(np.percentile(tts, 50)) if tts else None,
+           "tts_ms_p95": float(np.percentile(tts, 95)) if tts else None}
+
+    clocks = clk.summary()
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        try:
+            parents = frontier_parents(cfg, obs, start, goal)
+            rate, cores, sample = cpu_reference_rate(cfg, obs, parents, args.cpu_seconds)
+            cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample}
+        except (FileNotFoundError, OSError) as exc:
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {exc}"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000 * t_s / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": desc, "expansions_per_iter": cfg.expansions_per_iter,
+                       "children_per_step": tot["children"] // args.steps, "l2": "flushed before each timed iteration "
+                       "(256 MiB write, outside the events)", "parallelism": f"replicas x{ws}"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+            "breakdown_ms_per_step": {"frontier": float(times[:, 1].mean()), "expand": float(times[:, 2].mean()),
+                                      "scores": float(times[:, 3].mean())},
+        }
+        print(json.dumps(line), flush=True)
+    pl.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="quad")
+    ap.add_argument("--plans", type=int, default=8)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

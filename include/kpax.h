@@ -1,0 +1,213 @@
+/*
+ * kpax.h — C ABI of the B200-native Kino-PAX tree-expansion library (libkpax.so).
+ *
+ * The reference planner is a C++ class whose configuration is compile-time macros
+ * (include/config/config.h) and whose entry point is
+ *     void KPAX::plan(float* h_initial, float* h_goal, float* d_obstacles_ptr,
+ *                     uint h_obstaclesCount, bool saveTree)          (src/planners/KPAX.cu:51)
+ * This header replaces it with plain-C calls: a runtime configuration struct that carries
+ * every macro the hot path reads, an opaque planner handle owning the device buffers, and
+ * the same plan(init, goal, device obstacles) entry.  Kernel-level entry points expose the
+ * individual stages (propagation, collision, region index) for parity tests and the
+ * propagation micro-benchmark.
+ *
+ * Conventions
+ *  - Every call returns kpax_status; nothing calls exit() or traps on the device.
+ *  - Pointers named d_* are device pointers (cudaMalloc'd by the caller), h_* are host.
+ *  - Rows use the reference's sample layout [state | control | duration] with
+ *    SAMPLE_DIM = STATE_DIM + CONTROL_DIM + 1 floats (config.h:221).
+ *  - Obstacles are n x 6 floats [min x,y,z, max x,y,z] (helper.cu:13-39 CSV layout).
+ *  - `stream` arguments are cudaStream_t passed as void* (0 = legacy default stream).
+ */
+#ifndef KPAX_H_
+#define KPAX_H_
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KPAX_ABI_VERSION 1
+
+typedef enum kpax_status {
+    KPAX_OK = 0,
+    KPAX_EINVAL = 1,     /* bad argument or configuration */
+    KPAX_ENOMEM = 2,     /* device or host allocation failed */
+    KPAX_ECUDA = 3,      /* a CUDA runtime call failed (kpax_last_error() has the text) */
+    KPAX_ETIMEOUT = 4,   /* a bounded device-side wait gave up; results are incomplete */
+    KPAX_ECAPACITY = 5,  /* a fixed-size buffer (tree, frontier, path) would overflow */
+    KPAX_ENOTFOUND = 6   /* plan finished without reaching the goal (not an error for kpax_plan) */
+} kpax_status;
+
+/* Dynamics model ids follow the reference's MODEL macro (config.h:209). */
+typedef enum kpax_model {
+    KPAX_MODEL_DOUBLE_INTEGRATOR = 1, /* 6D (x,y,z,vx,vy,vz), ctrl (ax,ay,az) */
+    KPAX_MODEL_DUBINS_AIRPLANE = 2,   /* 6D (x,y,z,yaw,pitch,v), ctrl stored (yawRate,pitchRate,a) */
+    KPAX_MODEL_QUADROTOR = 3          /* 12D (x,y,z,phi,theta,psi,u,v,w,p,q,r), ctrl (Zc,Lc,Mc,Nc) */
+} kpax_model;
+
+/* Presets for the benchmark configurations (seeded synthetic environments). */
+typedef enum kpax_preset_id {
+    KPAX_PRESET_DI = 0,       /* 6D double integrator, h 0.1, steps U{1..10}, R1 8^3, R2 2^3 */
+    KPAX_PRESET_DUBINS = 1,   /* Dubins airplane, h 0.05, 20 fixed steps, v in [0.5,2] */
+    KPAX_PRESET_QUAD = 2,     /* 12D quadrotor, h 0.02, 25 fixed steps, Zc in [0,2g], torques +-0.1 */
+    KPAX_PRESET_QUAD_REF = 3  /* 12D quadrotor exactly as the reference's active block (config.h:209-308) */
+} kpax_preset_id;
+
+/*
+ * Runtime replacement for the reference's compile-time macros.  Field comments give the macro
+ * each one stands for.  kpax_config_preset() fills every field; callers then edit what they need.
+ */
+typedef struct kpax_config {
+    int32_t model;                  /* MODEL */
+    int32_t state_dim;              /* STATE_DIM (derived from model; checked) */
+    int32_t control_dim;            /* CONTROL_DIM (derived from model; checked) */
+    uint32_t max_tree_size;         /* MAX_TREE_SIZE */
+    uint32_t max_iter;              /* MAX_ITER */
+    float step_size;                /* STEP_SIZE (RK4 step, seconds) */
+    int32_t max_propagation_duration; /* MAX_PROPAGATION_DURATION (steps) */
+    int32_t fixed_steps;            /* 0: steps = 1 + (int)(u*N) like the reference; 1: always N */
+    float goal_thresh;              /* GOAL_THRESH */
+    float w_min, w_max, w_size;     /* W_MIN, W_MAX, W_SIZE */
+    double c_min, c_max;            /* C_MIN, C_MAX (double literals +-M_PI in the reference) */
+    float v_min, v_max;             /* V_MIN, V_MAX */
+    float ctrl_min[4], ctrl_max[4]; /* control ranges in the reference's draw order:
+                                       DI (A_MIN..A_MAX)x3; Dubins (a, yawRate, pitchRate);
+                                       quad (Zc, Lc, Mc, Nc) */
+    double pitch_min, pitch_max;    /* DUBINS_AIRPLANE_MIN/MAX_PITCH (double in the reference) */
+    int32_t c_dim, v_dim;           /* C_DIM, V_DIM (region split dims; W_DIM is always 3) */
+    int32_t w_r1_length, c_r1_length, v_r1_length; /* W/C/V_R1_LENGTH */
+    int32_t w_r2_length, c_r2_length, v_r2_length; /* W/C/V_R2_LENGTH */
+    int32_t region_compat;          /* 1: R2 min-corner table in the reference's order
+                                       (Graph.cu:53-97, bit-exact R2 ids); 0: intended order */
+    float epsilon;                  /* EPSILON (score floor) */
+    float hash_cell_size;           /* GRID_CELL_SIZE (spatialHash.cuh:9) */
+    uint32_t expansions_per_iter;   /* children budget per iteration */
+    uint32_t children_per_entry;    /* children per frontier entry (reference: 32, KPAX.cu:31) */
+    uint32_t root_repeat;           /* repeat count of the root (reference: 5, KPAX.cu:77) */
+    uint32_t sparse_repeat;         /* repeat of a new node in a sparse region (15, KPAX.cu:477) */
+    int32_t sparse_valid_threshold; /* region is sparse if valid count < this (10, KPAX.cu:476) */
+    uint64_t seed;                  /* Philox4x32-10 key (the reference seeds cuRAND from the clock) */
+    int32_t block_size;             /* threads per CTA for the expansion kernel (0 = default) */
+    int32_t unroll_iters;           /* planner iterations per captured CUDA graph (0 = default) */
+    int32_t reserved[8];
+} kpax_config;
+
+/* Result of kpax_plan (the reference exposes these as public fields h_pathToGoal_, h_itr_,
+ * h_treeSize_, h_controlPathToGoal_; Planner.cuh:31-43). */
+typedef struct kpax_result {
+    int32_t found;              /* 1 if a tree node reached the goal ball */
+    uint32_t goal_idx;          /* tree index of the goal node (0 = none, as h_pathToGoal_) */
+    uint32_t path_len;          /* rows in h_path: goal node first, root last */
+    uint32_t tree_size;         /* h_treeSize_ */
+    uint32_t iters;             /* h_itr_ */
+    int32_t tree_full;          /* 1 if the tree reached max_tree_size */
+    const float* h_path;        /* planner-owned host rows (SAMPLE_DIM floats each), valid until next call */
+    double ms;                  /* device time of the plan (CUDA events) */
+    uint64_t expansions;        /* children propagated (sum of the reference's d_counterArray_) */
+    uint64_t valid_expansions;  /* valid children (sum of d_validCounterArray_, KPAX.cu:393) */
+    double path_cost;           /* sum of segment durations along the path (column SAMPLE_DIM-1) */
+} kpax_result;
+
+typedef struct kpax_planner kpax_planner;
+typedef struct kpax_env kpax_env;
+
+/* ---- configuration ---------------------------------------------------------------------- */
+kpax_status kpax_config_preset(int32_t preset, kpax_config* out);
+kpax_status kpax_config_validate(const kpax_config* cfg);
+/* Number of R1 regions, R2 regions per R1, and SAMPLE_DIM for a configuration. */
+kpax_status kpax_config_sizes(const kpax_config* cfg, uint32_t* num_r1, uint32_t* r2_per_r1,
+                              uint32_t* sample_dim);
+const char* kpax_last_error(void);
+int32_t kpax_abi_version(void);
+
+/* ---- planner (replaces KPAX::KPAX / KPAX::plan, KPAX.cu:5-115) --------------------------- */
+kpax_status kpax_create(const kpax_config* cfg, kpax_planner** out);
+kpax_status kpax_destroy(kpax_planner* planner);
+/* One full plan.  h_init/h_goal: SAMPLE_DIM host floats (only state dims are read; the goal
+ * uses x,y,z).  d_obstacles: caller-owned device buffer of n_obs*6 floats.  Returns KPAX_OK
+ * whether or not the goal was reached (see out->found). */
+kpax_status kpax_plan(kpax_planner* planner, const float* h_init, const float* h_goal,
+                      const float* d_obstacles, uint32_t n_obs, int32_t save_tree,
+                      kpax_result* out);
+/* Same, with the obstacles in host memory (copied inside the call). */
+kpax_status kpax_plan_host(kpax_planner* planner, const float* h_init, const float* h_goal,
+                           const float* h_obstacles, uint32_t n_obs, kpax_result* out);
+/* Stepwise planning: begin (reset + obstacle grid), then single iterations that never stop
+ * at the goal (used by the throughput benchmark), then a synchronising result read. */
+kpax_status kpax_plan_begin(kpax_planner* planner, const float* h_init, const float* h_goal,
+                            const float* d_obstacles, uint32_t n_obs);
+kpax_status kpax_plan_iterate(kpax_planner* planner, uint32_t n_iters, int32_t stop_at_goal);
+kpax_status kpax_plan_result(kpax_planner* planner, kpax_result* out);
+/* Per-iteration device times (ms) from CUDA events on the planner stream. */
+typedef struct kpax_iter_timing {
+    float ms_total, ms_frontier, ms_expand, ms_scores;
+} kpax_iter_timing;
+/* Benchmark entry: runs n_iters iterations without stopping at the goal.  Each is preceded,
+ * outside its timed events, by a write of flush_bytes to a scratch buffer (0 = no flush; more
+ * than the 126 MB L2 evicts it).  h_times: n_iters entries (may be NULL); h_totals (may be NULL):
+ * children propagated, valid children, RK4 steps executed, nodes appended over the n_iters. */
+kpax_status kpax_plan_iterate_timed(kpax_planner* planner, uint32_t n_iters, uint64_t flush_bytes,
+                                    kpax_iter_timing* h_times, uint64_t* h_totals);
+/* The stream all planner work is issued on (cudaStream_t as void*). */
+void* kpax_planner_stream(kpax_planner* planner);
+
+/* Tree export in the reference AoS layout (d_treeSamples_, d_treeSamplesParentIdxs_,
+ * d_treeSampleCosts_; Planner.cuh:36-38).  Any output pointer may be NULL. */
+kpax_status kpax_export_tree(kpax_planner* planner, float* h_rows, int32_t* h_parents,
+                             float* h_costs, uint32_t max_rows, uint32_t* n_rows);
+/* Region buffers (graph_.d_counterArray_, d_validCounterArray_, d_vertexScoreArray_ and the
+ * R2 activation flags as a bitset of ceil(num_r2/32) words; Graph.cuh:25-29). */
+kpax_status kpax_export_regions(kpax_planner* planner, int32_t* h_counter, int32_t* h_valid,
+                                float* h_scores, uint32_t* h_r2_bits);
+/* Per-node frontier repeat counts (0 = not in the frontier) and R1 ids of the live tree. */
+kpax_status kpax_export_frontier(kpax_planner* planner, uint8_t* h_repeat, int32_t* h_r1,
+                                 uint32_t max_rows);
+
+/* Debug capture: when enabled, every child of the latest iteration is kept (row, validity,
+ * R1, R2, frontier flag, parent) for kpax_export_children. */
+kpax_status kpax_debug_capture(kpax_planner* planner, int32_t enable);
+kpax_status kpax_export_children(kpax_planner* planner, float* h_rows, uint8_t* h_valid,
+                                 int32_t* h_r1, int32_t* h_r2, uint8_t* h_next,
+                                 int32_t* h_parent, uint32_t max_rows, uint32_t* n_children);
+
+/* ---- obstacle environment: uniform-grid spatial hash (spatialHash.cu:9-67) ------------- */
+/* Builds a compressed-sparse-row grid (no per-cell cap, deterministic ascending obstacle
+ * order inside a cell) from a device obstacle buffer on `stream`. */
+kpax_status kpax_env_create(const kpax_config* cfg, const float* d_obstacles, uint32_t n_obs,
+                            void* stream, kpax_env** out);
+kpax_status kpax_env_destroy(kpax_env* env);
+/* Grid statistics: number of cells and of (cell, obstacle) entries. */
+kpax_status kpax_env_stats(kpax_env* env, uint32_t* n_cells, uint32_t* n_entries);
+
+/* ---- kernel-level entry points (device pointers) ---------------------------------------- */
+/* Propagate n independent segments (statePropagatorSpatialHash.cu:72-308).
+ *  d_parents: n x state_dim floats.
+ *  d_draws:   n x 5 uniforms in (0,1] in the reference's draw order (controls..., duration;
+ *             3-control models ignore column 3), or NULL to draw from Philox4x32-10 keyed by
+ *             (cfg->seed, draw_stream) with counter = segment index.
+ *  d_rows:    n x SAMPLE_DIM output rows (state after the last executed step, controls,
+ *             duration) exactly as the reference writes x1.
+ *  d_valid:   n bytes, 1 = collision free and within bounds.  d_steps (optional): executed steps. */
+kpax_status kpax_propagate_batch(const kpax_config* cfg, kpax_env* env, const float* d_parents,
+                                 const float* d_draws, uint32_t draw_stream, uint32_t n,
+                                 float* d_rows, uint8_t* d_valid, int32_t* d_steps, void* stream);
+/* Broad-phase check of n boxes against the grid (isMotionValidSpatialHash, spatialHash.cu:145-194).
+ * d_bbmin/d_bbmax: n x 3 floats.  d_free: n bytes, 1 = no obstacle overlaps the box. */
+kpax_status kpax_collide_batch(kpax_env* env, const float* d_bbmin, const float* d_bbmax,
+                               uint32_t n, uint8_t* d_free, void* stream);
+/* R1 / R2 region ids of n states (getRegion / getSubRegion, Graph.cu:99-205).
+ * d_states: n x state_dim floats; d_r2 may be NULL. */
+kpax_status kpax_region_batch(const kpax_config* cfg, const float* d_states, uint32_t n,
+                              int32_t* d_r1, int32_t* d_r2, void* stream);
+/* Number of propagation kernels (and other library kernels) launched since load; the
+ * benchmark reports it as evidence that the device path ran. */
+uint64_t kpax_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KPAX_H_ */

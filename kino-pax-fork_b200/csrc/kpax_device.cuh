@@ -1,0 +1,401 @@
+// kpax_device.cuh — device building blocks of the expansion step.
+//
+// Rounding contract with the CPU oracle (oracle/kpax_oracle.c):
+//  - control draws, step counts, region ids, cell ids, goal distance and scores are computed
+//    with explicitly rounded intrinsics (__fadd_rn/__fmul_rn/__fdiv_rn) so no multiply-add is
+//    fused; they are bit-identical to the oracle for identical inputs;
+//  - the double-integrator step is written the same way, so DI segments are bit-identical;
+//  - Dubins and quadrotor RK4 use the accurate sincosf/tanf/sqrtf and let the compiler fuse
+//    multiply-adds; they match the oracle within the propagation tolerance.
+#pragma once
+#include <stdint.h>
+
+#include "kpax_params.h"
+
+namespace kpax {
+
+// ------------------------------------------------------------------ Philox4x32-10
+// Salmon et al., SC'11.  ctr = {index, iter, sub-stream, stream}, key = seed.
+struct U4 {
+    uint32_t x, y, z, w;
+};
+
+__device__ __forceinline__ U4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1)
+{
+#pragma unroll
+    for(int r = 0; r < 10; ++r) {
+        uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+        uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+        uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0, c1 = lo1, c2 = n2, c3 = lo0;
+        k0 += 0x9E3779B9u, k1 += 0xBB67AE85u;
+    }
+    return {c0, c1, c2, c3};
+}
+
+// ((x >> 8) + 1) * 2^-24: exact, in (0, 1].
+__device__ __forceinline__ float u01(uint32_t x) { return __uint2float_rn((x >> 8) + 1u) * 5.9604644775390625e-8f; }
+
+// The six uniforms of a child: controls c0..c3, duration, frontier draw.
+__device__ __forceinline__ void child_draws(const KParams& p, uint32_t stream, uint32_t iter, uint32_t index, float u[6])
+{
+    U4 a = philox(index, iter, 0u, stream, p.seed_lo, p.seed_hi);
+    U4 b = philox(index, iter, 1u, stream, p.seed_lo, p.seed_hi);
+    u[0] = u01(a.x), u[1] = u01(a.y), u[2] = u01(a.z), u[3] = u01(a.w);
+    u[4] = u01(b.x), u[5] = u01(b.y);
+}
+
+__device__ __forceinline__ float reactivate_draw(const KParams& p, uint32_t stream, uint32_t iter, uint32_t index)
+{
+    return u01(philox(index, iter, 2u, stream, p.seed_lo, p.seed_hi).x);
+}
+
+// float -> int with the reference's device semantics (saturating, NaN -> 0).
+__device__ __forceinline__ int f2i(float x) { return __float2int_rz(x); }
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
+
+// ------------------------------------------------------------------ regions (Graph.cu:99-205)
+// state s: the first 3 + cdim + vdim floats are read.
+__device__ __forceinline__ int region_r1(const KParams& p, const float* s)
+{
+    int w = 0, f = 1;
+#pragma unroll
+    for(int i = 2; i >= 0; --i) {
+        int idx = f2i(__fdiv_rn(__fmul_rn((float)p.W1, __fsub_rn(s[i], p.wmin)), p.wspan));
+        w += f * clampi(idx, 0, p.W1 - 1);
+        f *= p.W1;
+    }
+    if(p.w_only) return w;
+    int a = 0, v = 0;
+    if(p.C1 > 1) {
+        f = 1;
+        for(int i = p.cdim - 1; i >= 0; --i) {
+            const float x = s[3 + i];
+            int idx = 0;
+            for(int k = 0; k < p.C1 - 1; ++k) idx += (x >= p.cthr1[k]);
+            a += f * idx;
+            f *= p.C1;
+        }
+    }
+    if(p.V1 > 1) {
+        f = 1;
+        for(int i = p.vdim - 1; i >= 0; --i) {
+            int idx = f2i(__fdiv_rn(__fmul_rn((float)p.V1, __fsub_rn(s[3 + p.cdim + i], p.vmin_r)), p.vspan));
+            v += f * clampi(idx, 0, p.V1 - 1);
+            f *= p.V1;
+        }
+    }
+    return w * p.r1_mulW + a * p.r1_mulA + v;
+}
+
+// Cell digits of an R1 id whose min corner getSubRegion reads.  In compat mode the id is
+// decoded the way initializeRegions_kernel lays out its table (Graph.cu:58-96: workspace part
+// fastest, C_R1^2 attitude cells, then velocity); otherwise in getRegion's order (Q5).
+struct R1Digits {
+    int w[3], a[8], v[8];
+};
+
+__device__ __forceinline__ void r1_digits(const KParams& p, int r1, R1Digits& d)
+{
+    int wr, ar, vr;
+    if(p.compat) {
+        const int W3 = p.W1 * p.W1 * p.W1;
+        wr = r1 % W3;
+        ar = (r1 / W3) % (p.C1 * p.C1);
+        vr = (r1 / (W3 * p.C1 * p.C1)) % p.V1;
+    } else {
+        wr = r1 / p.r1_mulW;
+        const int rem = r1 - wr * p.r1_mulW;
+        ar = rem / p.r1_mulA;
+        vr = rem - ar * p.r1_mulA;
+    }
+#pragma unroll
+    for(int i = 2; i >= 0; --i) d.w[i] = wr % p.W1, wr /= p.W1;
+    for(int i = p.cdim - 1; i >= 0; --i) d.a[i] = ar % p.C1, ar /= p.C1;
+    for(int i = p.vdim - 1; i >= 0; --i) d.v[i] = vr % p.V1, vr /= p.V1;
+}
+
+// getSubRegion (Graph.cu:155-205).  The R1 min corner is W_MIN + i*W_R1_SIZE (float),
+// C_MIN + i*C_R1_SIZE (double, tabulated) and V_MIN + i*V_R1_SIZE (float), as Graph.cu:69-95.
+__device__ __forceinline__ int region_r2(const KParams& p, const float* s, int r1)
+{
+    R1Digits d;
+    r1_digits(p, r1, d);
+    int w = 0, f = 1;
+#pragma unroll
+    for(int i = 2; i >= 0; --i) {
+        const float m = __fadd_rn(p.wmin, __fmul_rn((float)d.w[i], p.w1size));
+        int idx = f2i(__fdiv_rn(__fmul_rn((float)p.W2, __fsub_rn(s[i], m)), p.w1size));
+        w += f * clampi(idx, 0, p.W2 - 1);
+        f *= p.W2;
+    }
+    int a = 0, v = 0;
+    if(p.C2 > 1) {
+        f = 1;
+        for(int i = p.cdim - 1; i >= 0; --i) {
+            const float t = __fmul_rn((float)p.C2, __fsub_rn(s[3 + i], p.cmin_tab[d.a[i]]));
+            int idx = 0;
+            for(int k = 0; k < p.C2 - 1; ++k) idx += (t >= p.cthr2[k]);
+            a += f * idx;
+            f *= p.C2;
+        }
+    }
+    if(p.V2 > 1) {
+        f = 1;
+        for(int i = p.vdim - 1; i >= 0; --i) {
+            const float m = __fadd_rn(p.vmin_r, __fmul_rn((float)d.v[i], p.v1size));
+            int idx = f2i(__fdiv_rn(__fmul_rn((float)p.V2, __fsub_rn(s[3 + p.cdim + i], m)), p.v1size));
+            v += f * clampi(idx, 0, p.V2 - 1);
+            f *= p.V2;
+        }
+    }
+    return r1 * p.P + (w * p.r2_mulW + a * p.r2_mulA + v);
+}
+
+// ------------------------------------------------------------------ spatial hash
+// CSR grid over the workspace cube; obstacles as float4 pairs (min xyz, max xyz).
+struct Grid {
+    const float4* __restrict__ obs;
+    const uint32_t* __restrict__ off;  // cells + 1
+    const uint32_t* __restrict__ ent;
+    float wmin, cell;
+    int dim;
+};
+
+__device__ __forceinline__ int grid_coord(const Grid& g, float x)
+{
+    return clampi(f2i(__fdiv_rn(__fsub_rn(x, g.wmin), g.cell)), 0, g.dim - 1);
+}
+
+// isMotionValidSpatialHash (spatialHash.cu:145-194) with isBroadPhaseValid (collisionCheck.cu:3-10):
+// true when no obstacle overlaps the box strictly in all three dimensions.
+__device__ __forceinline__ bool box_free(const Grid& g, const float lo[3], const float hi[3])
+{
+    const int x0 = grid_coord(g, lo[0]), y0 = grid_coord(g, lo[1]), z0 = grid_coord(g, lo[2]);
+    const int x1 = grid_coord(g, hi[0]), y1 = grid_coord(g, hi[1]), z1 = grid_coord(g, hi[2]);
+    for(int gz = z0; gz <= z1; ++gz)
+        for(int gy = y0; gy <= y1; ++gy)
+            for(int gx = x0; gx <= x1; ++gx) {
+                const int c = gx + g.dim * (gy + g.dim * gz);
+                const uint32_t b = __ldg(g.off + c), e = __ldg(g.off + c + 1);
+                for(uint32_t k = b; k < e; ++k) {
+                    const uint32_t o = __ldg(g.ent + k);
+                    const float4 a = __ldg(g.obs + 2 * o), m = __ldg(g.obs + 2 * o + 1);
+                    if(hi[0] > a.x && m.x > lo[0] && hi[1] > a.y && m.y > lo[1] && hi[2] > a.z && m.z > lo[2]) return false;
+                }
+            }
+    return true;
+}
+
+__device__ __forceinline__ bool step_free(const Grid& g, const float p0[3], const float p1[3])
+{
+    float lo[3], hi[3];
+#pragma unroll
+    for(int d = 0; d < 3; ++d) {
+        const bool sw = p0[d] > p1[d];
+        lo[d] = sw ? p1[d] : p0[d];
+        hi[d] = sw ? p0[d] : p1[d];
+    }
+    return box_free(g, lo, hi);
+}
+
+__device__ __forceinline__ bool finite_all(const float* s, int n)
+{
+    bool ok = true;
+#pragma unroll
+    for(int i = 0; i < n; ++i) ok = ok && isfinite(s[i]);
+    return ok;
+}
+
+// ------------------------------------------------------------------ controls
+// statePropagatorSpatialHash.cu:74-77 / 141-144 / 236-241: c = MIN + u * (MAX - MIN);
+// steps = 1 + (int)(u * N) (N + 1 when u == 1, as in the reference).
+__device__ __forceinline__ int draw_controls(const KParams& p, const float u[6], float c[4])
+{
+#pragma unroll
+    for(int i = 0; i < 4; ++i) c[i] = __fadd_rn(p.clo[i], __fmul_rn(u[i], p.crng[i]));
+    return p.fixed_steps ? p.nsteps : 1 + f2i(__fmul_rn(u[4], (float)p.nsteps));
+}
+
+// ------------------------------------------------------------------ models
+// Each propagates `steps` steps from s (in place), checking every step like the reference,
+// and returns validity; `done` receives the number of steps executed.
+
+// Double integrator, statePropagatorSpatialHash.cu:72-134 (Q1: x += h(5v + 2ah)/6).
+__device__ __forceinline__ bool prop_di(const KParams& p, const Grid& g, float* s, const float* c, int steps, int& done)
+{
+    const float h = p.h;
+    bool valid = true;
+    int i = 0;
+    for(; i < steps; ++i) {
+        const float p0[3] = {s[0], s[1], s[2]};
+#pragma unroll
+        for(int d = 0; d < 3; ++d) {
+            const float v = s[3 + d], a = c[d];
+            // (v + (v + 2*(v + a*h/2) + (v + a*h))) * h / 6
+            const float t1 = __fadd_rn(v, __fdiv_rn(__fmul_rn(a, h), 2.0f));
+            const float t2 = __fadd_rn(v, __fmul_rn(a, h));
+            const float sum = __fadd_rn(v, __fadd_rn(__fadd_rn(v, __fmul_rn(2.0f, t1)), t2));
+            s[d] = __fadd_rn(s[d], __fdiv_rn(__fmul_rn(sum, h), 6.0f));
+            // (a + 2a + 2a + a) * h / 6
+            const float asum = __fadd_rn(__fadd_rn(__fadd_rn(a, __fmul_rn(2.0f, a)), __fmul_rn(2.0f, a)), a);
+            s[3 + d] = __fadd_rn(v, __fdiv_rn(__fmul_rn(asum, h), 6.0f));
+        }
+        if(s[3] < p.vmin || s[3] > p.vmax || s[4] < p.vmin || s[4] > p.vmax || s[5] < p.vmin || s[5] > p.vmax) {
+            valid = false;
+            break;
+        }
+        if(s[0] < p.ws_lo || s[0] > p.ws_hi || s[1] < p.ws_lo || s[1] > p.ws_hi || s[2] < p.ws_lo || s[2] > p.ws_hi) {
+            valid = false;
+            break;
+        }
+        if(!finite_all(s, 6) || !step_free(g, p0, s)) {
+            valid = false;
+            break;
+        }
+    }
+    done = i < steps ? i + 1 : steps;
+    return valid;
+}
+
+// Dubins airplane, statePropagatorSpatialHash.cu:139-229; c = (a, yawRate, pitchRate).
+__device__ __forceinline__ bool prop_dubins(const KParams& p, const Grid& g, float* s, const float* c, int steps, int& done)
+{
+    const float h = p.h, hh = p.hh, h6 = p.h6;
+    const float a = c[0], yr = c[1], pr = c[2];
+    bool valid = true;
+    int i = 0;
+    for(; i < steps; ++i) {
+        const float p0[3] = {s[0], s[1], s[2]};
+        const float yaw = s[3], pitch = s[4], v = s[5];
+        float sp0, cp0, sy0, cy0, sp1, cp1, sy1, cy1, sp2, cp2, sy2, cy2;
+        sincosf(pitch, &sp0, &cp0);
+        sincosf(yaw, &sy0, &cy0);
+        sincosf(pitch + hh * pr, &sp1, &cp1);
+        sincosf(yaw + hh * yr, &sy1, &cy1);
+        sincosf(pitch + h * pr, &sp2, &cp2);
+        sincosf(yaw + h * yr, &sy2, &cy2);
+        const float vm = v + hh * a, ve = v + h * a;
+        const float mx = vm * cp1 * cy1, my = vm * cp1 * sy1, mz = vm * sp1;
+        s[0] += h6 * (v * cp0 * cy0 + 2.0f * (mx + mx) + ve * cp2 * cy2);
+        s[1] += h6 * (v * cp0 * sy0 + 2.0f * (my + my) + ve * cp2 * sy2);
+        s[2] += h6 * (v * sp0 + 2.0f * (mz + mz) + ve * sp2);
+        s[3] = yaw + h * yr;
+        s[4] = pitch + h * pr;
+        s[5] = v + h6 * (a + 2.0f * (a + a) + a);
+        if(s[5] < p.vmin || s[5] > p.vmax || s[4] < p.pitch_lo || s[4] > p.pitch_hi) {
+            valid = false;
+            break;
+        }
+        if(s[0] < p.ws_lo || s[0] > p.ws_hi || s[1] < p.ws_lo || s[1] > p.ws_hi || s[2] < p.ws_lo || s[2] > p.ws_hi) {
+            valid = false;
+            break;
+        }
+        if(!finite_all(s, 6) || !step_free(g, p0, s)) {
+            valid = false;
+            break;
+        }
+    }
+    done = i < steps ? i + 1 : steps;
+    return valid;
+}
+
+// Quadrotor right-hand side, statePropagator.cu:325-370, evaluated at x0 + delta*k.
+// Model constants NU 10e-3, MU 2e-6, IX 1, IY 1, IZ 2, GRAVITY -9.81, MASS 1 (config.h:300-308).
+__device__ __forceinline__ void quad_rhs(float* xd, const float* x0, const float* k, float delta, const float* c)
+{
+    const float NU = 10e-3f, MU = 2e-6f, G = -9.81f;
+    const float phi = x0[3] + delta * k[3], theta = x0[4] + delta * k[4], psi = x0[5] + delta * k[5];
+    const float u = x0[6] + delta * k[6], v = x0[7] + delta * k[7], w = x0[8] + delta * k[8];
+    const float pp = x0[9] + delta * k[9], q = x0[10] + delta * k[10], r = x0[11] + delta * k[11];
+    float sf, cf, st, ct, sp, cp;
+    sincosf(phi, &sf, &cf);
+    sincosf(theta, &st, &ct);
+    sincosf(psi, &sp, &cp);
+    const float tt = tanf(theta);
+    xd[0] = ct * cp * u + (sf * st * cp - cf * sp) * v + (cf * st * cp + sf * sp) * w;
+    xd[1] = ct * sp * u + (sf * st * sp + cf * cp) * v + (cf * st * sp - sf * cp) * w;
+    xd[2] = -st * u + sf * ct * v + cf * ct * w;
+    const float qr = q * sf + r * cf;
+    xd[3] = pp + qr * tt;
+    xd[4] = q * cf - r * sf;
+    xd[5] = qr / ct;
+    const float XYZ = -NU * sqrtf(u * u + v * v + w * w);
+    xd[6] = (r * v - q * w) - G * st + XYZ * u;
+    xd[7] = (pp * w - r * u) + G * ct * sf + XYZ * v;
+    xd[8] = (q * u - pp * v) + G * ct * cf + XYZ * w + c[0];
+    const float LMN = -MU * sqrtf(pp * pp + q * q + r * r);
+    xd[9] = -(q * r) + LMN * pp + c[1];          // (IY - IZ)/IX = -1, 1/IX = 1
+    xd[10] = (pp * r) + LMN * q + c[2];          // (IZ - IX)/IY = 1,  1/IY = 1
+    xd[11] = 0.0f * (pp * q) + 0.5f * (LMN * r) + 0.5f * c[3];  // (IX - IY)/IZ = 0, 1/IZ = 0.5
+}
+
+// Quadrotor RK4, statePropagatorSpatialHash.cu:234-308.
+__device__ __forceinline__ bool prop_quad(const KParams& p, const Grid& g, float* s, const float* c, int steps, int& done)
+{
+    const float h = p.h, hh = p.hh, h6 = p.h6;
+    const float zero[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    bool valid = true;
+    int i = 0;
+    for(; i < steps; ++i) {
+        const float p0[3] = {s[0], s[1], s[2]};
+        float k1[12], k2[12], k3[12], k4[12];
+        quad_rhs(k1, s, zero, 1.0f, c);
+        quad_rhs(k2, s, k1, hh, c);
+        quad_rhs(k3, s, k2, hh, c);
+        quad_rhs(k4, s, k3, h, c);
+#pragma unroll
+        for(int j = 0; j < 12; ++j) s[j] += h6 * (k1[j] + 2.0f * k2[j] + 2.0f * k3[j] + k4[j]);
+        if(s[6] < p.vmin || s[6] > p.vmax || s[7] < p.vmin || s[7] > p.vmax || s[8] < p.vmin || s[8] > p.vmax) {
+            valid = false;
+            break;
+        }
+        if(s[0] < p.ws_lo || s[0] > p.ws_hi || s[1] < p.ws_lo || s[1] > p.ws_hi || s[2] < p.ws_lo || s[2] > p.ws_hi) {
+            valid = false;
+            break;
+        }
+        if(!finite_all(s, 12) || !step_free(g, p0, s)) {
+            valid = false;
+            break;
+        }
+    }
+    done = i < steps ? i + 1 : steps;
+    return valid;
+}
+
+template <int M>
+__device__ __forceinline__ bool propagate(const KParams& p, const Grid& g, float* s, const float* c, int steps, int& done)
+{
+    if constexpr(M == KPAX_MODEL_DOUBLE_INTEGRATOR) return prop_di(p, g, s, c, steps, done);
+    else if constexpr(M == KPAX_MODEL_DUBINS_AIRPLANE) return prop_dubins(p, g, s, c, steps, done);
+    else return prop_quad(p, g, s, c, steps, done);
+}
+
+template <int M>
+struct ModelDims;
+template <>
+struct ModelDims<KPAX_MODEL_DOUBLE_INTEGRATOR> {
+    static constexpr int SD = 6, CD = 3;
+};
+template <>
+struct ModelDims<KPAX_MODEL_DUBINS_AIRPLANE> {
+    static constexpr int SD = 6, CD = 3;
+};
+template <>
+struct ModelDims<KPAX_MODEL_QUADROTOR> {
+    static constexpr int SD = 12, CD = 4;
+};
+
+// Controls as stored in the row: Dubins stores (yawRate, pitchRate, a) (statePropagatorSpatialHash.cu:223-225).
+template <int M>
+__device__ __forceinline__ void row_controls(const float* c, float* out)
+{
+    if constexpr(M == KPAX_MODEL_DUBINS_AIRPLANE) {
+        out[0] = c[1], out[1] = c[2], out[2] = c[0], out[3] = 0.0f;
+    } else {
+#pragma unroll
+        for(int i = 0; i < 4; ++i) out[i] = c[i];
+    }
+}
+
+}  // namespace kpax

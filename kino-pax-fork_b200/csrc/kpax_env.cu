@@ -1,0 +1,323 @@
+// kpax_env.cu — obstacle grid build and the kernel-level batch entry points.
+//
+// The reference keeps a fixed 16-slot list per 5 m cell and rebuilds it with atomics every
+// iteration (spatialHash.cu:9-67, KPAX.cu:306), silently dropping entries past 16 (Q2).  Here
+// the grid is compressed sparse rows (count -> scan -> fill), holds every (cell, obstacle)
+// pair and is built once per plan.  Query verdicts equal the brute-force isMotionValid
+// (collisionCheck.cu:49-62) for every box: the cell map is monotone, so any strictly
+// overlapping obstacle shares at least one cell with the box.
+#include <stdio.h>
+#include <string.h>
+
+#include "kpax_internal.h"
+
+namespace kpax {
+
+std::atomic<uint64_t> g_launches{0};
+
+namespace {
+
+__device__ __forceinline__ void obstacle_cells(const Grid& g, const float4& lo, const float4& hi, int c0[3], int c1[3])
+{
+    c0[0] = grid_coord(g, lo.x), c0[1] = grid_coord(g, lo.y), c0[2] = grid_coord(g, lo.z);
+    c1[0] = grid_coord(g, hi.x), c1[1] = grid_coord(g, hi.y), c1[2] = grid_coord(g, hi.z);
+}
+
+// Pack n x 6 floats into float4 pairs and count (cell, obstacle) pairs per cell.
+__global__ void k_env_count(Grid g, const float* __restrict__ obs, uint32_t n, float4* __restrict__ packed,
+                            uint32_t* __restrict__ counts)
+{
+    const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+    if(o >= n) return;
+    const float* b = obs + (size_t)6 * o;
+    const float4 lo = make_float4(b[0], b[1], b[2], 0.0f), hi = make_float4(b[3], b[4], b[5], 0.0f);
+    packed[2 * o] = lo;
+    packed[2 * o + 1] = hi;
+    int c0[3], c1[3];
+    obstacle_cells(g, lo, hi, c0, c1);
+    for(int z = c0[2]; z <= c1[2]; ++z)
+        for(int y = c0[1]; y <= c1[1]; ++y)
+            for(int x = c0[0]; x <= c1[0]; ++x) atomicAdd(counts + x + g.dim * (y + g.dim * z), 1u);
+}
+
+// Exclusive scan of counts[0, n) in place (single CTA of 1024 threads); counts[n] = total;
+// cursor gets a copy of the offsets.
+__global__ void __launch_bounds__(1024) k_env_scan(uint32_t* __restrict__ counts, uint32_t n, uint32_t* __restrict__ cursor)
+{
+    __shared__ uint32_t s_warp[32];
+    __shared__ uint32_t s_carry;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if(threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    for(uint32_t base = 0; base < n; base += 1024) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t v = i < n ? counts[i] : 0u;
+        uint32_t x = v;
+#pragma unroll
+        for(int d = 1; d < 32; d <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+            if(lane >= d) x += y;
+        }
+        if(lane == 31) s_warp[warp] = x;
+        __syncthreads();
+        if(warp == 0) {
+            uint32_t w = s_warp[lane];
+#pragma unroll
+            for(int d = 1; d < 32; d <<= 1) {
+                uint32_t y = __shfl_up_sync(0xffffffffu, w, d);
+                if(lane >= d) w += y;
+            }
+            s_warp[lane] = w;
+        }
+        __syncthreads();
+        const uint32_t excl = s_carry + (warp ? s_warp[warp - 1] : 0u) + x - v;
+        if(i < n) counts[i] = excl, cursor[i] = excl;
+        __syncthreads();
+        if(threadIdx.x == 1023) s_carry = excl + v;
+        __syncthreads();
+    }
+    if(threadIdx.x == 0) counts[n] = s_carry;
+}
+
+__global__ void k_env_fill(Grid g, const float4* __restrict__ packed, uint32_t n, uint32_t* __restrict__ cursor,
+                           uint32_t* __restrict__ ent)
+{
+    const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+    if(o >= n) return;
+    int c0[3], c1[3];
+    obstacle_cells(g, packed[2 * o], packed[2 * o + 1], c0, c1);
+    for(int z = c0[2]; z <= c1[2]; ++z)
+        for(int y = c0[1]; y <= c1[1]; ++y)
+            for(int x = c0[0]; x <= c1[0]; ++x) ent[atomicAdd(cursor + x + g.dim * (y + g.dim * z), 1u)] = o;
+}
+
+// ---------------------------------------------------------------- batch kernels
+
+template <int M>
+__global__ void __launch_bounds__(256) k_propagate_batch(KParams p, Grid g, const float* __restrict__ parents,
+                                                         const float* __restrict__ draws, uint32_t stream_id, uint32_t n,
+                                                         float* __restrict__ rows, uint8_t* __restrict__ valid,
+                                                         int32_t* __restrict__ steps_out)
+{
+    constexpr int SD = ModelDims<M>::SD, CD = ModelDims<M>::CD, S = SD + CD + 1;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    float s[SD], u[6], c[4], rc[4];
+#pragma unroll
+    for(int k = 0; k < SD; ++k) s[k] = __ldg(parents + (size_t)i * SD + k);
+    if(draws) {
+#pragma unroll
+        for(int k = 0; k < 5; ++k) u[k] = __ldg(draws + (size_t)i * 5 + k);
+        u[5] = 0.0f;
+    } else {
+        child_draws(p, stream_id, 0u, i, u);
+    }
+    const int steps = draw_controls(p, u, c);
+    int done = 0;
+    const bool ok = propagate<M>(p, g, s, c, steps, done);
+    row_controls<M>(c, rc);
+    float* dst = rows + (size_t)i * S;
+#pragma unroll
+    for(int k = 0; k < SD; ++k) dst[k] = s[k];
+#pragma unroll
+    for(int k = 0; k < CD; ++k) dst[SD + k] = rc[k];
+    dst[SD + CD] = __fmul_rn(p.h, (float)steps);  // STEP_SIZE * propagationDuration
+    valid[i] = ok ? 1 : 0;
+    if(steps_out) steps_out[i] = done;
+}
+
+__global__ void k_collide_batch(Grid g, const float* __restrict__ bbmin, const float* __restrict__ bbmax, uint32_t n,
+                                uint8_t* __restrict__ free_out)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    const float lo[3] = {bbmin[3 * i], bbmin[3 * i + 1], bbmin[3 * i + 2]};
+    const float hi[3] = {bbmax[3 * i], bbmax[3 * i + 1], bbmax[3 * i + 2]};
+    free_out[i] = box_free(g, lo, hi) ? 1 : 0;
+}
+
+__global__ void k_region_batch(KParams p, const float* __restrict__ states, uint32_t n, int32_t* __restrict__ r1,
+                               int32_t* __restrict__ r2)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    float s[12];
+    for(int k = 0; k < p.sd; ++k) s[k] = states[(size_t)i * p.sd + k];
+    const int a = region_r1(p, s);
+    r1[i] = a;
+    if(r2) r2[i] = region_r2(p, s, a);
+}
+
+}  // namespace
+
+kpax_status Env::build(const KParams& p, const float* d_obstacles, uint32_t n, cudaStream_t stream)
+{
+    cell = p.cell;
+    wmin = p.wmin;
+    dim = p.gdim;
+    const uint32_t cells = (uint32_t)dim * dim * dim;
+    if(cells != n_cells) {
+        if(d_off) cudaFree(d_off), d_off = nullptr;
+        if(d_cursor) cudaFree(d_cursor), d_cursor = nullptr;
+        KPAX_CUDA(cudaMalloc(&d_off, sizeof(uint32_t) * (cells + 1)));
+        KPAX_CUDA(cudaMalloc(&d_cursor, sizeof(uint32_t) * cells));
+        n_cells = cells;
+    }
+    if(!h_total) KPAX_CUDA(cudaMallocHost(&h_total, sizeof(uint32_t)));
+    if(n > obs_cap) {
+        if(d_obs) cudaFree(d_obs), d_obs = nullptr;
+        KPAX_CUDA(cudaMalloc(&d_obs, sizeof(float4) * 2 * n));
+        obs_cap = n;
+    }
+    n_obs = n;
+    KPAX_CUDA(cudaMemsetAsync(d_off, 0, sizeof(uint32_t) * (cells + 1), stream));
+    const Grid g0 = view();
+    if(n) {
+        k_env_count<<<(n + 255) / 256, 256, 0, stream>>>(g0, d_obstacles, n, d_obs, d_off);
+        KPAX_CHECK_LAUNCH();
+        k_env_scan<<<1, 1024, 0, stream>>>(d_off, cells, d_cursor);
+        KPAX_CHECK_LAUNCH();
+        count_launch(2);
+        KPAX_CUDA(cudaMemcpyAsync(h_total, d_off + cells, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        KPAX_CUDA(cudaStreamSynchronize(stream));
+        n_ent = *h_total;
+        if(n_ent > ent_cap) {
+            if(d_ent) cudaFree(d_ent), d_ent = nullptr;
+            const uint32_t want = n_ent + n_ent / 4 + 1024;
+            KPAX_CUDA(cudaMalloc(&d_ent, sizeof(uint32_t) * want));
+            ent_cap = want;
+        }
+        k_env_fill<<<(n + 255) / 256, 256, 0, stream>>>(view(), d_obs, n, d_cursor, d_ent);
+        KPAX_CHECK_LAUNCH();
+        count_launch(1);
+    } else {
+        n_ent = 0;
+        if(!d_ent) {
+            KPAX_CUDA(cudaMalloc(&d_ent, sizeof(uint32_t) * 1024));
+            ent_cap = 1024;
+        }
+        if(!d_obs) {
+            KPAX_CUDA(cudaMalloc(&d_obs, sizeof(float4) * 2));
+            obs_cap = 1;
+        }
+    }
+    return KPAX_OK;
+}
+
+void Env::release()
+{
+    if(d_obs) cudaFree(d_obs);
+    if(d_off) cudaFree(d_off);
+    if(d_cursor) cudaFree(d_cursor);
+    if(d_ent) cudaFree(d_ent);
+    if(h_total) cudaFreeHost(h_total);
+    d_obs = nullptr, d_off = d_cursor = d_ent = h_total = nullptr;
+    obs_cap = ent_cap = n_cells = n_ent = n_obs = 0;
+}
+
+kpax_status launch_propagate(const KParams& p, const Grid& g, const float* parents, const float* draws, uint32_t stream_id,
+                             uint32_t n, float* rows, uint8_t* valid, int32_t* steps, cudaStream_t stream)
+{
+    if(!n) return KPAX_OK;
+    const uint32_t blocks = (n + 255) / 256;
+    switch(p.model) {
+        case KPAX_MODEL_DOUBLE_INTEGRATOR:
+            k_propagate_batch<KPAX_MODEL_DOUBLE_INTEGRATOR><<<blocks, 256, 0, stream>>>(p, g, parents, draws, stream_id, n, rows, valid, steps);
+            break;
+        case KPAX_MODEL_DUBINS_AIRPLANE:
+            k_propagate_batch<KPAX_MODEL_DUBINS_AIRPLANE><<<blocks, 256, 0, stream>>>(p, g, parents, draws, stream_id, n, rows, valid, steps);
+            break;
+        default:
+            k_propagate_batch<KPAX_MODEL_QUADROTOR><<<blocks, 256, 0, stream>>>(p, g, parents, draws, stream_id, n, rows, valid, steps);
+            break;
+    }
+    KPAX_CHECK_LAUNCH();
+    count_launch();
+    return KPAX_OK;
+}
+
+}  // namespace kpax
+
+using namespace kpax;
+
+extern "C" {
+
+uint64_t kpax_kernel_launches(void) { return g_launches.load(); }
+
+kpax_status kpax_env_create(const kpax_config* cfg, const float* d_obstacles, uint32_t n_obs, void* stream, kpax_env** out)
+{
+    if(!out || (n_obs && !d_obstacles)) return set_error("kpax_env_create: null argument"), KPAX_EINVAL;
+    *out = nullptr;
+    kpax_env* e = new kpax_env();
+    kpax_status st = derive_params(*cfg, &e->params);
+    if(st == KPAX_OK) st = e->env.build(e->params, d_obstacles, n_obs, (cudaStream_t)stream);
+    if(st == KPAX_OK) {
+        cudaError_t err = cudaStreamSynchronize((cudaStream_t)stream);
+        if(err != cudaSuccess) set_error("kpax_env_create: %s", cudaGetErrorString(err)), st = KPAX_ECUDA;
+    }
+    if(st != KPAX_OK) {
+        e->env.release();
+        delete e;
+        return st;
+    }
+    *out = e;
+    return KPAX_OK;
+}
+
+kpax_status kpax_env_destroy(kpax_env* e)
+{
+    if(!e) return KPAX_OK;
+    e->env.release();
+    delete e;
+    return KPAX_OK;
+}
+
+kpax_status kpax_env_stats(kpax_env* e, uint32_t* n_cells, uint32_t* n_entries)
+{
+    if(!e) return set_error("kpax_env_stats: null env"), KPAX_EINVAL;
+    if(n_cells) *n_cells = e->env.n_cells;
+    if(n_entries) *n_entries = e->env.n_ent;
+    return KPAX_OK;
+}
+
+kpax_status kpax_propagate_batch(const kpax_config* cfg, kpax_env* env, const float* d_parents, const float* d_draws,
+                                 uint32_t draw_stream, uint32_t n, float* d_rows, uint8_t* d_valid, int32_t* d_steps,
+                                 void* stream)
+{
+    if(!cfg || !env || (n && (!d_parents || !d_rows || !d_valid)))
+        return set_error("kpax_propagate_batch: null argument"), KPAX_EINVAL;
+    KParams p;
+    kpax_status st = derive_params(*cfg, &p);
+    if(st != KPAX_OK) return st;
+    if(p.gdim != env->env.dim || p.cell != env->env.cell || p.wmin != env->env.wmin)
+        return set_error("kpax_propagate_batch: env was built for another workspace grid"), KPAX_EINVAL;
+    return launch_propagate(p, env->env.view(), d_parents, d_draws, draw_stream, n, d_rows, d_valid, d_steps,
+                            (cudaStream_t)stream);
+}
+
+kpax_status kpax_collide_batch(kpax_env* env, const float* d_bbmin, const float* d_bbmax, uint32_t n, uint8_t* d_free,
+                               void* stream)
+{
+    if(!env || (n && (!d_bbmin || !d_bbmax || !d_free))) return set_error("kpax_collide_batch: null argument"), KPAX_EINVAL;
+    if(!n) return KPAX_OK;
+    k_collide_batch<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(env->env.view(), d_bbmin, d_bbmax, n, d_free);
+    KPAX_CHECK_LAUNCH();
+    count_launch();
+    return KPAX_OK;
+}
+
+kpax_status kpax_region_batch(const kpax_config* cfg, const float* d_states, uint32_t n, int32_t* d_r1, int32_t* d_r2,
+                              void* stream)
+{
+    if(!cfg || (n && (!d_states || !d_r1))) return set_error("kpax_region_batch: null argument"), KPAX_EINVAL;
+    KParams p;
+    kpax_status st = derive_params(*cfg, &p);
+    if(st != KPAX_OK) return st;
+    if(!n) return KPAX_OK;
+    k_region_batch<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(p, d_states, n, d_r1, d_r2);
+    KPAX_CHECK_LAUNCH();
+    count_launch();
+    return KPAX_OK;
+}
+
+}  // extern "C"

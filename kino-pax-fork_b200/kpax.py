@@ -1,0 +1,354 @@
+"""ctypes binding of libkpax.so (the C ABI declared in include/kpax.h).
+
+The Python mirror of the reference planner: ``KPAX(config).plan(h_initial, h_goal,
+d_obstacles_ptr, h_obstaclesCount, saveTree)`` (src/planners/KPAX.cu:51) with the reference's
+public result fields (``h_pathToGoal_``, ``h_itr_``, ``h_treeSize_``,
+``h_controlPathToGoal_``; include/planners/Planner.cuh:31-43).  Device buffers are passed as
+integer pointers (e.g. ``torch.Tensor.data_ptr()``).  There is no CPU fallback: loading fails
+loudly when the library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libkpax.so"
+
+OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, ECAPACITY, ENOTFOUND = range(7)
+MODEL_DOUBLE_INTEGRATOR, MODEL_DUBINS_AIRPLANE, MODEL_QUADROTOR = 1, 2, 3
+PRESET_DI, PRESET_DUBINS, PRESET_QUAD, PRESET_QUAD_REF = 0, 1, 2, 3
+
+
+class KpaxError(RuntimeError):
+    def __init__(self, status: int, where: str, msg: str):
+        super().__init__(f"{where}: status {status}: {msg}")
+        self.status = status
+
+
+class Config(ctypes.Structure):
+    _fields_ = [
+        ("model", ctypes.c_int32),
+        ("state_dim", ctypes.c_int32),
+        ("control_dim", ctypes.c_int32),
+        ("max_tree_size", ctypes.c_uint32),
+        ("max_iter", ctypes.c_uint32),
+        ("step_size", ctypes.c_float),
+        ("max_propagation_duration", ctypes.c_int32),
+        ("fixed_steps", ctypes.c_int32),
+        ("goal_thresh", ctypes.c_float),
+        ("w_min", ctypes.c_float),
+        ("w_max", ctypes.c_float),
+        ("w_size", ctypes.c_float),
+        ("c_min", ctypes.c_double),
+        ("c_max", ctypes.c_double),
+        ("v_min", ctypes.c_float),
+        ("v_max", ctypes.c_float),
+        ("ctrl_min", ctypes.c_float * 4),
+        ("ctrl_max", ctypes.c_float * 4),
+        ("pitch_min", ctypes.c_double),
+        ("pitch_max", ctypes.c_double),
+        ("c_dim", ctypes.c_int32),
+        ("v_dim", ctypes.c_int32),
+        ("w_r1_length", ctypes.c_int32),
+        ("c_r1_length", ctypes.c_int32),
+        ("v_r1_length", ctypes.c_int32),
+        ("w_r2_length", ctypes.c_int32),
+        ("c_r2_length", ctypes.c_int32),
+        ("v_r2_length", ctypes.c_int32),
+        ("region_compat", ctypes.c_int32),
+        ("epsilon", ctypes.c_float),
+        ("hash_cell_size", ctypes.c_float),
+        ("expansions_per_iter", ctypes.c_uint32),
+        ("children_per_entry", ctypes.c_uint32),
+        ("root_repeat", ctypes.c_uint32),
+        ("sparse_repeat", ctypes.c_uint32),
+        ("sparse_valid_threshold", ctypes.c_int32),
+        ("seed", ctypes.c_uint64),
+        ("block_size", ctypes.c_int32),
+        ("unroll_iters", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 8),
+    ]
+
+    @property
+    def sample_dim(self) -> int:
+        return self.state_dim + self.control_dim + 1
+
+    def copy(self) -> "Config":
+        c = Config()
+        ctypes.pointer(c)[0] = self
+        return c
+
+
+class Result(ctypes.Structure):
+    _fields_ = [
+        ("found", ctypes.c_int32),
+        ("goal_idx", ctypes.c_uint32),
+        ("path_len", ctypes.c_uint32),
+        ("tree_size", ctypes.c_uint32),
+        ("iters", ctypes.c_uint32),
+        ("tree_full", ctypes.c_int32),
+        ("h_path", ctypes.POINTER(ctypes.c_float)),
+        ("ms", ctypes.c_double),
+        ("expansions", ctypes.c_uint64),
+        ("valid_expansions", ctypes.c_uint64),
+        ("path_cost", ctypes.c_double),
+    ]
+
+
+class IterTiming(ctypes.Structure):
+    _fields_ = [("ms_total", ctypes.c_float), ("ms_frontier", ctypes.c_float), ("ms_expand", ctypes.c_float),
+                ("ms_scores", ctypes.c_float)]
+
+
+_VP, _U32, _I32, _F = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int32, ctypes.POINTER(ctypes.c_float)
+_SIGNATURES = {
+    "kpax_config_preset": (_I32, [_I32, ctypes.POINTER(Config)]),
+    "kpax_config_validate": (_I32, [ctypes.POINTER(Config)]),
+    "kpax_config_sizes": (_I32, [ctypes.POINTER(Config), _VP, _VP, _VP]),
+    "kpax_last_error": (ctypes.c_char_p, []),
+    "kpax_abi_version": (_I32, []),
+    "kpax_create": (_I32, [ctypes.POINTER(Config), ctypes.POINTER(_VP)]),
+    "kpax_destroy": (_I32, [_VP]),
+    "kpax_plan": (_I32, [_VP, _VP, _VP, _VP, _U32, _I32, ctypes.POINTER(Result)]),
+    "kpax_plan_host": (_I32, [_VP, _VP, _VP, _VP, _U32, ctypes.POINTER(Result)]),
+    "kpax_plan_begin": (_I32, [_VP, _VP, _VP, _VP, _U32]),
+    "kpax_plan_iterate": (_I32, [_VP, _U32, _I32]),
+    "kpax_plan_result": (_I32, [_VP, ctypes.POINTER(Result)]),
+    "kpax_plan_iterate_timed": (_I32, [_VP, _U32, ctypes.c_uint64, _VP, _VP]),
+    "kpax_planner_stream": (_VP, [_VP]),
+    "kpax_export_tree": (_I32, [_VP, _VP, _VP, _VP, _U32, _VP]),
+    "kpax_export_regions": (_I32, [_VP, _VP, _VP, _VP, _VP]),
+    "kpax_export_frontier": (_I32, [_VP, _VP, _VP, _U32]),
+    "kpax_debug_capture": (_I32, [_VP, _I32]),
+    "kpax_export_children": (_I32, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _U32, _VP]),
+    "kpax_env_create": (_I32, [ctypes.POINTER(Config), _VP, _U32, _VP, ctypes.POINTER(_VP)]),
+    "kpax_env_destroy": (_I32, [_VP]),
+    "kpax_env_stats": (_I32, [_VP, _VP, _VP]),
+    "kpax_propagate_batch": (_I32, [ctypes.POINTER(Config), _VP, _VP, _VP, _U32, _U32, _VP, _VP, _VP, _VP]),
+    "kpax_collide_batch": (_I32, [_VP, _VP, _VP, _U32, _VP, _VP]),
+    "kpax_region_batch": (_I32, [ctypes.POINTER(Config), _VP, _U32, _VP, _VP, _VP]),
+    "kpax_kernel_launches": (ctypes.c_uint64, []),
+}
+
+_lib = None
+
+
+def load(path: os.PathLike | None = None) -> ctypes.CDLL:
+    """Load libkpax.so (built by `make -C kino-pax-fork_b200`); raises if it is missing."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise ImportError(f"{p} is missing: build it with `make -C {HERE}` (no CPU fallback exists)")
+    lib = ctypes.CDLL(str(p))
+    for name, (res, args) in _SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype, fn.argtypes = res, args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def exported_symbols() -> list[str]:
+    return sorted(_SIGNATURES)
+
+
+def check(status: int, where: str) -> None:
+    if status != OK:
+        raise KpaxError(status, where, load().kpax_last_error().decode(errors="replace"))
+
+
+def preset(which: int) -> Config:
+    c = Config()
+    check(load().kpax_config_preset(which, ctypes.byref(c)), "kpax_config_preset")
+    return c
+
+
+def sizes(cfg: Config) -> tuple[int, int, int]:
+    a, b, s = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+    check(load().kpax_config_sizes(ctypes.byref(cfg), ctypes.byref(a), ctypes.byref(b), ctypes.byref(s)), "kpax_config_sizes")
+    return a.value, b.value, s.value
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+class Env:
+    """Spatial-hash grid over a device obstacle buffer (n x 6 floats)."""
+
+    def __init__(self, cfg: Config, d_obstacles: int, n_obs: int, stream: int = 0):
+        self._h = _VP()
+        check(load().kpax_env_create(ctypes.byref(cfg), d_obstacles, n_obs, stream, ctypes.byref(self._h)), "kpax_env_create")
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    def stats(self) -> tuple[int, int]:
+        a, b = ctypes.c_uint32(), ctypes.c_uint32()
+        check(load().kpax_env_stats(self._h, ctypes.byref(a), ctypes.byref(b)), "kpax_env_stats")
+        return a.value, b.value
+
+    def close(self) -> None:
+        if self._h:
+            load().kpax_env_destroy(self._h)
+            self._h = _VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def propagate_batch(cfg: Config, env: Env, d_parents: int, d_draws: int | None, draw_stream: int, n: int, d_rows: int,
+                    d_valid: int, d_steps: int | None = None, stream: int = 0) -> None:
+    check(load().kpax_propagate_batch(ctypes.byref(cfg), env.handle, d_parents, d_draws or None, draw_stream, n, d_rows,
+                                      d_valid, d_steps or None, stream), "kpax_propagate_batch")
+
+
+def collide_batch(env: Env, d_bbmin: int, d_bbmax: int, n: int, d_free: int, stream: int = 0) -> None:
+    check(load().kpax_collide_batch(env.handle, d_bbmin, d_bbmax, n, d_free, stream), "kpax_collide_batch")
+
+
+def region_batch(cfg: Config, d_states: int, n: int, d_r1: int, d_r2: int | None, stream: int = 0) -> None:
+    check(load().kpax_region_batch(ctypes.byref(cfg), d_states, n, d_r1, d_r2 or None, stream), "kpax_region_batch")
+
+
+def kernel_launches() -> int:
+    return int(load().kpax_kernel_launches())
+
+
+class KPAX:
+    """Planner handle with the reference's plan() entry and public result fields."""
+
+    def __init__(self, cfg: Config):
+        self.cfg = cfg.copy()
+        self.num_r1, self.r2_per_r1, self.sample_dim = sizes(self.cfg)
+        self._h = _VP()
+        check(load().kpax_create(ctypes.byref(self.cfg), ctypes.byref(self._h)), "kpax_create")
+        self.result = Result()
+        self.h_pathToGoal_ = 0
+        self.h_itr_ = 0
+        self.h_treeSize_ = 0
+        self.h_controlPathToGoal_ = np.zeros((0, self.sample_dim), np.float32)
+
+    @property
+    def stream(self) -> int:
+        return load().kpax_planner_stream(self._h) or 0
+
+    def _publish(self) -> Result:
+        r = self.result
+        self.h_pathToGoal_ = int(r.goal_idx)
+        self.h_itr_ = int(r.iters)
+        self.h_treeSize_ = int(r.tree_size)
+        if r.path_len:
+            flat = np.ctypeslib.as_array(r.h_path, shape=(r.path_len * self.sample_dim,))
+            self.h_controlPathToGoal_ = flat.reshape(r.path_len, self.sample_dim).copy()
+        else:
+            self.h_controlPathToGoal_ = np.zeros((0, self.sample_dim), np.float32)
+        return r
+
+    @staticmethod
+    def _row(x, S: int) -> np.ndarray:
+        a = np.zeros(S, np.float32)
+        x = np.asarray(x, np.float32).ravel()
+        a[: min(S, x.size)] = x[:S]
+        return a
+
+    def plan(self, h_initial, h_goal, d_obstacles_ptr: int, h_obstaclesCount: int, saveTree: bool = False) -> Result:
+        S = self.sample_dim
+        init, goal = self._row(h_initial, S), self._row(h_goal, S)
+        check(load().kpax_plan(self._h, _ptr(init), _ptr(goal), d_obstacles_ptr, h_obstaclesCount, int(saveTree),
+                               ctypes.byref(self.result)), "kpax_plan")
+        return self._publish()
+
+    def plan_host(self, h_initial, h_goal, obstacles: np.ndarray) -> Result:
+        S = self.sample_dim
+        init, goal = self._row(h_initial, S), self._row(h_goal, S)
+        obs = np.ascontiguousarray(obstacles, np.float32).reshape(-1, 6)
+        check(load().kpax_plan_host(self._h, _ptr(init), _ptr(goal), _ptr(obs), obs.shape[0], ctypes.byref(self.result)),
+              "kpax_plan_host")
+        return self._publish()
+
+    def begin(self, h_initial, h_goal, d_obstacles_ptr: int, n_obs: int) -> None:
+        S = self.sample_dim
+        init, goal = self._row(h_initial, S), self._row(h_goal, S)
+        check(load().kpax_plan_begin(self._h, _ptr(init), _ptr(goal), d_obstacles_ptr, n_obs), "kpax_plan_begin")
+
+    def iterate(self, n_iters: int, stop_at_goal: bool = False) -> None:
+        check(load().kpax_plan_iterate(self._h, n_iters, int(stop_at_goal)), "kpax_plan_iterate")
+
+    def iterate_timed(self, n_iters: int, flush_bytes: int = 0):
+        """Per-iteration kernel times (ms: total, frontier, expand, scores) and the totals
+        (children, valid children, RK4 steps, appended nodes) over the n_iters."""
+        times = (IterTiming * max(n_iters, 1))()
+        totals = np.zeros(4, np.uint64)
+        check(load().kpax_plan_iterate_timed(self._h, n_iters, flush_bytes, ctypes.addressof(times), _ptr(totals)),
+              "kpax_plan_iterate_timed")
+        t = np.array([[x.ms_total, x.ms_frontier, x.ms_expand, x.ms_scores] for x in times[:n_iters]], np.float64)
+        return t, {"children": int(totals[0]), "valid": int(totals[1]), "steps": int(totals[2]), "appended": int(totals[3])}
+
+    def finish(self) -> Result:
+        check(load().kpax_plan_result(self._h, ctypes.byref(self.result)), "kpax_plan_result")
+        return self._publish()
+
+    def export_tree(self, max_rows: int | None = None):
+        n_max = max_rows or self.cfg.max_tree_size
+        rows = np.zeros((n_max, self.sample_dim), np.float32)
+        parents = np.zeros(n_max, np.int32)
+        costs = np.zeros(n_max, np.float32)
+        n = ctypes.c_uint32()
+        check(load().kpax_export_tree(self._h, _ptr(rows), _ptr(parents), _ptr(costs), n_max, ctypes.byref(n)),
+              "kpax_export_tree")
+        k = n.value
+        return rows[:k], parents[:k], costs[:k]
+
+    def export_regions(self):
+        words = (self.num_r1 * self.r2_per_r1 + 31) // 32
+        counter = np.zeros(self.num_r1, np.int32)
+        valid = np.zeros(self.num_r1, np.int32)
+        scores = np.zeros(self.num_r1, np.float32)
+        bits = np.zeros(words, np.uint32)
+        check(load().kpax_export_regions(self._h, _ptr(counter), _ptr(valid), _ptr(scores), _ptr(bits)), "kpax_export_regions")
+        return counter, valid, scores, bits
+
+    def export_frontier(self, n: int):
+        rep = np.zeros(n, np.uint8)
+        r1 = np.zeros(n, np.int32)
+        check(load().kpax_export_frontier(self._h, _ptr(rep), _ptr(r1), n), "kpax_export_frontier")
+        return rep, r1
+
+    def debug_capture(self, on: bool = True) -> None:
+        check(load().kpax_debug_capture(self._h, int(on)), "kpax_debug_capture")
+
+    def export_children(self):
+        n_max = self.cfg.expansions_per_iter
+        rows = np.zeros((n_max, self.sample_dim), np.float32)
+        valid = np.zeros(n_max, np.uint8)
+        r1 = np.zeros(n_max, np.int32)
+        r2 = np.zeros(n_max, np.int32)
+        nxt = np.zeros(n_max, np.uint8)
+        par = np.zeros(n_max, np.int32)
+        n = ctypes.c_uint32()
+        check(load().kpax_export_children(self._h, _ptr(rows), _ptr(valid), _ptr(r1), _ptr(r2), _ptr(nxt), _ptr(par), n_max,
+                                          ctypes.byref(n)), "kpax_export_children")
+        k = n.value
+        return rows[:k], valid[:k], r1[:k], r2[:k], nxt[:k], par[:k]
+
+    def close(self) -> None:
+        if self._h:
+            load().kpax_destroy(self._h)
+            self._h = _VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,151 @@
+"""Seeded synthetic environments, start states and the obstacle CSV format.
+
+Obstacles are rows [min x, min y, min z, max x, max y, max z] (float32), the layout the
+reference reads from include/config/obstacles/*/obstacles.csv (src/helper/helper.cu:13-39).
+All generators use numpy's PCG64 with an explicit seed, so every run sees the same scene.
+"""
+from __future__ import annotations
+
+import math
+from pathlib import Path
+
+import numpy as np
+
+W_MIN, W_MAX = 0.0, 100.0
+
+
+def read_obstacles_csv(path: str | Path) -> np.ndarray:
+    """Comma-separated floats, 6 per obstacle (readObstaclesFromCSV, helper.cu:13-39)."""
+    vals: list[float] = []
+    for line in Path(path).read_text().splitlines():
+        vals.extend(float(t) for t in line.replace(",", " ").split())
+    n = len(vals) // 6
+    return np.asarray(vals[: 6 * n], np.float32).reshape(n, 6)
+
+
+def write_obstacles_csv(path: str | Path, obs: np.ndarray) -> None:
+    with open(path, "w") as f:
+        for row in np.asarray(obs, np.float32).reshape(-1, 6):
+            f.write(",".join(f"{v:.6f}" for v in row) + "\n")
+
+
+def _covers(box: np.ndarray, p: np.ndarray) -> bool:
+    p = np.asarray(p, np.float32)[:3]
+    return bool(np.all(box[:3] <= p) and np.all(p <= box[3:]))
+
+
+def random_boxes(n: int, seed: int, side=(5.0, 15.0), avoid=(), rng: np.random.Generator | None = None) -> np.ndarray:
+    """n axis-aligned boxes: centres U[0,100]^3, sides U[side]; boxes covering a point of
+    `avoid` are redrawn."""
+    rng = rng or np.random.default_rng(seed)
+    avoid = [np.asarray(a, np.float32)[:3] for a in avoid]
+    out = []
+    while len(out) < n:
+        c = rng.uniform(W_MIN, W_MAX, 3)
+        s = rng.uniform(side[0], side[1], 3)
+        b = np.concatenate([c - s / 2, c + s / 2]).astype(np.float32)
+        if any(_covers(b, a) for a in avoid):
+            continue
+        out.append(b)
+    return np.asarray(out, np.float32).reshape(-1, 6)
+
+
+def di_scene(seed: int = 0):
+    """Double-integrator benchmark: 20 boxes (sides U[5,15]) avoiding start (5,5,5) and the goal
+    centre (95,95,95); goal ball radius 5."""
+    start = np.array([5, 5, 5, 0, 0, 0], np.float32)
+    goal = np.array([95, 95, 95, 0, 0, 0], np.float32)
+    return random_boxes(20, seed, avoid=(start, goal)), start, goal
+
+
+def forest(n: int = 200, seed: int = 1) -> np.ndarray:
+    """Vertical columns from z = 0: xy footprint sides U[2,6], height U[20,100], centres U[0,100]^2."""
+    rng = np.random.default_rng(seed)
+    xy = rng.uniform(W_MIN, W_MAX, (n, 2))
+    fp = rng.uniform(2.0, 6.0, (n, 2))
+    h = rng.uniform(20.0, 100.0, n)
+    lo = np.column_stack([xy - fp / 2, np.zeros(n)])
+    hi = np.column_stack([xy + fp / 2, h])
+    return np.concatenate([lo, hi], axis=1).astype(np.float32)
+
+
+def dubins_scene(seed: int = 1):
+    start = np.array([5, 5, 50, 0.7853982, 0, 1.0], np.float32)
+    goal = np.array([95, 95, 50, 0, 0, 0], np.float32)
+    obs = forest(200, seed)
+    keep = [b for b in obs if not (_covers(b, start) or _covers(b, goal))]
+    return np.asarray(keep, np.float32).reshape(-1, 6), start, goal
+
+
+WALL_X, WALL_T, WINDOW = 50.0, 1.0, 6.0
+WINDOW_CENTRES = ((25.0, 25.0), (75.0, 25.0), (25.0, 75.0), (75.0, 75.0))
+
+
+def wall_with_windows() -> np.ndarray:
+    """A 1 m thick wall at x = 50 spanning y, z in [0,100] with four 6x6 windows, as boxes."""
+    x0, x1 = WALL_X - WALL_T / 2, WALL_X + WALL_T / 2
+    zs = sorted({0.0, 100.0, *(c[1] - WINDOW / 2 for c in WINDOW_CENTRES), *(c[1] + WINDOW / 2 for c in WINDOW_CENTRES)})
+    ys = sorted({0.0, 100.0, *(c[0] - WINDOW / 2 for c in WINDOW_CENTRES), *(c[0] + WINDOW / 2 for c in WINDOW_CENTRES)})
+    boxes = []
+    for za, zb in zip(zs[:-1], zs[1:]):
+        zm = (za + zb) / 2
+        in_band = any(abs(zm - c[1]) < WINDOW / 2 for c in WINDOW_CENTRES)
+        if not in_band:
+            boxes.append([x0, 0.0, za, x1, 100.0, zb])
+            continue
+        for ya, yb in zip(ys[:-1], ys[1:]):
+            ym = (ya + yb) / 2
+            if any(abs(ym - c[0]) < WINDOW / 2 and abs(zm - c[1]) < WINDOW / 2 for c in WINDOW_CENTRES):
+                continue
+            boxes.append([x0, ya, za, x1, yb, zb])
+    return np.asarray(boxes, np.float32)
+
+
+def building(n_total: int = 1000, seed: int = 2, start=(10.0, 8.0, 5.0), goal=(80.0, 95.0, 90.0)) -> np.ndarray:
+    """`n_total` boxes: the windowed wall plus random boxes (sides U[5,15]) that leave the start,
+    the goal and the window openings (extended 4 m either side of the wall) free."""
+    wall = wall_with_windows()
+    rng = np.random.default_rng(seed)
+    tunnels = [np.array([WALL_X - 4, cy - WINDOW / 2, cz - WINDOW / 2, WALL_X + 4, cy + WINDOW / 2, cz + WINDOW / 2])
+               for cy, cz in WINDOW_CENTRES]
+    out = []
+    p_s, p_g = np.asarray(start, np.float32), np.asarray(goal, np.float32)
+    while len(out) < n_total - len(wall):
+        b = random_boxes(1, 0, rng=rng)[0]
+        if _covers(b, p_s) or _covers(b, p_g):
+            continue
+        if any(np.all(b[:3] < t[3:]) and np.all(t[:3] < b[3:]) for t in tunnels):
+            continue
+        out.append(b)
+    return np.concatenate([wall, np.asarray(out, np.float32)]).astype(np.float32)
+
+
+def quad_scene(seed: int = 2, n_total: int = 1000):
+    start = np.array([10, 8, 5] + [0] * 9, np.float32)
+    goal = np.array([80, 95, 90] + [0] * 9, np.float32)
+    return building(n_total, seed, start[:3], goal[:3]), start, goal
+
+
+def sample_states(model: int, n: int, seed: int, vmin: float = -1.0, vmax: float = 1.0) -> np.ndarray:
+    """Parent states uniform within the model's bounds (positions in [0,100]^3)."""
+    rng = np.random.default_rng(seed)
+    pos = rng.uniform(W_MIN, W_MAX, (n, 3))
+    if model == 1:
+        vel = rng.uniform(vmin, vmax, (n, 3))
+        return np.column_stack([pos, vel]).astype(np.float32)
+    if model == 2:
+        yaw = rng.uniform(-math.pi, math.pi, n)
+        pitch = rng.uniform(-math.pi / 3, math.pi / 3, n)
+        v = rng.uniform(max(vmin, 0.5), vmax, n)
+        return np.column_stack([pos, yaw, pitch, v]).astype(np.float32)
+    ang = rng.uniform(-0.5, 0.5, (n, 3))
+    vel = rng.uniform(-5.0, 5.0, (n, 3))
+    rates = rng.uniform(-0.5, 0.5, (n, 3))
+    return np.column_stack([pos, ang, vel, rates]).astype(np.float32)
+
+
+def uniform_draws(n: int, seed: int) -> np.ndarray:
+    """n x 6 uniforms in (0, 1] on the 2^-24 grid the device generator uses."""
+    rng = np.random.default_rng(seed)
+    k = rng.integers(1, 1 << 24, (n, 6), endpoint=True)
+    return (k.astype(np.float64) * 2.0 ** -24).astype(np.float32)

@@ -1,0 +1,93 @@
+"""The C ABI library loads without a GPU, exports every symbol include/kpax.h declares, and its
+pure-host calls (presets, validation, sizes) behave as documented.  No device calls here."""
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import kpax
+import oracle as O
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_functions() -> set[str]:
+    text = (ROOT / "include" / "kpax.h").read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return set(re.findall(r"\b(kpax_[a-z0-9_]+)\s*\(", text))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = kpax.load()
+    names = declared_functions()
+    assert len(names) >= 25
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+    # the Python binding types every declared entry point
+    assert names <= set(kpax.exported_symbols())
+
+
+def test_abi_version():
+    assert kpax.load().kpax_abi_version() == 1
+
+
+@pytest.mark.parametrize("which", [kpax.PRESET_DI, kpax.PRESET_DUBINS, kpax.PRESET_QUAD, kpax.PRESET_QUAD_REF])
+def test_presets_validate_and_size(which):
+    cfg = kpax.preset(which)
+    assert kpax.load().kpax_config_validate(ctypes.byref(cfg)) == kpax.OK
+    n1, P, S = kpax.sizes(cfg)
+    assert (n1, P, S) == O.sizes(cfg)
+    assert S == cfg.state_dim + cfg.control_dim + 1
+
+
+def test_preset_values_follow_benchmark_configs():
+    di = kpax.preset(kpax.PRESET_DI)
+    assert (di.step_size, di.max_propagation_duration, di.fixed_steps) == (np.float32(0.1), 10, 0)
+    assert kpax.sizes(di)[:2] == (512, 8)
+    assert di.expansions_per_iter == 1 << 14 and di.max_tree_size == 1 << 20
+    q = kpax.preset(kpax.PRESET_QUAD)
+    assert (q.step_size, q.max_propagation_duration, q.fixed_steps) == (np.float32(0.02), 25, 1)
+    assert q.ctrl_max[0] == np.float32(19.62) and q.ctrl_min[1] == np.float32(-0.1)
+    assert kpax.sizes(q)[:2] == (32768, 64)
+    assert q.expansions_per_iter == 1 << 16
+    d = kpax.preset(kpax.PRESET_DUBINS)
+    assert (d.v_min, d.v_max) == (0.5, 2.0) and d.max_propagation_duration == 20
+
+
+@pytest.mark.parametrize(
+    "field,value",
+    [("model", 7), ("state_dim", 5), ("max_tree_size", 1), ("step_size", 0.0), ("w_max", -1.0), ("c_r1_length", 40),
+     ("hash_cell_size", 0.0), ("children_per_entry", 0), ("expansions_per_iter", 0), ("c_dim", 9), ("block_size", 33)],
+)
+def test_invalid_configs_are_rejected_with_a_message(field, value):
+    cfg = kpax.preset(kpax.PRESET_QUAD)
+    setattr(cfg, field, value)
+    lib = kpax.load()
+    assert lib.kpax_config_validate(ctypes.byref(cfg)) == kpax.EINVAL
+    assert lib.kpax_last_error()
+    with pytest.raises(kpax.KpaxError):
+        kpax.sizes(cfg)
+
+
+def test_unknown_preset():
+    with pytest.raises(kpax.KpaxError):
+        kpax.preset(99)
+
+
+def test_cpp_wrapper_header_compiles():
+    """include/kpax.hpp (the C++ mirror of the reference KPAX class) compiles against the ABI."""
+    import shutil
+    import subprocess
+    import tempfile
+
+    gxx = shutil.which("g++")
+    if not gxx:
+        pytest.skip("no g++")
+    src = '#include "kpax.hpp"\nint main(){ kpax_config c; return kpax_config_preset(KPAX_PRESET_QUAD, &c) == KPAX_OK ? 0 : 1; }\n'
+    with tempfile.TemporaryDirectory() as d:
+        p = Path(d) / "t.cpp"
+        p.write_text(src)
+        r = subprocess.run([gxx, "-std=c++17", "-fsyntax-only", f"-I{ROOT / 'include'}", str(p)], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr

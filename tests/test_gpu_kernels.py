@@ -1,0 +1,186 @@
+"""Parity of the sm_100a kernels with the reference (golden vectors) and the CPU oracle.
+
+Bars: double-integrator segments, control draws, step counts, region ids, collision verdicts and
+the obstacle grid are bit-exact.  Dubins and quadrotor states use the accurate device trig with
+fused multiply-adds and must match the reference's FP32 RK4 within REL_TOL relative error
+(|gpu - ref| <= REL_TOL * max(|ref|, 1)).  A segment whose validity differs is accepted only when
+its smallest check margin (oracle) is below NEAR_TOL, and is listed."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import kpax
+import kpax_envs as E
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+PRESETS = {"di": kpax.PRESET_DI, "dubins": kpax.PRESET_DUBINS, "quad": kpax.PRESET_QUAD}
+SCENES = {"di": E.di_scene, "dubins": E.dubins_scene, "quad": E.quad_scene}
+REL_TOL = 1e-5
+NEAR_TOL = 1e-4
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+def dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def gpu_propagate(torch, cfg, obs, parents, draws=None, stream_id=0):
+    n = parents.shape[0]
+    S = cfg.state_dim + cfg.control_dim + 1
+    d_obs = dev(torch, obs.astype(np.float32))
+    env = kpax.Env(cfg, d_obs.data_ptr(), obs.shape[0])
+    d_par = dev(torch, parents.astype(np.float32))
+    d_draw = dev(torch, np.ascontiguousarray(draws[:, :5], np.float32)) if draws is not None else None
+    rows = torch.zeros((n, S), dtype=torch.float32, device="cuda")
+    valid = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    steps = torch.zeros(n, dtype=torch.int32, device="cuda")
+    kpax.propagate_batch(cfg, env, d_par.data_ptr(), d_draw.data_ptr() if d_draw is not None else None, stream_id, n,
+                         rows.data_ptr(), valid.data_ptr(), steps.data_ptr())
+    torch.cuda.synchronize()
+    return rows.cpu().numpy(), valid.cpu().numpy(), steps.cpu().numpy(), env
+
+
+def compare_segments(cfg, rows, valid, ref_rows, ref_valid, margin, label):
+    """Returns the list of accepted near-boundary disagreements."""
+    sd, cd = cfg.state_dim, cfg.control_dim
+    # controls and duration come from the draws: bit-exact for every model
+    assert np.array_equal(bits(rows[:, sd:]), bits(ref_rows[:, sd:])), f"{label}: control/duration columns differ"
+    flips = np.where(valid != ref_valid)[0]
+    near = [int(i) for i in flips if margin[i] < NEAR_TOL]
+    assert len(near) == len(flips), f"{label}: verdict differs on segments with margin >= {NEAR_TOL}: " \
+                                    f"{[(int(i), float(margin[i])) for i in flips if margin[i] >= NEAR_TOL][:5]}"
+    same = np.setdiff1d(np.arange(rows.shape[0]), flips)
+    a, b = rows[same, :sd].astype(np.float64), ref_rows[same, :sd].astype(np.float64)
+    # segments that stopped on a check compare their last state only when both stopped at the same step;
+    # a near-boundary margin can move the stop by one step without changing the verdict
+    err = np.abs(a - b) / np.maximum(np.abs(b), 1.0)
+    row_err = err.max(axis=1)
+    bad = np.where((row_err > REL_TOL) & (margin[same] >= NEAR_TOL))[0]
+    assert bad.size == 0, f"{label}: {bad.size} rows beyond {REL_TOL}: worst {row_err.max():.3g}"
+    return near, float(row_err.max()) if row_err.size else 0.0
+
+
+@pytest.mark.parametrize("name", list(PRESETS))
+def test_propagate_matches_reference_golden(cuda, name):
+    import torch
+
+    g = np.load(GOLDEN / f"{name}.npz")
+    cfg = kpax.preset(PRESETS[name])
+    rows, valid, steps, env = gpu_propagate(torch, cfg, g["obstacles"], g["parents"], g["draws"])
+    orow, oval, ostep, margin, nonfinite, kind = O.propagate(cfg, g["obstacles"], g["parents"], g["draws"])
+    assert np.array_equal(bits(orow), bits(g["rows"]))  # oracle pinned to the reference
+    if cfg.model == kpax.MODEL_DOUBLE_INTEGRATOR:
+        assert np.array_equal(bits(rows), bits(g["rows"]))
+        assert np.array_equal(valid, g["valid"])
+        assert np.array_equal(steps, ostep)
+    else:
+        near, worst = compare_segments(cfg, rows, valid, g["rows"], g["valid"], margin, name)
+        print(f"{name}: worst relative state error {worst:.3g}; near-boundary verdict flips {near}")
+
+
+@pytest.mark.parametrize("name", list(PRESETS))
+def test_propagate_philox_draws_match_oracle(cuda, name):
+    import torch
+
+    cfg = kpax.preset(PRESETS[name])
+    obs, _, _ = SCENES[name]()
+    n = 8192
+    par = E.sample_states(cfg.model, n, 77, cfg.v_min, cfg.v_max)
+    rows, valid, steps, env = gpu_propagate(torch, cfg, obs, par, None, stream_id=5)
+    orow, oval, ostep, margin, nonfinite, kind = O.propagate(cfg, obs, par, None, stream=5, nthreads=8)
+    if cfg.model == kpax.MODEL_DOUBLE_INTEGRATOR:
+        assert np.array_equal(bits(rows), bits(orow)) and np.array_equal(valid, oval) and np.array_equal(steps, ostep)
+    else:
+        near, worst = compare_segments(cfg, rows, valid, orow, oval, margin, name)
+        print(f"{name}: worst relative state error {worst:.3g}; near-boundary flips {len(near)} of {n}")
+        assert len(near) <= n // 1000
+
+
+@pytest.mark.parametrize("name", list(PRESETS))
+@pytest.mark.parametrize("compat", [1, 0])
+def test_regions_bit_exact(cuda, name, compat):
+    import torch
+
+    cfg = kpax.preset(PRESETS[name])
+    cfg.region_compat = compat
+    rng = np.random.default_rng(3 + compat)
+    n = 20000
+    s = E.sample_states(cfg.model, n, 8, cfg.v_min, cfg.v_max)
+    s[: n // 4] = rng.uniform(-150, 250, (n // 4, cfg.state_dim)).astype(np.float32)
+    edge = np.array([0.0, 100.0, 12.5, 25.0, -0.0, 1e30, -1e30, np.inf, -np.inf, np.nan, np.pi, -np.pi,
+                     np.float32(np.pi) * 0.25, 30.0, -30.0, 0.5, 2.0], np.float32)
+    k = n // 4
+    s[k: k + 4000] = rng.choice(edge, size=(4000, cfg.state_dim))
+    d_s = dev(torch, s)
+    r1 = torch.zeros(n, dtype=torch.int32, device="cuda")
+    r2 = torch.zeros(n, dtype=torch.int32, device="cuda")
+    kpax.region_batch(cfg, d_s.data_ptr(), n, r1.data_ptr(), r2.data_ptr())
+    torch.cuda.synchronize()
+    o1, o2 = O.regions(cfg, s)
+    g1, g2 = r1.cpu().numpy(), r2.cpu().numpy()
+    assert np.array_equal(g1, o1), np.where(g1 != o1)[0][:10]
+    assert np.array_equal(g2, o2), np.where(g2 != o2)[0][:10]
+
+
+def test_collision_bit_exact_and_grid(cuda):
+    import torch
+
+    cfg = kpax.preset(kpax.PRESET_QUAD)
+    obs, _, _ = E.quad_scene()
+    d_obs = dev(torch, obs)
+    env = kpax.Env(cfg, d_obs.data_ptr(), obs.shape[0])
+    cells, entries = env.stats()
+    off, ent = O.OEnv(cfg, obs).grid()
+    assert cells == off.size - 1 and entries == ent.size
+    rng = np.random.default_rng(11)
+    n = 50000
+    lo = rng.uniform(-5, 105, (n, 3)).astype(np.float32)
+    hi = (lo + rng.uniform(0, 4, (n, 3))).astype(np.float32)
+    lo[:500] = obs[:500, 3:]  # touching faces are free
+    hi[:500] = obs[:500, 3:] + 2.0
+    lo[500:1000] = obs[:500, :3] - 1.0
+    hi[500:1000] = obs[:500, :3]
+    free = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    kpax.collide_batch(env, dev(torch, lo).data_ptr(), dev(torch, hi).data_ptr(), n, free.data_ptr())
+    torch.cuda.synchronize()
+    want = O.OEnv(cfg, obs).collide(lo, hi)
+    assert np.array_equal(free.cpu().numpy(), want)
+    assert 0.05 < want.mean() < 0.95
+
+
+def test_empty_environment_and_zero_batch(cuda):
+    import torch
+
+    cfg = kpax.preset(kpax.PRESET_DI)
+    empty = np.zeros((0, 6), np.float32)
+    par = E.sample_states(1, 64, 1)
+    d = E.uniform_draws(64, 2)
+    rows, valid, steps, env = gpu_propagate(torch, cfg, empty, par, d)
+    orow, oval, *_ = O.propagate(cfg, empty, par, d)
+    assert np.array_equal(bits(rows), bits(orow)) and np.array_equal(valid, oval)
+    assert env.stats()[1] == 0
+    kpax.propagate_batch(cfg, env, 0, None, 0, 0, 0, 0)  # n = 0 is a no-op
+
+
+def test_invalid_arguments_are_reported(cuda):
+    import torch
+
+    cfg = kpax.preset(kpax.PRESET_DI)
+    obs = np.zeros((1, 6), np.float32)
+    d_obs = dev(torch, obs)
+    env = kpax.Env(cfg, d_obs.data_ptr(), 1)
+    with pytest.raises(kpax.KpaxError) as e:
+        kpax.propagate_batch(cfg, env, 0, None, 0, 16, 0, 0)
+    assert e.value.status == kpax.EINVAL
+    other = kpax.preset(kpax.PRESET_DI)
+    other.hash_cell_size = 2.0
+    buf = torch.zeros(16 * 10, device="cuda")
+    with pytest.raises(kpax.KpaxError):
+        kpax.propagate_batch(other, env, buf.data_ptr(), None, 0, 1, buf.data_ptr(), buf.data_ptr())
