@@ -289,7 +289,7 @@ def run_ours(args) -> None:
         if r.found:
             found += 1
             tts.append(1000 * dt)
-    e2e = {"value": e2e_v / e2e_t, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h // max(plans, 1),
+    e2e = {"value": e2e_v / e2e_t if e2e_t > 0 else None, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h // max(plans, 1),
            "plans": plans, "success_rate": found / max(plans, 1),
            "tts_ms_p50": float(np.percentile(tts, 50)) if tts else None,
            "tts_ms_p95": float(np.percentile(tts, 95)) if tts else None}

@@ -148,7 +148,8 @@ def test_collision_bit_exact_and_grid(cuda):
     lo[500:1000] = obs[:500, :3] - 1.0
     hi[500:1000] = obs[:500, :3]
     free = torch.zeros(n, dtype=torch.uint8, device="cuda")
-    kpax.collide_batch(env, dev(torch, lo).data_ptr(), dev(torch, hi).data_ptr(), n, free.data_ptr())
+    d_lo, d_hi = dev(torch, lo), dev(torch, hi)  # keep the tensors alive while the kernel runs
+    kpax.collide_batch(env, d_lo.data_ptr(), d_hi.data_ptr(), n, free.data_ptr())
     torch.cuda.synchronize()
     want = O.OEnv(cfg, obs).collide(lo, hi)
     assert np.array_equal(free.cpu().numpy(), want)
