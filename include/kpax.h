@@ -194,6 +194,24 @@ kpax_status kpax_env_stats(kpax_env* env, uint32_t* n_cells, uint32_t* n_entries
 kpax_status kpax_propagate_batch(const kpax_config* cfg, kpax_env* env, const float* d_parents,
                                  const float* d_draws, uint32_t draw_stream, uint32_t n,
                                  float* d_rows, uint8_t* d_valid, int32_t* d_steps, void* stream);
+/* Allocation-free variant of kpax_propagate_batch; it has no counterpart in the reference.
+ * For callers that must not allocate device memory while they run — a planner inside a robot's
+ * real-time control cycle, where cudaMalloc can synchronise the device and take unbounded time,
+ * or a host application that hands all device memory to its own pool at start-up.  The obstacle
+ * grid is built in a fixed array inside the library (about 2.1 MiB, held by every GPU that loads
+ * the library until exit) instead of in memory from cudaMalloc; nothing is allocated or freed.
+ * Limits: at most 4096 obstacles, 131072 grid cells and 262144 (cell, obstacle) pairs; larger
+ * inputs return KPAX_ECAPACITY with a message.  All calls share that one array and each call
+ * overwrites it, so calls whose GPU work overlaps (other streams, other host threads) race; issue
+ * them one after another on one stream.  The call synchronises `stream` once, after counting the
+ * grid entries.  The first call on a device looks up the array's device address, so make it
+ * before any stream capture.  Arguments as kpax_propagate_batch, with the obstacles (n_obs x 6
+ * device floats) in place of an environment. */
+kpax_status kpax_propagate_batch_noalloc(const kpax_config* cfg, const float* d_obstacles,
+                                         uint32_t n_obs, const float* d_parents,
+                                         const float* d_draws, uint32_t draw_stream, uint32_t n,
+                                         float* d_rows, uint8_t* d_valid, int32_t* d_steps,
+                                         void* stream);
 /* Broad-phase check of n boxes against the grid (isMotionValidSpatialHash, spatialHash.cu:145-194).
  * d_bbmin/d_bbmax: n x 3 floats.  d_free: n bytes, 1 = no obstacle overlaps the box. */
 kpax_status kpax_collide_batch(kpax_env* env, const float* d_bbmin, const float* d_bbmax,

@@ -9,6 +9,8 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <mutex>
+
 #include "kpax_internal.h"
 
 namespace kpax {
@@ -321,3 +323,93 @@ kpax_status kpax_region_batch(const kpax_config* cfg, const float* d_states, uin
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- allocation-free propagation
+// kpax_propagate_batch_noalloc builds the obstacle grid in a fixed device array instead of
+// memory from cudaMalloc, for callers that must not allocate device memory while they run: a
+// planner called from a robot's real-time control cycle (cudaMalloc can synchronise the device
+// and take unbounded time) or a host application that reserves all device memory up front for
+// its own pool.  The array below lives in every GPU that loads this library, until exit.
+namespace {
+
+constexpr uint32_t kNoAllocMaxObstacles = 4096;
+constexpr uint32_t kNoAllocMaxCells = 1u << 17;    // e.g. a 50^3 grid
+constexpr uint32_t kNoAllocMaxEntries = 1u << 18;  // (cell, obstacle) pairs
+
+struct NoAllocScratch {
+    float4 obs[2 * kNoAllocMaxObstacles];
+    uint32_t off[kNoAllocMaxCells + 1];
+    uint32_t cursor[kNoAllocMaxCells];
+    uint32_t ent[kNoAllocMaxEntries];
+};
+
+// In host code this name is only a stand-in for the device array; kernels get the address
+// from cudaGetSymbolAddress below.
+static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+NoAllocScratch* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device, looked up once per device.
+kpax_status noalloc_scratch(NoAllocScratch** out)
+{
+    int dev = 0;
+    KPAX_CUDA(cudaGetDevice(&dev));
+    if(dev < 0 || dev >= kNoAllocMaxDevices) return set_error("device ordinal %d not supported", dev), KPAX_EINVAL;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if(!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if(e != cudaSuccess || !p)
+            return set_error("cudaGetSymbolAddress(scratch) failed: %s", cudaGetErrorString(e)), KPAX_ECUDA;
+        g_noalloc_addr[dev] = (NoAllocScratch*)p;
+    }
+    *out = g_noalloc_addr[dev];
+    return KPAX_OK;
+}
+
+}  // namespace
+
+extern "C" kpax_status kpax_propagate_batch_noalloc(const kpax_config* cfg, const float* d_obstacles, uint32_t n_obs,
+                                                    const float* d_parents, const float* d_draws, uint32_t draw_stream,
+                                                    uint32_t n, float* d_rows, uint8_t* d_valid, int32_t* d_steps,
+                                                    void* stream)
+{
+    if(!cfg || (n_obs && !d_obstacles) || (n && (!d_parents || !d_rows || !d_valid)))
+        return set_error("kpax_propagate_batch_noalloc: null argument"), KPAX_EINVAL;
+    KParams p;
+    kpax_status st = derive_params(*cfg, &p);
+    if(st != KPAX_OK) return st;
+    const uint32_t cells = (uint32_t)p.gdim * p.gdim * p.gdim;
+    if(n_obs > kNoAllocMaxObstacles)
+        return set_error("kpax_propagate_batch_noalloc: %u obstacles exceed the limit of %u", n_obs, kNoAllocMaxObstacles),
+               KPAX_ECAPACITY;
+    if(cells > kNoAllocMaxCells)
+        return set_error("kpax_propagate_batch_noalloc: %u grid cells exceed the limit of %u", cells, kNoAllocMaxCells),
+               KPAX_ECAPACITY;
+    NoAllocScratch* s = nullptr;
+    if((st = noalloc_scratch(&s)) != KPAX_OK) return st;
+    cudaStream_t cs = (cudaStream_t)stream;
+    const Grid g{s->obs, s->off, s->ent, p.wmin, p.cell, p.gdim};
+    // the array keeps the previous call's grid: the counts must start from zero
+    KPAX_CUDA(cudaMemsetAsync(s->off, 0, sizeof(uint32_t) * (cells + 1), cs));
+    if(n_obs) {
+        k_env_count<<<(n_obs + 255) / 256, 256, 0, cs>>>(g, d_obstacles, n_obs, s->obs, s->off);
+        KPAX_CHECK_LAUNCH();
+        k_env_scan<<<1, 1024, 0, cs>>>(s->off, cells, s->cursor);
+        KPAX_CHECK_LAUNCH();
+        count_launch(2);
+        uint32_t total = 0;
+        KPAX_CUDA(cudaMemcpyAsync(&total, s->off + cells, sizeof(uint32_t), cudaMemcpyDeviceToHost, cs));
+        KPAX_CUDA(cudaStreamSynchronize(cs));
+        if(total > kNoAllocMaxEntries)
+            return set_error("kpax_propagate_batch_noalloc: %u (cell, obstacle) pairs exceed the limit of %u", total,
+                             kNoAllocMaxEntries),
+                   KPAX_ECAPACITY;
+        k_env_fill<<<(n_obs + 255) / 256, 256, 0, cs>>>(g, s->obs, n_obs, s->cursor, s->ent);
+        KPAX_CHECK_LAUNCH();
+        count_launch(1);
+    }
+    return launch_propagate(p, g, d_parents, d_draws, draw_stream, n, d_rows, d_valid, d_steps, cs);
+}

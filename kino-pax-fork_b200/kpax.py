@@ -129,6 +129,8 @@ _SIGNATURES = {
     "kpax_env_destroy": (_I32, [_VP]),
     "kpax_env_stats": (_I32, [_VP, _VP, _VP]),
     "kpax_propagate_batch": (_I32, [ctypes.POINTER(Config), _VP, _VP, _VP, _U32, _U32, _VP, _VP, _VP, _VP]),
+    "kpax_propagate_batch_noalloc": (_I32, [ctypes.POINTER(Config), _VP, _U32, _VP, _VP, _U32, _U32, _VP, _VP, _VP,
+                                             _VP]),
     "kpax_collide_batch": (_I32, [_VP, _VP, _VP, _U32, _VP, _VP]),
     "kpax_region_batch": (_I32, [ctypes.POINTER(Config), _VP, _U32, _VP, _VP, _VP]),
     "kpax_kernel_launches": (ctypes.c_uint64, []),
@@ -211,6 +213,15 @@ def propagate_batch(cfg: Config, env: Env, d_parents: int, d_draws: int | None, 
                     d_valid: int, d_steps: int | None = None, stream: int = 0) -> None:
     check(load().kpax_propagate_batch(ctypes.byref(cfg), env.handle, d_parents, d_draws or None, draw_stream, n, d_rows,
                                       d_valid, d_steps or None, stream), "kpax_propagate_batch")
+
+
+def propagate_batch_noalloc(cfg: Config, d_obstacles: int, n_obs: int, d_parents: int, d_draws: int | None,
+                            draw_stream: int, n: int, d_rows: int, d_valid: int, d_steps: int | None = None,
+                            stream: int = 0) -> None:
+    """kpax_propagate_batch without any device allocation (grid in the library's fixed array)."""
+    check(load().kpax_propagate_batch_noalloc(ctypes.byref(cfg), d_obstacles or None, n_obs, d_parents, d_draws or None,
+                                              draw_stream, n, d_rows, d_valid, d_steps or None, stream),
+          "kpax_propagate_batch_noalloc")
 
 
 def collide_batch(env: Env, d_bbmin: int, d_bbmax: int, n: int, d_free: int, stream: int = 0) -> None:
