@@ -111,15 +111,17 @@ class Clocks:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def frontier_parents(cfg, obs, start, goal, n_parents: int = 2048):
-    """States of late frontier nodes from a short CPU plan (the oracle; CPU-baseline inputs only)."""
+def frontier_parents(cfg, obs, start, goal, n_parents: int = 2048, iters: int = 12):
+    """Parents for the CPU baseline: the nodes a short CPU plan (the oracle, same configuration)
+    appended in its last iterations, i.e. a steady-state frontier like the GPU's timed iterations."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
 
     small = cfg.copy()
-    small.expansions_per_iter = min(cfg.expansions_per_iter, 1 << 13)
-    r = O.plan(small, start, goal, obs, plan_idx=7, max_iters=6, stop_at_goal=False)
-    rows = r["rows"][-n_parents:, : cfg.state_dim]
+    small.expansions_per_iter = min(cfg.expansions_per_iter, 1 << 15)
+    r = O.plan(small, start, goal, obs, plan_idx=7, max_iters=iters, stop_at_goal=False)
+    new = int(r["iter_appended"][-3:].sum())
+    rows = r["rows"][-max(min(new, n_parents), 1):, : cfg.state_dim]
     return np.ascontiguousarray(rows, np.float32)
 
 
@@ -152,7 +154,9 @@ def cpu_reference_rate(cfg, obs, parents, budget_s: float, per_parent: int = 32,
         batches += 1
         if batches == 1 and dt > budget_s / 3 and n > 4096:
             n //= 4
-    return valid_total / t_total, threads, f"{batches} batches of <= {n} children (32 per frontier parent), {t_total:.1f} s"
+    return valid_total / t_total, threads, (f"{batches} batches of {n} children (32 per parent) of {parents.shape[0]} "
+                                            f"steady-state frontier parents, {valid_total / (batches * n):.2f} valid, "
+                                            f"{t_total:.1f} s")
 
 
 def dist_setup(n_gpus: int):

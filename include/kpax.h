@@ -220,6 +220,9 @@ kpax_status kpax_collide_batch(kpax_env* env, const float* d_bbmin, const float*
  * d_states: n x state_dim floats; d_r2 may be NULL. */
 kpax_status kpax_region_batch(const kpax_config* cfg, const float* d_states, uint32_t n,
                               int32_t* d_r1, int32_t* d_r2, void* stream);
+/* Test hook: for each x, writes (sin, cos) of the propagation kernels' sine/cosine and
+ * (sin, cos) of CUDA's sincosf, 4 floats per input, so tests can bound their difference. */
+kpax_status kpax_test_sincos(const float* d_x, uint32_t n, float* d_out, void* stream);
 /* Number of propagation kernels (and other library kernels) launched since load; the
  * benchmark reports it as evidence that the device path ran. */
 uint64_t kpax_kernel_launches(void);

@@ -5,8 +5,9 @@
 //    with explicitly rounded intrinsics (__fadd_rn/__fmul_rn/__fdiv_rn) so no multiply-add is
 //    fused; they are bit-identical to the oracle for identical inputs;
 //  - the double-integrator step is written the same way, so DI segments are bit-identical;
-//  - Dubins and quadrotor RK4 use the accurate sincosf/tanf/sqrtf and let the compiler fuse
-//    multiply-adds; they match the oracle within the propagation tolerance.
+//  - Dubins and quadrotor RK4 use a branch-free sine/cosine (sincos_fast, within a few ulp of
+//    CUDA's sincosf), tan as sin times the reciprocal cosine, IEEE sqrtf, and let the compiler
+//    fuse multiply-adds; they match the oracle within the propagation tolerance.
 #pragma once
 #include <stdint.h>
 
@@ -48,6 +49,37 @@ __device__ __forceinline__ void child_draws(const KParams& p, uint32_t stream, u
 __device__ __forceinline__ float reactivate_draw(const KParams& p, uint32_t stream, uint32_t iter, uint32_t index)
 {
     return u01(philox(index, iter, 2u, stream, p.seed_lo, p.seed_hi).x);
+}
+
+// ------------------------------------------------------------------ sine / cosine
+// Branch-free sin and cos of one argument for |x| <= kTrigFastMax: Cody-Waite reduction by pi/2
+// with pi/2 split in three parts (1.5703125 + 4.837512969970703125e-4 + 7.54978995489188216e-8),
+// then the single-precision minimax polynomials of the Cephes library (S. L. Moshier, sinf.c /
+// cosf.c) on [-pi/4, pi/4] and the quadrant map.  Straight-line code, so several calls interleave;
+// outside the range the caller falls back to CUDA's sincosf.  Error bound checked against
+// sincosf in tests/test_gpu_kernels.py.
+constexpr float kTrigFastMax = 8192.0f;
+
+__device__ __forceinline__ void sincos_fast(float x, float* sn, float* cs)
+{
+    const float n = rintf(x * 0.636619772367581343f);  // 2 / pi
+    float r = fmaf(n, -1.5703125f, x);
+    r = fmaf(n, -4.837512969970703125e-4f, r);
+    r = fmaf(n, -7.54978995489188216e-8f, r);
+    const float z = r * r;
+    const float ps = fmaf(fmaf(fmaf(-1.9515295891e-4f, z, 8.3321608736e-3f), z, -1.6666654611e-1f), z * r, r);
+    const float pc = fmaf(fmaf(fmaf(2.443315711809948e-5f, z, -1.388731625493765e-3f), z, 4.166664568298827e-2f), z * z,
+                          fmaf(-0.5f, z, 1.0f));
+    const int q = (int)n & 3;
+    const float a = (q & 1) ? pc : ps, b = (q & 1) ? ps : pc;
+    *sn = (q & 2) ? -a : a;
+    *cs = ((q + 1) & 2) ? -b : b;
+}
+
+__device__ __forceinline__ void sincos_checked(float x, float* sn, float* cs)
+{
+    sincos_fast(x, sn, cs);
+    if(!(fabsf(x) <= kTrigFastMax)) sincosf(x, sn, cs);  // huge or non-finite arguments
 }
 
 // float -> int with the reference's device semantics (saturating, NaN -> 0).
@@ -158,13 +190,16 @@ struct Grid {
     const float4* __restrict__ obs;
     const uint32_t* __restrict__ off;  // cells + 1
     const uint32_t* __restrict__ ent;
-    float wmin, cell;
+    float wmin, inv_cell;  // 1 / GRID_CELL_SIZE
     int dim;
 };
 
+// Cell of a coordinate.  Any non-decreasing map gives the brute-force verdict as long as the
+// build and the query use the same one; a multiply by the reciprocal replaces the reference's
+// division (spatialHash.cuh:236-246), which can move a point on a cell face by one cell.
 __device__ __forceinline__ int grid_coord(const Grid& g, float x)
 {
-    return clampi(f2i(__fdiv_rn(__fsub_rn(x, g.wmin), g.cell)), 0, g.dim - 1);
+    return clampi(f2i(__fmul_rn(__fsub_rn(x, g.wmin), g.inv_cell)), 0, g.dim - 1);
 }
 
 // isMotionValidSpatialHash (spatialHash.cu:145-194) with isBroadPhaseValid (collisionCheck.cu:3-10):
@@ -269,12 +304,23 @@ __device__ __forceinline__ bool prop_dubins(const KParams& p, const Grid& g, flo
         const float p0[3] = {s[0], s[1], s[2]};
         const float yaw = s[3], pitch = s[4], v = s[5];
         float sp0, cp0, sy0, cy0, sp1, cp1, sy1, cy1, sp2, cp2, sy2, cy2;
-        sincosf(pitch, &sp0, &cp0);
-        sincosf(yaw, &sy0, &cy0);
-        sincosf(pitch + hh * pr, &sp1, &cp1);
-        sincosf(yaw + hh * yr, &sy1, &cy1);
-        sincosf(pitch + h * pr, &sp2, &cp2);
-        sincosf(yaw + h * yr, &sy2, &cy2);
+        const float p1 = pitch + hh * pr, y1 = yaw + hh * yr, p2 = pitch + h * pr, y2 = yaw + h * yr;
+        sincos_fast(pitch, &sp0, &cp0);
+        sincos_fast(yaw, &sy0, &cy0);
+        sincos_fast(p1, &sp1, &cp1);
+        sincos_fast(y1, &sy1, &cy1);
+        sincos_fast(p2, &sp2, &cp2);
+        sincos_fast(y2, &sy2, &cy2);
+        if(!(fmaxf(fmaxf(fabsf(yaw), fabsf(y1)), fabsf(y2)) <= kTrigFastMax)) {
+            sincosf(yaw, &sy0, &cy0);
+            sincosf(y1, &sy1, &cy1);
+            sincosf(y2, &sy2, &cy2);
+        }
+        if(!(fmaxf(fmaxf(fabsf(pitch), fabsf(p1)), fabsf(p2)) <= kTrigFastMax)) {
+            sincosf(pitch, &sp0, &cp0);
+            sincosf(p1, &sp1, &cp1);
+            sincosf(p2, &sp2, &cp2);
+        }
         const float vm = v + hh * a, ve = v + h * a;
         const float mx = vm * cp1 * cy1, my = vm * cp1 * sy1, mz = vm * sp1;
         s[0] += h6 * (v * cp0 * cy0 + 2.0f * (mx + mx) + ve * cp2 * cy2);
@@ -302,24 +348,29 @@ __device__ __forceinline__ bool prop_dubins(const KParams& p, const Grid& g, flo
 
 // Quadrotor right-hand side, statePropagator.cu:325-370, evaluated at x0 + delta*k.
 // Model constants NU 10e-3, MU 2e-6, IX 1, IY 1, IZ 2, GRAVITY -9.81, MASS 1 (config.h:300-308).
-__device__ __forceinline__ void quad_rhs(float* xd, const float* x0, const float* k, float delta, const float* c)
+__device__ __forceinline__ void quad_rhs(float* xd, const float* x0, const float* k, float delta, const float* c)  // xd may alias k
 {
     const float NU = 10e-3f, MU = 2e-6f, G = -9.81f;
     const float phi = x0[3] + delta * k[3], theta = x0[4] + delta * k[4], psi = x0[5] + delta * k[5];
     const float u = x0[6] + delta * k[6], v = x0[7] + delta * k[7], w = x0[8] + delta * k[8];
     const float pp = x0[9] + delta * k[9], q = x0[10] + delta * k[10], r = x0[11] + delta * k[11];
     float sf, cf, st, ct, sp, cp;
-    sincosf(phi, &sf, &cf);
-    sincosf(theta, &st, &ct);
-    sincosf(psi, &sp, &cp);
-    const float tt = tanf(theta);
+    sincos_fast(phi, &sf, &cf);
+    sincos_fast(theta, &st, &ct);
+    sincos_fast(psi, &sp, &cp);
+    if(!(fmaxf(fabsf(phi), fmaxf(fabsf(theta), fabsf(psi))) <= kTrigFastMax)) {
+        sincosf(phi, &sf, &cf);
+        sincosf(theta, &st, &ct);
+        sincosf(psi, &sp, &cp);
+    }
+    const float sec = __frcp_rn(ct);  // tan(theta) = sin * sec, 1/cos(theta) = sec
     xd[0] = ct * cp * u + (sf * st * cp - cf * sp) * v + (cf * st * cp + sf * sp) * w;
     xd[1] = ct * sp * u + (sf * st * sp + cf * cp) * v + (cf * st * sp - sf * cp) * w;
     xd[2] = -st * u + sf * ct * v + cf * ct * w;
     const float qr = q * sf + r * cf;
-    xd[3] = pp + qr * tt;
+    xd[3] = pp + qr * (st * sec);
     xd[4] = q * cf - r * sf;
-    xd[5] = qr / ct;
+    xd[5] = qr * sec;
     const float XYZ = -NU * sqrtf(u * u + v * v + w * w);
     xd[6] = (r * v - q * w) - G * st + XYZ * u;
     xd[7] = (pp * w - r * u) + G * ct * sf + XYZ * v;
@@ -330,22 +381,34 @@ __device__ __forceinline__ void quad_rhs(float* xd, const float* x0, const float
     xd[11] = 0.0f * (pp * q) + 0.5f * (LMN * r) + 0.5f * c[3];  // (IX - IY)/IZ = 0, 1/IZ = 0.5
 }
 
-// Quadrotor RK4, statePropagatorSpatialHash.cu:234-308.
+// Quadrotor RK4, statePropagatorSpatialHash.cu:234-308.  The four stages run as a loop over one
+// copy of the right-hand side (k is updated in place: each stage reads the previous stage's k
+// before writing its own); the stage sum keeps the reference's order ((k1 + 2k2) + 2k3) + k4.
 __device__ __forceinline__ bool prop_quad(const KParams& p, const Grid& g, float* s, const float* c, int steps, int& done)
 {
     const float h = p.h, hh = p.hh, h6 = p.h6;
-    const float zero[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     bool valid = true;
     int i = 0;
     for(; i < steps; ++i) {
         const float p0[3] = {s[0], s[1], s[2]};
-        float k1[12], k2[12], k3[12], k4[12];
-        quad_rhs(k1, s, zero, 1.0f, c);
-        quad_rhs(k2, s, k1, hh, c);
-        quad_rhs(k3, s, k2, hh, c);
-        quad_rhs(k4, s, k3, h, c);
+        float k[12], acc[12];
 #pragma unroll
-        for(int j = 0; j < 12; ++j) s[j] += h6 * (k1[j] + 2.0f * k2[j] + 2.0f * k3[j] + k4[j]);
+        for(int j = 0; j < 12; ++j) k[j] = 0.0f;
+#pragma unroll 1
+        for(int stage = 0; stage < 4; ++stage) {
+            const float delta = stage == 0 ? 1.0f : (stage == 3 ? h : hh);
+            quad_rhs(k, s, k, delta, c);
+            if(stage == 0) {
+#pragma unroll
+                for(int j = 0; j < 12; ++j) acc[j] = k[j];
+            } else {
+                const float w = stage == 3 ? 1.0f : 2.0f;
+#pragma unroll
+                for(int j = 0; j < 12; ++j) acc[j] = acc[j] + w * k[j];
+            }
+        }
+#pragma unroll
+        for(int j = 0; j < 12; ++j) s[j] += h6 * acc[j];
         if(s[6] < p.vmin || s[6] > p.vmax || s[7] < p.vmin || s[7] > p.vmax || s[8] < p.vmin || s[8] > p.vmax) {
             valid = false;
             break;

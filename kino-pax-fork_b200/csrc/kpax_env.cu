@@ -25,21 +25,33 @@ __device__ __forceinline__ void obstacle_cells(const Grid& g, const float4& lo, 
     c1[0] = grid_coord(g, hi.x), c1[1] = grid_coord(g, hi.y), c1[2] = grid_coord(g, hi.z);
 }
 
-// Pack n x 6 floats into float4 pairs and count (cell, obstacle) pairs per cell.
+// Cell (x, y, z) of the k-th cell of an obstacle's cell box [c0, c1].
+__device__ __forceinline__ int box_cell(const Grid& g, const int c0[3], const int c1[3], int k)
+{
+    const int nx = c1[0] - c0[0] + 1, ny = c1[1] - c0[1] + 1;
+    const int x = c0[0] + k % nx, y = c0[1] + (k / nx) % ny, z = c0[2] + k / (nx * ny);
+    return x + g.dim * (y + g.dim * z);
+}
+
+__device__ __forceinline__ int box_cells(const int c0[3], const int c1[3])
+{
+    return (c1[0] - c0[0] + 1) * (c1[1] - c0[1] + 1) * (c1[2] - c0[2] + 1);
+}
+
+// One warp per obstacle: pack n x 6 floats into float4 pairs and count (cell, obstacle) pairs.
 __global__ void k_env_count(Grid g, const float* __restrict__ obs, uint32_t n, float4* __restrict__ packed,
                             uint32_t* __restrict__ counts)
 {
-    const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t o = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if(o >= n) return;
     const float* b = obs + (size_t)6 * o;
     const float4 lo = make_float4(b[0], b[1], b[2], 0.0f), hi = make_float4(b[3], b[4], b[5], 0.0f);
-    packed[2 * o] = lo;
-    packed[2 * o + 1] = hi;
+    if(lane == 0) packed[2 * o] = lo, packed[2 * o + 1] = hi;
     int c0[3], c1[3];
     obstacle_cells(g, lo, hi, c0, c1);
-    for(int z = c0[2]; z <= c1[2]; ++z)
-        for(int y = c0[1]; y <= c1[1]; ++y)
-            for(int x = c0[0]; x <= c1[0]; ++x) atomicAdd(counts + x + g.dim * (y + g.dim * z), 1u);
+    const int total = box_cells(c0, c1);
+    for(int k = lane; k < total; k += 32) atomicAdd(counts + box_cell(g, c0, c1, k), 1u);
 }
 
 // Exclusive scan of counts[0, n) in place (single CTA of 1024 threads); counts[n] = total;
@@ -84,14 +96,16 @@ __global__ void __launch_bounds__(1024) k_env_scan(uint32_t* __restrict__ counts
 __global__ void k_env_fill(Grid g, const float4* __restrict__ packed, uint32_t n, uint32_t* __restrict__ cursor,
                            uint32_t* __restrict__ ent)
 {
-    const uint32_t o = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t o = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if(o >= n) return;
     int c0[3], c1[3];
     obstacle_cells(g, packed[2 * o], packed[2 * o + 1], c0, c1);
-    for(int z = c0[2]; z <= c1[2]; ++z)
-        for(int y = c0[1]; y <= c1[1]; ++y)
-            for(int x = c0[0]; x <= c1[0]; ++x) ent[atomicAdd(cursor + x + g.dim * (y + g.dim * z), 1u)] = o;
+    const int total = box_cells(c0, c1);
+    for(int k = lane; k < total; k += 32) ent[atomicAdd(cursor + box_cell(g, c0, c1, k), 1u)] = o;
 }
+
+inline uint32_t warp_blocks(uint32_t n) { return (uint32_t)(((uint64_t)n * 32 + 255) / 256); }
 
 // ---------------------------------------------------------------- batch kernels
 
@@ -150,6 +164,16 @@ __global__ void k_region_batch(KParams p, const float* __restrict__ states, uint
     if(r2) r2[i] = region_r2(p, s, a);
 }
 
+__global__ void k_sincos_pair(const float* __restrict__ x, uint32_t n, float* __restrict__ out)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= n) return;
+    float s, c, s2, c2;
+    sincos_checked(x[i], &s, &c);
+    sincosf(x[i], &s2, &c2);
+    out[4 * i] = s, out[4 * i + 1] = c, out[4 * i + 2] = s2, out[4 * i + 3] = c2;
+}
+
 }  // namespace
 
 kpax_status Env::build(const KParams& p, const float* d_obstacles, uint32_t n, cudaStream_t stream)
@@ -175,7 +199,7 @@ kpax_status Env::build(const KParams& p, const float* d_obstacles, uint32_t n, c
     KPAX_CUDA(cudaMemsetAsync(d_off, 0, sizeof(uint32_t) * (cells + 1), stream));
     const Grid g0 = view();
     if(n) {
-        k_env_count<<<(n + 255) / 256, 256, 0, stream>>>(g0, d_obstacles, n, d_obs, d_off);
+        k_env_count<<<warp_blocks(n), 256, 0, stream>>>(g0, d_obstacles, n, d_obs, d_off);
         KPAX_CHECK_LAUNCH();
         k_env_scan<<<1, 1024, 0, stream>>>(d_off, cells, d_cursor);
         KPAX_CHECK_LAUNCH();
@@ -189,7 +213,7 @@ kpax_status Env::build(const KParams& p, const float* d_obstacles, uint32_t n, c
             KPAX_CUDA(cudaMalloc(&d_ent, sizeof(uint32_t) * want));
             ent_cap = want;
         }
-        k_env_fill<<<(n + 255) / 256, 256, 0, stream>>>(view(), d_obs, n, d_cursor, d_ent);
+        k_env_fill<<<warp_blocks(n), 256, 0, stream>>>(view(), d_obs, n, d_cursor, d_ent);
         KPAX_CHECK_LAUNCH();
         count_launch(1);
     } else {
@@ -245,6 +269,15 @@ using namespace kpax;
 extern "C" {
 
 uint64_t kpax_kernel_launches(void) { return g_launches.load(); }
+
+kpax_status kpax_test_sincos(const float* d_x, uint32_t n, float* d_out, void* stream)
+{
+    if(n && (!d_x || !d_out)) return set_error("kpax_test_sincos: null argument"), KPAX_EINVAL;
+    if(!n) return KPAX_OK;
+    k_sincos_pair<<<(n + 255) / 256, 256, 0, (cudaStream_t)stream>>>(d_x, n, d_out);
+    KPAX_CHECK_LAUNCH();
+    return KPAX_OK;
+}
 
 kpax_status kpax_env_create(const kpax_config* cfg, const float* d_obstacles, uint32_t n_obs, void* stream, kpax_env** out)
 {
@@ -391,11 +424,11 @@ extern "C" kpax_status kpax_propagate_batch_noalloc(const kpax_config* cfg, cons
     NoAllocScratch* s = nullptr;
     if((st = noalloc_scratch(&s)) != KPAX_OK) return st;
     cudaStream_t cs = (cudaStream_t)stream;
-    const Grid g{s->obs, s->off, s->ent, p.wmin, p.cell, p.gdim};
+    const Grid g{s->obs, s->off, s->ent, p.wmin, 1.0f / p.cell, p.gdim};
     // the array keeps the previous call's grid: the counts must start from zero
     KPAX_CUDA(cudaMemsetAsync(s->off, 0, sizeof(uint32_t) * (cells + 1), cs));
     if(n_obs) {
-        k_env_count<<<(n_obs + 255) / 256, 256, 0, cs>>>(g, d_obstacles, n_obs, s->obs, s->off);
+        k_env_count<<<warp_blocks(n_obs), 256, 0, cs>>>(g, d_obstacles, n_obs, s->obs, s->off);
         KPAX_CHECK_LAUNCH();
         k_env_scan<<<1, 1024, 0, cs>>>(s->off, cells, s->cursor);
         KPAX_CHECK_LAUNCH();
@@ -407,7 +440,7 @@ extern "C" kpax_status kpax_propagate_batch_noalloc(const kpax_config* cfg, cons
             return set_error("kpax_propagate_batch_noalloc: %u (cell, obstacle) pairs exceed the limit of %u", total,
                              kNoAllocMaxEntries),
                    KPAX_ECAPACITY;
-        k_env_fill<<<(n_obs + 255) / 256, 256, 0, cs>>>(g, s->obs, n_obs, s->cursor, s->ent);
+        k_env_fill<<<warp_blocks(n_obs), 256, 0, cs>>>(g, s->obs, n_obs, s->cursor, s->ent);
         KPAX_CHECK_LAUNCH();
         count_launch(1);
     }

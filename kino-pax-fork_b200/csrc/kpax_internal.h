@@ -38,7 +38,7 @@ struct Env {
     uint32_t obs_cap = 0, ent_cap = 0;
     bool owned_by_planner = false;
 
-    Grid view() const { return Grid{d_obs, d_off, d_ent, wmin, cell, dim}; }
+    Grid view() const { return Grid{d_obs, d_off, d_ent, wmin, 1.0f / cell, dim}; }
     // Build from n x 6 device floats on `stream` (synchronises once to size the entry list).
     kpax_status build(const KParams& p, const float* d_obstacles, uint32_t n, cudaStream_t stream);
     void release();

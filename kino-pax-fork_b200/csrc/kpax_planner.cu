@@ -27,7 +27,9 @@ namespace {
 constexpr uint8_t kPending = 255;
 constexpr uint32_t kNone = 0xFFFFFFFFu;
 constexpr int kFrontierBS = 256, kItems = 4, kTile = kFrontierBS * kItems;
-constexpr int kExpandBS = 128;
+constexpr int kExpandBS = 448;  // 2^16 children over 148 SMs: one 14-warp block per SM
+constexpr int kFrontierCTAs = 2 * 148;
+constexpr int kScoreBS = 256, kScoreCTAs = 128, kPartials = 1024;
 constexpr uint32_t kSpinLimit = 1u << 22;  // ~4 s of polling before a wait gives up
 constexpr uint32_t kErrTimeout = 1u, kErrCapacity = 2u;
 
@@ -64,6 +66,8 @@ struct alignas(16) Ctl {
     uint32_t plan_idx, max_iters, stop_at_goal, epoch;
     uint32_t ticket1, ticket2, iters_done, path_len;
     float faccept, goal[3];
+    float score_total;      // sum of raw region scores of the last score pass
+    uint32_t scores_ready;  // 0 until the first score pass of a plan (scores read as 0, KPAX.cu:69)
     unsigned long long n_exp, n_valid, n_steps;
     double path_cost;
 };
@@ -77,25 +81,42 @@ __device__ __forceinline__ void lb_publish(unsigned long long* slot, uint32_t ep
     atomicExch(slot, w);
 }
 
-// Exclusive prefix of block b; false if a predecessor never published (bounded wait).
+// Exclusive prefix of tile b, computed by the 32 lanes of one warp: each probe reads the status
+// of 32 predecessors at once and stops at the nearest inclusive prefix.  Returns false when a
+// predecessor never published (bounded wait, ~4 s).
 __device__ __forceinline__ bool lb_exclusive(unsigned long long* lb, uint32_t b, uint32_t epoch, uint32_t& excl)
 {
-    excl = 0;
-    int j = (int)b - 1;
-    uint32_t spins = 0;
     const uint32_t tag = epoch & 0x3FFFFFFFu;
-    while(j >= 0) {
-        const unsigned long long w = atomicAdd(lb + j, 0ull);
-        const uint32_t flag = (uint32_t)(w >> 32) & 3u;
-        if((uint32_t)(w >> 34) != tag || flag == 0u) {
-            if(++spins > kSpinLimit) return false;
+    const int lane = threadIdx.x & 31;
+    uint32_t acc = 0, spins = 0;
+    int top = (int)b - 1;
+    while(top >= 0) {
+        const int j = top - lane;  // lane 0 probes the nearest predecessor
+        uint32_t flag = 2u, val = 0u;  // past tile 0: an inclusive prefix of zero
+        if(j >= 0) {
+            const unsigned long long w = atomicAdd(lb + j, 0ull);
+            flag = (uint32_t)(w >> 34) == tag ? (uint32_t)(w >> 32) & 3u : 0u;
+            val = (uint32_t)w;
+        }
+        const uint32_t ready = __ballot_sync(0xffffffffu, flag != 0u), incl = __ballot_sync(0xffffffffu, flag == 2u);
+        const int first = incl ? __ffs(incl) - 1 : 31;
+        const uint32_t need = first == 31 ? 0xffffffffu : ((2u << first) - 1u);
+        if((ready & need) != need) {
+            if(++spins > kSpinLimit) {
+                excl = acc;
+                return false;
+            }
             if(spins > 32) __nanosleep(100);
             continue;
         }
-        excl += (uint32_t)w;
-        if(flag == 2u) break;
-        --j;
+        uint32_t v = lane <= first ? val : 0u;
+#pragma unroll
+        for(int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+        acc += v;
+        if(incl) break;
+        top -= 32;
     }
+    excl = acc;
     return true;
 }
 
@@ -113,6 +134,13 @@ __device__ __forceinline__ uint32_t popcount_range(const uint32_t* __restrict__ 
         n += __popc(m);
     }
     return n;
+}
+
+// Normalised score of a region (Graph.cu:297-304, 349-357) from its stored raw score.
+__device__ __forceinline__ float region_score(float raw, float total, uint32_t ready, float eps)
+{
+    if(!ready) return 0.0f;
+    return raw < 0.0f ? 1.0f : __fadd_rn(eps, __fdiv_rn(raw, total));
 }
 
 template <int SD>
@@ -172,99 +200,159 @@ __global__ void k_begin(KParams p, TreeDev t, Ctl* ctl, const float* __restrict_
     *ctl = z;
 }
 
-__global__ void __launch_bounds__(kFrontierBS) k_frontier(KParams p, TreeDev t, RegDev rg, Ctl* ctl,
-                                                          uint32_t* __restrict__ entries, unsigned long long* __restrict__ lb)
+// Frontier pass 1: resolve every live node's repeat count (re-activation of the previous
+// iteration, KPAX.cu:505-517; repeat of nodes added last iteration, KPAX.cu:476-479) and write
+// one sum per tile of kTile nodes.  The last CTA to finish scans the tile sums, giving the total
+// entry count R, and sets this iteration's budget (KPAX.cu:323-350).
+__device__ __forceinline__ uint32_t resolve_repeat(const KParams& p, const TreeDev& t, const RegDev& rg, uint32_t i,
+                                                   uint32_t tree_old, uint32_t iter, uint32_t plan, float fa, float total,
+                                                   uint32_t ready)
 {
-    __shared__ uint32_t s_b, s_excl, s_done, s_ok;
-    __shared__ uint32_t s_warp[kFrontierBS / 32];
-    if(threadIdx.x == 0) {
-        s_done = ctl->done;
-        s_b = s_done ? 0u : atomicAdd(&ctl->ticket1, 1u);
+    const uint32_t r0 = t.rep[i];
+    uint32_t r = r0;
+    if(r == 0u) {
+        if(i < tree_old) {
+            const float sc = region_score(rg.score[t.r1[i]], total, ready, p.eps);
+            if(reactivate_draw(p, plan, iter - 1u, i) <= __fadd_rn(sc, fa)) r = 1u;
+        }
+    } else if(r == kPending) {
+        r = rg.valid[t.r1[i]] < p.sparse_thr ? p.sparse_repeat : 1u;
     }
+    if(r != r0) t.rep[i] = (uint8_t)r;
+    return r;
+}
+
+__global__ void __launch_bounds__(kFrontierBS) k_frontier_count(KParams p, TreeDev t, RegDev rg, Ctl* ctl,
+                                                                uint32_t* __restrict__ tile_sums, uint32_t* __restrict__ arrivals)
+{
+    __shared__ uint32_t s_done, s_last, s_carry;
+    __shared__ uint32_t s_warp[kFrontierBS / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if(threadIdx.x == 0) s_done = ctl->done;
     __syncthreads();
     if(s_done) return;
-    const uint32_t b = s_b, tree = ctl->tree, tree_old = ctl->tree_old, iter = ctl->iter;
-    const uint32_t plan = ctl->plan_idx, epoch = ctl->epoch;
-    const float fa = ctl->faccept;
-    const uint32_t nblk = (tree + kTile - 1) / kTile;
-    if(b >= nblk) return;
-    const uint32_t i0 = b * kTile + threadIdx.x * kItems;
-    uint32_t cnt[kItems], sum = 0;
+    const uint32_t tree = ctl->tree, tree_old = ctl->tree_old, iter = ctl->iter, plan = ctl->plan_idx;
+    const uint32_t ready = ctl->scores_ready;
+    const float fa = ctl->faccept, total = ctl->score_total;
+    const uint32_t ntiles = (tree + kTile - 1) / kTile;
+    for(uint32_t b = blockIdx.x; b < ntiles; b += gridDim.x) {
+        uint32_t sum = 0;
 #pragma unroll
-    for(int j = 0; j < kItems; ++j) {
-        const uint32_t i = i0 + j;
-        uint32_t c = 0;
-        if(i < tree) {
-            const uint32_t r0 = t.rep[i];
-            uint32_t r = r0;
-            if(r == 0u) {
-                if(i < tree_old && reactivate_draw(p, plan, iter - 1u, i) <= __fadd_rn(rg.score[t.r1[i]], fa)) r = 1u;
-            } else if(r == kPending) {
-                r = rg.valid[t.r1[i]] < p.sparse_thr ? p.sparse_repeat : 1u;
-            }
-            if(r != r0) t.rep[i] = (uint8_t)r;
-            c = r;
+        for(int j = 0; j < kItems; ++j) {
+            const uint32_t i = b * kTile + j * kFrontierBS + threadIdx.x;  // coalesced
+            if(i < tree) sum += resolve_repeat(p, t, rg, i, tree_old, iter, plan, fa, total, ready);
         }
-        cnt[j] = c;
-        sum += c;
-    }
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t x = sum;
 #pragma unroll
-    for(int d = 1; d < 32; d <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
-        if(lane >= d) x += y;
+        for(int d = 16; d > 0; d >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, d);
+        if(lane == 0) s_warp[warp] = sum;
+        __syncthreads();
+        if(threadIdx.x == 0) {
+            uint32_t acc = 0;
+            for(int w = 0; w < kFrontierBS / 32; ++w) acc += s_warp[w];
+            tile_sums[b] = acc;
+        }
+        __syncthreads();
     }
-    if(lane == 31) s_warp[warp] = x;
+    __threadfence();
     __syncthreads();
+    if(threadIdx.x == 0) s_last = atomicAdd(arrivals, 1u) == gridDim.x - 1u;
+    __syncthreads();
+    if(!s_last) return;
+    __threadfence();
+    // exclusive scan of the tile sums in place (kFrontierBS at a time), total R
+    if(threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    volatile uint32_t* ts = tile_sums;
+    for(uint32_t base = 0; base < ntiles; base += kFrontierBS) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t v = i < ntiles ? ts[i] : 0u;
+        uint32_t x = v;
+#pragma unroll
+        for(int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+            if(lane >= d) x += y;
+        }
+        if(lane == 31) s_warp[warp] = x;
+        __syncthreads();
+        uint32_t wex = 0;
+        for(int w = 0; w < warp; ++w) wex += s_warp[w];
+        const uint32_t excl = s_carry + wex + x - v;
+        if(i < ntiles) ts[i] = excl;
+        __syncthreads();
+        if(threadIdx.x == kFrontierBS - 1) s_carry = excl + v;
+        __syncthreads();
+    }
     if(threadIdx.x == 0) {
-        uint32_t acc = 0;
-        for(int w = 0; w < kFrontierBS / 32; ++w) {
-            const uint32_t v = s_warp[w];
-            s_warp[w] = acc;
-            acc += v;
-        }
-        uint32_t excl = 0;
-        bool ok = true;
-        if(b == 0) {
-            lb_publish(lb, epoch, 2u, acc);
-        } else {
-            lb_publish(lb + b, epoch, 1u, acc);
-            ok = lb_exclusive(lb, b, epoch, excl);
-            if(ok) lb_publish(lb + b, epoch, 2u, excl + acc);
-        }
-        if(!ok) {
-            atomicOr(&ctl->error, kErrTimeout);
+        *arrivals = 0u;
+        const uint64_t R = s_carry;
+        const uint32_t B = min(p.budget, p.cap - tree);
+        uint32_t k = p.per_entry, E = 0, n = 0;
+        if(B == 0) {
+            ctl->full = 1u;
             ctl->done = 1u;
-        }
-        s_excl = excl;
-        s_ok = ok;
-        if(ok && b == nblk - 1) {  // the budget of this iteration (KPAX.cu:323-350)
-            const uint64_t R = (uint64_t)excl + acc;
-            const uint32_t B = min(p.budget, p.cap - tree);
-            uint32_t k = p.per_entry, E = 0, n = 0;
-            if(B == 0) {
-                ctl->full = 1u;
-                ctl->done = 1u;
-            } else {
-                if(R * k > B) {
-                    k = (uint32_t)(B / (R ? R : 1));
-                    if(k == 0) k = 1;
-                }
-                E = (uint32_t)(R < (uint64_t)(B / k) ? R : (uint64_t)(B / k));
-                n = E * k;
+        } else if(R) {
+            if(R * k > B) {
+                k = (uint32_t)(B / R);
+                if(k == 0) k = 1;
             }
-            ctl->R = (uint32_t)(R < 0xFFFFFFFFull ? R : 0xFFFFFFFFull);
-            ctl->k = k, ctl->E = E, ctl->n = n;
+            E = (uint32_t)(R < (uint64_t)(B / k) ? R : (uint64_t)(B / k));
+            n = E * k;
         }
+        ctl->R = (uint32_t)R;
+        ctl->k = k, ctl->E = E, ctl->n = n;
     }
+}
+
+// Frontier pass 2: node i owns virtual entries [a, a + rep) with a from the tile scan.  Entry j
+// of the E taken is virtual entry floor(j*R/E), i.e. node i writes entries ceil(a*E/R) ..
+// ceil((a+rep)*E/R) - 1 (all of its entries when E == R).  Nodes with an entry taken leave the
+// frontier (KPAX.cu:372).
+__global__ void __launch_bounds__(kFrontierBS) k_frontier_write(KParams p, TreeDev t, Ctl* ctl,
+                                                                const uint32_t* __restrict__ tile_pre,
+                                                                uint32_t* __restrict__ entries)
+{
+    __shared__ uint32_t s_done;
+    __shared__ uint32_t s_warp[kFrontierBS / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if(threadIdx.x == 0) s_done = ctl->done;
     __syncthreads();
-    if(!s_ok) return;
-    uint32_t pos = s_excl + s_warp[warp] + x - sum;
+    if(s_done) return;
+    const uint32_t tree = ctl->tree, E = ctl->E;
+    const uint64_t R = ctl->R;
+    if(E == 0) return;
+    const uint32_t ntiles = (tree + kTile - 1) / kTile;
+    for(uint32_t b = blockIdx.x; b < ntiles; b += gridDim.x) {
+        // kItems consecutive nodes per thread so the in-tile prefix is a plain block scan
+        const uint32_t i0 = b * kTile + threadIdx.x * kItems;
+        uint32_t cnt[kItems], sum = 0;
 #pragma unroll
-    for(int j = 0; j < kItems; ++j)
-        for(uint32_t r = 0; r < cnt[j]; ++r, ++pos)
-            if(pos < p.budget) entries[pos] = i0 + j;
+        for(int j = 0; j < kItems; ++j) {
+            const uint32_t i = i0 + j;
+            cnt[j] = i < tree ? (uint32_t)t.rep[i] : 0u;
+            sum += cnt[j];
+        }
+        uint32_t x = sum;
+#pragma unroll
+        for(int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+            if(lane >= d) x += y;
+        }
+        if(lane == 31) s_warp[warp] = x;
+        __syncthreads();
+        uint32_t wex = 0;
+        for(int w = 0; w < warp; ++w) wex += s_warp[w];
+        uint64_t a = (uint64_t)tile_pre[b] + wex + x - sum;
+#pragma unroll
+        for(int j = 0; j < kItems; ++j) {
+            if(!cnt[j]) continue;
+            const uint64_t bnd = a + cnt[j];
+            const uint64_t lo = (a * E + R - 1) / R, hi = (bnd * E + R - 1) / R;
+            for(uint64_t e = lo; e < hi; ++e) entries[e] = i0 + j;
+            if(lo < hi) t.rep[i0 + j] = 0;
+            a = bnd;
+        }
+        __syncthreads();
+    }
 }
 
 template <int M>
@@ -283,6 +371,8 @@ __global__ void __launch_bounds__(kExpandBS) k_expand(KParams p, Grid g, TreeDev
     __syncthreads();
     if(s_done) return;
     const uint32_t n = ctl->n, k = ctl->k, tree = ctl->tree, iter = ctl->iter, plan = ctl->plan_idx, epoch = ctl->epoch;
+    const uint32_t ready = ctl->scores_ready;
+    const float total = ctl->score_total;
     const uint32_t nblk = n ? (n + kExpandBS - 1) / kExpandBS : 1u, b = s_b;
     if(b >= nblk) return;
     const uint32_t c = b * kExpandBS + threadIdx.x;
@@ -294,7 +384,6 @@ __global__ void __launch_bounds__(kExpandBS) k_expand(KParams p, Grid g, TreeDev
     if(active) {
         const uint32_t e = c / k;
         parent = entries[e];
-        if(c == e * k) t.rep[parent] = 0;  // expanded nodes leave the frontier (KPAX.cu:372)
         load_state<SD>(t, parent, s);
         child_draws(p, plan, iter, c, u);
         steps = draw_controls(p, u, cc);
@@ -306,7 +395,7 @@ __global__ void __launch_bounds__(kExpandBS) k_expand(KParams p, Grid g, TreeDev
             atomicAdd(rg.valid + r1v, 1);
             const uint32_t word = (uint32_t)r2v >> 5, bit = 1u << (r2v & 31);
             const bool seen = (__ldg(rg.cur + word) & bit) != 0u;
-            next = (u[5] < __ldg(rg.score + r1v)) || !seen;
+            next = (u[5] < region_score(__ldg(rg.score + r1v), total, ready, p.eps)) || !seen;
             atomicOr(rg.nxt + word, bit);
         }
         row_controls<M>(cc, rc);
@@ -326,38 +415,36 @@ __global__ void __launch_bounds__(kExpandBS) k_expand(KParams p, Grid g, TreeDev
     for(int d = 16; d > 0; d >>= 1) wsteps += __shfl_xor_sync(0xffffffffu, wsteps, d);
     if(lane == 0) s_wn[warp] = __popc(mn), s_wv[warp] = __popc(mv), s_ws[warp] = wsteps;
     __syncthreads();
-    if(threadIdx.x == 0) {
+    if(warp == 0) {
         uint32_t acc = 0, nv = 0;
         unsigned long long ns = 0;
-        for(int w = 0; w < NW; ++w) {
-            const uint32_t v = s_wn[w];
-            s_wn[w] = acc;
-            acc += v;
-            nv += s_wv[w];
-            ns += s_ws[w];
-        }
-        if(nv) atomicAdd(&ctl->n_valid, (unsigned long long)nv);
-        if(ns) atomicAdd(&ctl->n_steps, ns);
+        for(int w = 0; w < NW; ++w) acc += s_wn[w], nv += s_wv[w], ns += s_ws[w];
         uint32_t excl = 0;
         bool ok = true;
         if(b == 0) {
-            lb_publish(lb, epoch, 2u, acc);
+            if(lane == 0) lb_publish(lb, epoch, 2u, acc);
         } else {
-            lb_publish(lb + b, epoch, 1u, acc);
+            if(lane == 0) lb_publish(lb + b, epoch, 1u, acc);
             ok = lb_exclusive(lb, b, epoch, excl);
-            if(ok) lb_publish(lb + b, epoch, 2u, excl + acc);
+            if(ok && lane == 0) lb_publish(lb + b, epoch, 2u, excl + acc);
         }
-        if(!ok) {
-            atomicOr(&ctl->error, kErrTimeout);
-            ctl->done = 1u;
+        if(lane == 0) {
+            if(nv) atomicAdd(&ctl->n_valid, (unsigned long long)nv);
+            if(ns) atomicAdd(&ctl->n_steps, ns);
+            if(!ok) {
+                atomicOr(&ctl->error, kErrTimeout);
+                ctl->done = 1u;
+            }
+            if(ok && b == nblk - 1) ctl->appended = excl + acc;
+            s_excl = excl;
+            s_ok = ok;
         }
-        if(ok && b == nblk - 1) ctl->appended = excl + acc;
-        s_excl = excl;
-        s_ok = ok;
     }
     __syncthreads();
     if(!next || !s_ok) return;
-    const uint32_t slot = tree + s_excl + s_wn[warp] + rank;
+    uint32_t wex = 0;  // accepted children of the lower warps of this block
+    for(int w = 0; w < warp; ++w) wex += s_wn[w];
+    const uint32_t slot = tree + s_excl + wex + rank;
     if(slot >= p.cap) {
         atomicOr(&ctl->error, kErrCapacity);
         return;
@@ -373,41 +460,65 @@ __global__ void __launch_bounds__(kExpandBS) k_expand(KParams p, Grid g, TreeDev
     if(d < p.goal_thresh) atomicMin(&ctl->goal_idx, slot);
 }
 
-__global__ void __launch_bounds__(1024) k_scores(KParams p, RegDev rg, Ctl* ctl)
+// Region scores (Graph.cu:233-358) over kScoreCTAs CTAs, one warp per partial sum j: lane m
+// scores region j + 1024*m and the warp adds them in ascending region order; the last CTA to
+// finish adds the 1024 partials with a fixed halving tree, so the total (and every normalised
+// score) is bit-identical to the oracle's.  Scores are stored raw (negative = no valid sample) and
+// normalised where they are read (region_score).
+__global__ void __launch_bounds__(kScoreBS) k_scores(KParams p, RegDev rg, Ctl* ctl, float* __restrict__ partials,
+                                                     uint32_t* __restrict__ arrivals)
 {
-    __shared__ float s_part[1024];
-    __shared__ uint32_t s_done;
-    const int tid = threadIdx.x;
+    __shared__ float s_part[kPartials];
+    __shared__ uint32_t s_done, s_last;
+    const int tid = threadIdx.x, lane = tid & 31;
     if(tid == 0) s_done = ctl->done;
     __syncthreads();
     if(s_done) return;
-    for(uint32_t w = tid; w < p.r2_words; w += 1024) rg.cur[w] = rg.nxt[w];
-    float part = 0.0f;
-    for(int r = tid; r < p.num_r1; r += 1024) {
-        const int nv = rg.valid[r];
-        float raw = 0.0f;
-        if(nv > 0) {  // Graph.cu:241-256 with an exact R2 popcount for the coverage
-            const int cnt = rg.counter[r];
-            const uint32_t pc = popcount_range(rg.nxt, (uint64_t)r * p.P, (uint64_t)(r + 1) * p.P);
-            const float cov = __fdiv_rn((float)pc, (float)p.P);
-            const float fnv = __fadd_rn(p.eps, (float)nv);
-            const float fv = __fmul_rn(__fdiv_rn(fnv, __fadd_rn(fnv, (float)(cnt - nv))), p.vol);
-            const float fv2 = __fmul_rn(fv, fv), fv4 = __fmul_rn(fv2, fv2), cf = (float)cnt;
-            raw = __fdiv_rn(fv4, __fmul_rn(__fadd_rn(1.0f, cov), __fadd_rn(1.0f, __fmul_rn(cf, cf))));
+    const uint32_t gtid = blockIdx.x * blockDim.x + tid, gsize = gridDim.x * blockDim.x;
+    for(uint32_t w = gtid; w < p.r2_words; w += gsize) rg.cur[w] = rg.nxt[w];
+    const int nwarps = gridDim.x * (kScoreBS / 32);
+    for(int j = blockIdx.x * (kScoreBS / 32) + (tid >> 5); j < kPartials; j += nwarps) {
+        float part = 0.0f;
+        for(int m0 = 0; j + kPartials * m0 < p.num_r1; m0 += 32) {
+            const int r = j + kPartials * (m0 + lane);
+            float contrib = 0.0f;
+            if(r < p.num_r1) {
+                const int nv = rg.valid[r];
+                float stored = -1.0f;  // region without valid samples: score 1
+                if(nv > 0) {           // Graph.cu:241-256, coverage from an exact R2 popcount
+                    const int cnt = rg.counter[r];
+                    const uint32_t pc = popcount_range(rg.nxt, (uint64_t)r * p.P, (uint64_t)(r + 1) * p.P);
+                    const float cov = __fdiv_rn((float)pc, (float)p.P);
+                    const float fnv = __fadd_rn(p.eps, (float)nv);
+                    const float fv = __fmul_rn(__fdiv_rn(fnv, __fadd_rn(fnv, (float)(cnt - nv))), p.vol);
+                    const float fv2 = __fmul_rn(fv, fv), fv4 = __fmul_rn(fv2, fv2), cf = (float)cnt;
+                    stored = contrib = __fdiv_rn(fv4, __fmul_rn(__fadd_rn(1.0f, cov), __fadd_rn(1.0f, __fmul_rn(cf, cf))));
+                }
+                rg.score[r] = stored;
+            }
+            for(int q = 0; q < 32; ++q) {
+                const float v = __shfl_sync(0xffffffffu, contrib, q);
+                if(j + kPartials * (m0 + q) < p.num_r1) part = __fadd_rn(part, v);
+            }
         }
-        rg.score[r] = raw;
-        part = __fadd_rn(part, raw);
+        if(lane == 0) partials[j] = part;
     }
-    s_part[tid] = part;
+    __threadfence();
     __syncthreads();
-    for(int s = 512; s > 0; s >>= 1) {
-        if(tid < s) s_part[tid] = __fadd_rn(s_part[tid], s_part[tid + s]);
+    if(tid == 0) s_last = atomicAdd(arrivals, 1u) == gridDim.x - 1u;
+    __syncthreads();
+    if(!s_last) return;
+    __threadfence();
+    for(int j = tid; j < kPartials; j += kScoreBS) s_part[j] = ((volatile float*)partials)[j];
+    __syncthreads();
+    for(int s = kPartials / 2; s > 0; s >>= 1) {
+        for(int j = tid; j < s; j += kScoreBS) s_part[j] = __fadd_rn(s_part[j], s_part[j + s]);
         __syncthreads();
     }
-    const float total = s_part[0];
-    for(int r = tid; r < p.num_r1; r += 1024)
-        rg.score[r] = rg.valid[r] == 0 ? 1.0f : __fadd_rn(p.eps, __fdiv_rn(rg.score[r], total));
     if(tid == 0) {
+        *arrivals = 0u;
+        ctl->score_total = s_part[0];
+        ctl->scores_ready = 1u;
         const uint32_t iter = ctl->iter, tree_old = ctl->tree, tree_new = tree_old + ctl->appended;
         ctl->tree_old = tree_old;
         ctl->tree = tree_new;
@@ -431,8 +542,8 @@ __global__ void k_reactivate(KParams p, TreeDev t, RegDev rg, const Ctl* ctl)
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t tree_old = ctl->tree_old;
     if(i >= tree_old || ctl->iters_done == 0u) return;
-    if(t.rep[i] == 0 && reactivate_draw(p, ctl->plan_idx, ctl->iter - 1u, i) <= __fadd_rn(rg.score[t.r1[i]], ctl->faccept))
-        t.rep[i] = 1;
+    const float sc = region_score(rg.score[t.r1[i]], ctl->score_total, ctl->scores_ready, p.eps);
+    if(t.rep[i] == 0 && reactivate_draw(p, ctl->plan_idx, ctl->iter - 1u, i) <= __fadd_rn(sc, ctl->faccept)) t.rep[i] = 1;
 }
 
 // Goal-to-root walk (KPAX.cu:482-501), goal row first, root row last.
@@ -490,6 +601,10 @@ struct kpax_planner {
     float* d_obs_host = nullptr;
     uint32_t obs_host_cap = 0;
     uint32_t* d_entries = nullptr;
+    uint32_t* d_tiles = nullptr;
+    uint32_t* d_farrivals = nullptr;
+    float* d_partials = nullptr;
+    uint32_t* d_arrivals = nullptr;
     unsigned long long *d_lb1 = nullptr, *d_lb2 = nullptr;
     uint32_t nblk1 = 0, nblk2 = 0;
     float* d_path = nullptr;
@@ -535,6 +650,11 @@ struct kpax_planner {
             return st;
         nblk1 = (p.cap + kTile - 1) / kTile;
         nblk2 = (p.budget + kExpandBS - 1) / kExpandBS;
+        if((st = alloc(&d_partials, kPartials)) || (st = alloc(&d_arrivals, 1)) || (st = alloc(&d_farrivals, 1)) ||
+           (st = alloc(&d_tiles, (p.cap + kTile - 1) / kTile + 1)))
+            return st;
+        KPAX_CUDA(cudaMemsetAsync(d_arrivals, 0, sizeof(uint32_t), stream));
+        KPAX_CUDA(cudaMemsetAsync(d_farrivals, 0, sizeof(uint32_t), stream));
         if((st = alloc(&d_entries, p.budget)) || (st = alloc(&d_lb1, nblk1)) || (st = alloc(&d_lb2, nblk2)) ||
            (st = alloc(&d_ctl, 1)) || (st = alloc(&d_init, 2 * (size_t)p.S)))
             return st;
@@ -597,7 +717,9 @@ struct kpax_planner {
     void launch_iteration(cudaEvent_t* ev = nullptr)
     {
         if(ev) cudaEventRecord(ev[0], stream);
-        k_frontier<<<nblk1, kFrontierBS, 0, stream>>>(p, tree, reg, d_ctl, d_entries, d_lb1);
+        const uint32_t fgrid = std::min<uint32_t>(nblk1, kFrontierCTAs);
+        k_frontier_count<<<fgrid, kFrontierBS, 0, stream>>>(p, tree, reg, d_ctl, d_tiles, d_farrivals);
+        k_frontier_write<<<fgrid, kFrontierBS, 0, stream>>>(p, tree, d_ctl, d_tiles, d_entries);
         if(ev) cudaEventRecord(ev[1], stream);
         const Grid g = env.view();
         switch(p.model) {
@@ -612,7 +734,7 @@ struct kpax_planner {
                 break;
         }
         if(ev) cudaEventRecord(ev[2], stream);
-        k_scores<<<1, 1024, 0, stream>>>(p, reg, d_ctl);
+        k_scores<<<kScoreCTAs, kScoreBS, 0, stream>>>(p, reg, d_ctl, d_partials, d_arrivals);
         if(ev) cudaEventRecord(ev[3], stream);
     }
 
@@ -648,7 +770,7 @@ struct kpax_planner {
             if(flush) KPAX_CUDA(cudaMemsetAsync(d_flush, (int)(i & 0xff), flush, stream));
             launch_iteration(&tev[4 * (size_t)i]);
             KPAX_CHECK_LAUNCH();
-            count_launch(3);
+            count_launch(4);
         }
         KPAX_CUDA(cudaStreamSynchronize(stream));
         for(uint32_t i = 0; i < n; ++i) {
@@ -718,12 +840,12 @@ struct kpax_planner {
         if(!poll) {
             for(uint32_t g = 0; g < guard; ++g) {
                 KPAX_CUDA(cudaGraphLaunch(graph, stream));
-                count_launch(3 * (uint64_t)unroll);
+                count_launch(4 * (uint64_t)unroll);
             }
         }
         for(uint32_t g = 0; poll && g < guard; ++g) {
             KPAX_CUDA(cudaGraphLaunch(graph, stream));
-            count_launch(3 * (uint64_t)unroll);
+            count_launch(4 * (uint64_t)unroll);
             KPAX_CUDA(cudaMemcpyAsync(h_ctl, d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, stream));
             KPAX_CUDA(cudaStreamSynchronize(stream));
             if(h_ctl->done) break;
@@ -915,8 +1037,17 @@ kpax_status kpax_export_regions(kpax_planner* pl, int32_t* h_counter, int32_t* h
     if(h_counter) KPAX_CUDA(cudaMemcpyAsync(h_counter, pl->reg.counter, sizeof(int32_t) * p.num_r1, cudaMemcpyDeviceToHost, pl->stream));
     if(h_valid) KPAX_CUDA(cudaMemcpyAsync(h_valid, pl->reg.valid, sizeof(int32_t) * p.num_r1, cudaMemcpyDeviceToHost, pl->stream));
     if(h_scores) KPAX_CUDA(cudaMemcpyAsync(h_scores, pl->reg.score, sizeof(float) * p.num_r1, cudaMemcpyDeviceToHost, pl->stream));
+    KPAX_CUDA(cudaMemcpyAsync(pl->h_ctl, pl->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, pl->stream));
     if(h_r2_bits) KPAX_CUDA(cudaMemcpyAsync(h_r2_bits, pl->reg.cur, sizeof(uint32_t) * p.r2_words, cudaMemcpyDeviceToHost, pl->stream));
     KPAX_CUDA(cudaStreamSynchronize(pl->stream));
+    if(h_scores) {  // stored raw (negative = no valid sample); normalised as region_score does
+        const float total = pl->h_ctl->score_total;
+        const bool ready = pl->h_ctl->scores_ready != 0u;
+        for(int r = 0; r < p.num_r1; ++r) {
+            const float raw = h_scores[r];
+            h_scores[r] = !ready ? 0.0f : (raw < 0.0f ? 1.0f : p.eps + raw / total);
+        }
+    }
     return KPAX_OK;
 }
 

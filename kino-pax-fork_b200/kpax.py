@@ -134,6 +134,7 @@ _SIGNATURES = {
     "kpax_collide_batch": (_I32, [_VP, _VP, _VP, _U32, _VP, _VP]),
     "kpax_region_batch": (_I32, [ctypes.POINTER(Config), _VP, _U32, _VP, _VP, _VP]),
     "kpax_kernel_launches": (ctypes.c_uint64, []),
+    "kpax_test_sincos": (_I32, [_VP, _U32, _VP, _VP]),
 }
 
 _lib = None

@@ -740,14 +740,21 @@ int ko_plan(const kpax_config* cfg, const float* init, const float* goal, const 
             if(k == 0) k = 1;
         }
         uint32_t E = (uint32_t)(R < B / k ? R : B / k), n = E * k;
-        /* entry list (repeatInd, Planner.cu:68-80) limited to E entries; expanded nodes leave
-         * the frontier (KPAX.cu:372) */
-        uint32_t e = 0;
-        for(uint32_t i = 0; i < tree && e < E; ++i) {
-            uint32_t cnt = rep[i];
+        if(R == 0) E = 0, n = 0;
+        /* entry list (repeatInd, Planner.cu:68-80).  Node i owns virtual entries [a, a + rep[i]).
+         * When the R entries exceed the budget (E < R, one child each), entry j is virtual entry
+         * floor(j * R / E): E entries evenly spaced over the whole frontier (the reference gives
+         * every entry at least one child instead, KPAX.cu:323-336).  A node leaves the frontier
+         * when at least one of its entries is taken (KPAX.cu:372). */
+        uint64_t a = 0;
+        for(uint32_t i = 0; i < tree; ++i) {
+            const uint32_t cnt = rep[i];
             if(!cnt) continue;
-            for(uint32_t j = 0; j < cnt && e < E; ++j) entry[e++] = i;
-            rep[i] = 0;
+            const uint64_t b = a + cnt;
+            const uint64_t lo = (a * E + R - 1) / R, hi = (b * E + R - 1) / R;
+            for(uint64_t j = lo; j < hi; ++j) entry[j] = i;
+            if(lo < hi) rep[i] = 0;
+            a = b;
         }
         memcpy(nxt, cur, sizeof(uint32_t) * words);
         /* propagateFrontier_kernel1 body (KPAX.cu:381-396) with snapshot R2 reads */

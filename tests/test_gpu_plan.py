@@ -120,15 +120,20 @@ def test_plan_without_obstacles_and_with_tiny_tree(cuda):
 
 
 def expected_parents(rep_after, tree, cfg):
-    """Frontier entries of the next iteration from the exported repeat counts (Planner.cu:68-80)."""
-    idx = np.repeat(np.arange(tree), rep_after[:tree].astype(np.int64))
-    R = idx.size
+    """Frontier entries of the next iteration from the exported repeat counts (Planner.cu:68-80):
+    with R entries and E taken, entry j is virtual entry floor(j*R/E); k children each."""
+    rep = rep_after[:tree].astype(np.int64)
+    R = int(rep.sum())
+    if R == 0:
+        return np.zeros(0, np.int64)
     B = min(cfg.expansions_per_iter, cfg.max_tree_size - tree)
     k = cfg.children_per_entry
     if R * k > B:
-        k = max(1, B // max(R, 1))
-    E_ = min(R, B // k)
-    return np.repeat(idx[:E_], k)
+        k = max(1, B // R)
+    E = min(R, B // k)
+    v = (np.arange(E, dtype=np.int64) * R) // E
+    node = np.searchsorted(np.cumsum(rep), v, side="right")
+    return np.repeat(node, k)
 
 
 @pytest.mark.parametrize("preset,scene", [(kpax.PRESET_QUAD, E.quad_scene), (kpax.PRESET_DUBINS, E.dubins_scene)])
