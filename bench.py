@@ -159,6 +159,19 @@ def cpu_reference_rate(cfg, obs, parents, budget_s: float, per_parent: int = 32,
                                             f"{t_total:.1f} s")
 
 
+def combine_over_ranks(dist, device, t_s: float, valid: float) -> tuple[float, float]:
+    """Replicas: the job time is the slowest rank's device time, the work is the sum over ranks."""
+    if dist is None:
+        return t_s, float(valid)
+    import torch
+
+    tt = torch.tensor([t_s], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    vv = torch.tensor([float(valid)], dtype=torch.float64, device=device)
+    dist.all_reduce(vv, op=dist.ReduceOp.SUM)
+    return float(tt.item()), float(vv.item())
+
+
 def dist_setup(n_gpus: int):
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -254,15 +267,7 @@ def run_ours(args) -> None:
     launches = kpax.kernel_launches() - launches0
     t_s = float(times[:, 0].sum()) / 1000.0
     t_exp = float(times[:, 2].sum()) / 1000.0
-    valid = tot["valid"]
-    if dist:
-        tt = torch.tensor([t_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        vv = torch.tensor([valid], dtype=torch.float64, device="cuda")
-        dist.all_reduce(vv, op=dist.ReduceOp.SUM)
-        t_s, valid_all = float(tt.item()), float(vv.item())
-    else:
-        valid_all = float(valid)
+    t_s, valid_all = combine_over_ranks(dist, "cuda", t_s, tot["valid"])
     value = valid_all / t_s
 
     # roofline of the expansion kernel: FP32 issue bound
