@@ -173,6 +173,29 @@ kpax_status kpax_export_children(kpax_planner* planner, float* h_rows, uint8_t* 
                                  int32_t* h_r1, int32_t* h_r2, uint8_t* h_next,
                                  int32_t* h_parent, uint32_t max_rows, uint32_t* n_children);
 
+/* ---- batches of independent queries (no counterpart in the reference, which plans one query
+ * per KPAX::plan call with a compile-time model) -------------------------------------------- */
+typedef struct kpax_batch kpax_batch;
+typedef struct kpax_batch_stats {
+    double ms;                  /* device time of the whole batch */
+    uint32_t iters;             /* iterations of the longest-running query */
+    uint32_t found;             /* queries that reached their goal */
+    uint64_t expansions, valid_expansions, steps;
+} kpax_batch_stats;
+/* One configuration per query (models, trees, budgets may differ).  All queries run every
+ * iteration stage in the same kernel launches: blocks index a query table. */
+kpax_status kpax_batch_create(const kpax_config* cfgs, uint32_t n, kpax_batch** out);
+kpax_status kpax_batch_destroy(kpax_batch* batch);
+/* h_inits / h_goals: n rows, row_stride floats apart (>= the largest SAMPLE_DIM).
+ * d_obstacles[q]: device buffer of n_obs[q] x 6 floats.  results[q].ms is the device time from
+ * the batch's start until query q finished (time to solution when results[q].found);
+ * results[q].h_path holds path_len rows of query q's own SAMPLE_DIM.  Every query of one call
+ * uses the same plan index in its random stream, so a query reproduces exactly what a single
+ * planner's plan with the same configuration and plan count gives. */
+kpax_status kpax_batch_plan(kpax_batch* batch, const float* h_inits, const float* h_goals,
+                            uint32_t row_stride, const float* const* d_obstacles,
+                            const uint32_t* n_obs, kpax_result* results, kpax_batch_stats* stats);
+
 /* ---- obstacle environment: uniform-grid spatial hash (spatialHash.cu:9-67) ------------- */
 /* Builds a compressed-sparse-row grid (no per-cell cap, deterministic ascending obstacle
  * order inside a cell) from a device obstacle buffer on `stream`. */

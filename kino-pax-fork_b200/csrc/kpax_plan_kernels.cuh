@@ -1,0 +1,630 @@
+// kpax_plan_kernels.cuh — the per-iteration kernels of the plan loop, over a batch of queries.
+//
+// One iteration of the reference (KPAX.cu:94-105) is propagateFrontier (303-351),
+// Graph::updateVertices (Graph.cu:207-227) and updateFrontier (520-543), with thrust scans over
+// the full tree capacity and ~6 host synchronisations.  Here it is four kernels with every size
+// on the device.  Each kernel serves many independent queries at once: blockIdx.y selects a
+// query (through an index list), whose parameters, buffers and control block are described by a
+// QueryDev copied into shared memory at block start.  A single plan is a batch of one.
+//   k_frontier_count  re-activation of the previous iteration (KPAX.cu:505-517) and repeat counts
+//                     of new nodes (476-479); tile sums; the last CTA scans them and sets the budget
+//   k_frontier_write  order-preserving entry list (Planner.cu:52-80), strided when the budget is
+//                     below the frontier; expanded nodes leave the frontier (KPAX.cu:372)
+//   k_expand<model>   per child: draw, RK4 + per-step collision, R1/R2 ids, counters, frontier
+//                     mark (KPAX.cu:381-396); stable append of accepted children with cost and
+//                     goal test (458-502) through a decoupled look-back
+//   k_scores          R2 snapshot update, region scores with a fixed-order total (Graph.cu:233-358),
+//                     then the iteration bookkeeping (tree size, fAccept, stop flags)
+// Deterministic replacements for the reference's races are listed in oracle/kpax_oracle.h.
+#pragma once
+#include <stdint.h>
+
+#include "kpax_device.cuh"
+
+namespace kpax {
+namespace plan {
+
+constexpr uint8_t kPending = 255;
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+constexpr int kFrontierBS = 256, kItems = 4, kTile = kFrontierBS * kItems;
+constexpr int kExpandBS = 448;  // 2^16 children over 148 SMs: one 14-warp block per SM
+constexpr int kScoreBS = 256, kPartials = 1024;
+constexpr uint32_t kSpinLimit = 1u << 22;  // ~4 s of polling before a wait gives up
+constexpr uint32_t kErrTimeout = 1u, kErrCapacity = 2u;
+
+struct TreeDev {
+    float4* s[3];  // state planes: floats 4k..4k+3 of every node
+    float4* ctl;   // controls as stored in the row
+    float* dur;
+    int32_t* parent;
+    float* cost;
+    int32_t* r1;
+    uint8_t* rep;  // frontier repeat count; 0 = not in frontier; kPending = added last iteration
+};
+
+struct RegDev {
+    int32_t* counter;
+    int32_t* valid;
+    float* score;   // raw score; negative = region without valid samples
+    uint32_t* cur;  // R2 activation bits as of the start of the iteration
+    uint32_t* nxt;  // R2 activation bits including this iteration
+};
+
+struct CaptureDev {
+    float* rows;
+    uint8_t* valid;
+    int32_t* r1;
+    int32_t* r2;
+    uint8_t* next;
+    int32_t* parent;
+};
+
+struct alignas(16) Ctl {
+    uint32_t tree, tree_old, iter, R, k, E, n, appended;
+    uint32_t goal_idx, done, full, error;
+    uint32_t plan_idx, max_iters, stop_at_goal, epoch;
+    uint32_t iters_done, path_len, scores_ready, pad0;
+    float faccept, goal[3];
+    float score_total, pad1[3];
+    unsigned long long n_exp, n_valid, n_steps;
+    unsigned long long t_begin_ns, t_done_ns;
+    double path_cost;
+};
+
+// Everything a kernel needs about one query.
+struct alignas(16) QueryDev {
+    KParams p;
+    Grid g;
+    TreeDev t;
+    RegDev rg;
+    CaptureDev cap;
+    Ctl* ctl;
+    uint32_t* entries;
+    uint32_t* tiles;      // tile sums, then their exclusive prefixes
+    uint32_t* farr;       // arrival counter of k_frontier_count
+    unsigned long long* lb;  // look-back status of k_expand, one per block
+    float* partials;      // kPartials partial score sums
+    uint32_t* sarr;       // arrival counter of k_scores
+    float* path;
+    const float* init_goal;  // init row then goal row, S floats each
+    uint32_t path_rows, pad[3];
+};
+
+__device__ __forceinline__ unsigned long long globaltimer()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Copies the block's query descriptor into shared memory (all threads call it).
+__device__ __forceinline__ void load_query(const QueryDev* __restrict__ qs, const uint32_t* __restrict__ qidx, QueryDev& sq)
+{
+    const uint32_t q = qidx ? qidx[blockIdx.y] : blockIdx.y;
+    const uint4* src = reinterpret_cast<const uint4*>(qs + q);
+    uint4* dst = reinterpret_cast<uint4*>(&sq);
+    for(int i = threadIdx.x; i < (int)(sizeof(QueryDev) / 16); i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+}
+
+// Marks a query finished; the first transition counts it off the batch's active count.
+__device__ __forceinline__ void finish_query(Ctl* ctl, uint32_t* active)
+{
+    if(atomicExch(&ctl->done, 1u) == 0u) {
+        ctl->t_done_ns = globaltimer();
+        if(active) atomicSub(active, 1u);
+    }
+}
+
+// Status word: [epoch:30 | flag:2 | value:32]; flag 1 = block aggregate, 2 = inclusive prefix.
+__device__ __forceinline__ void lb_publish(unsigned long long* slot, uint32_t epoch, uint32_t flag, uint32_t value)
+{
+    const unsigned long long w = ((unsigned long long)(epoch & 0x3FFFFFFFu) << 34) | ((unsigned long long)flag << 32) | value;
+    __threadfence();
+    atomicExch(slot, w);
+}
+
+// Exclusive prefix of tile b, computed by the 32 lanes of one warp: each probe reads the status
+// of 32 predecessors at once and stops at the nearest inclusive prefix.  Returns false when a
+// predecessor never published (bounded wait).
+__device__ __forceinline__ bool lb_exclusive(unsigned long long* lb, uint32_t b, uint32_t epoch, uint32_t& excl)
+{
+    const uint32_t tag = epoch & 0x3FFFFFFFu;
+    const int lane = threadIdx.x & 31;
+    uint32_t acc = 0, spins = 0;
+    int top = (int)b - 1;
+    while(top >= 0) {
+        const int j = top - lane;  // lane 0 probes the nearest predecessor
+        uint32_t flag = 2u, val = 0u;  // past tile 0: an inclusive prefix of zero
+        if(j >= 0) {
+            const unsigned long long w = atomicAdd(lb + j, 0ull);
+            flag = (uint32_t)(w >> 34) == tag ? (uint32_t)(w >> 32) & 3u : 0u;
+            val = (uint32_t)w;
+        }
+        const uint32_t ready = __ballot_sync(0xffffffffu, flag != 0u), incl = __ballot_sync(0xffffffffu, flag == 2u);
+        const int first = incl ? __ffs(incl) - 1 : 31;
+        const uint32_t need = first == 31 ? 0xffffffffu : ((2u << first) - 1u);
+        if((ready & need) != need) {
+            if(++spins > kSpinLimit) {
+                excl = acc;
+                return false;
+            }
+            if(spins > 32) __nanosleep(100);
+            continue;
+        }
+        uint32_t v = lane <= first ? val : 0u;
+#pragma unroll
+        for(int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+        acc += v;
+        if(incl) break;
+        top -= 32;
+    }
+    excl = acc;
+    return true;
+}
+
+__device__ __forceinline__ uint32_t popcount_range(const uint32_t* __restrict__ bits, uint64_t lo, uint64_t hi)
+{
+    uint32_t n = 0;
+    const uint64_t w0 = lo >> 5, w1 = (hi - 1) >> 5;
+    for(uint64_t w = w0; w <= w1; ++w) {
+        uint32_t m = bits[w];
+        if(w == w0) m &= ~0u << (lo & 31);
+        if(w == w1) {
+            const uint32_t top = (uint32_t)((hi - 1) & 31);
+            m &= top == 31 ? ~0u : ((1u << (top + 1)) - 1u);
+        }
+        n += __popc(m);
+    }
+    return n;
+}
+
+// Normalised score of a region (Graph.cu:297-304, 349-357) from its stored raw score; every
+// score reads 0 before the first score pass of a plan (KPAX.cu:69).
+__device__ __forceinline__ float region_score(float raw, float total, uint32_t ready, float eps)
+{
+    if(!ready) return 0.0f;
+    return raw < 0.0f ? 1.0f : __fadd_rn(eps, __fdiv_rn(raw, total));
+}
+
+template <int SD>
+__device__ __forceinline__ void load_state(const TreeDev& t, uint32_t i, float* s)
+{
+    const float4 a = t.s[0][i], b = t.s[1][i];
+    s[0] = a.x, s[1] = a.y, s[2] = a.z, s[3] = a.w, s[4] = b.x, s[5] = b.y;
+    if constexpr(SD == 12) {
+        const float4 c = t.s[2][i];
+        s[6] = b.z, s[7] = b.w, s[8] = c.x, s[9] = c.y, s[10] = c.z, s[11] = c.w;
+    }
+}
+
+template <int SD>
+__device__ __forceinline__ void store_state(const TreeDev& t, uint32_t i, const float* s)
+{
+    if constexpr(SD == 12) {
+        t.s[0][i] = make_float4(s[0], s[1], s[2], s[3]);
+        t.s[1][i] = make_float4(s[4], s[5], s[6], s[7]);
+        t.s[2][i] = make_float4(s[8], s[9], s[10], s[11]);
+    } else {
+        t.s[0][i] = make_float4(s[0], s[1], s[2], s[3]);
+        t.s[1][i] = make_float4(s[4], s[5], 0.0f, 0.0f);
+    }
+}
+
+__device__ __forceinline__ float goal_distance(const float* s, const float* g)
+{
+    const float dx = __fsub_rn(s[0], g[0]), dy = __fsub_rn(s[1], g[1]), dz = __fsub_rn(s[2], g[2]);
+    return __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)));
+}
+
+// ---------------------------------------------------------------- kernels
+
+// Root node and control block of each query (KPAX.cu:59-91).
+__global__ void k_begin(const QueryDev* __restrict__ qs, uint32_t plan_base, uint32_t max_iters, uint32_t stop_at_goal)
+{
+    __shared__ QueryDev sq;
+    load_query(qs, nullptr, sq);
+    if(threadIdx.x != 0) return;
+    const KParams& p = sq.p;
+    const TreeDev& t = sq.t;
+    const float* ig = sq.init_goal;
+    float s[12] = {0};
+    for(int k = 0; k < p.sd; ++k) s[k] = ig[k];
+    if(p.sd == 12) store_state<12>(t, 0, s);
+    else store_state<6>(t, 0, s);
+    float c[4] = {0, 0, 0, 0};
+    for(int k = 0; k < p.cd; ++k) c[k] = ig[p.sd + k];
+    t.ctl[0] = make_float4(c[0], c[1], c[2], c[3]);
+    t.dur[0] = ig[p.S - 1];
+    t.parent[0] = -1;
+    t.cost[0] = 0.0f;
+    t.r1[0] = region_r1(p, s);
+    t.rep[0] = (uint8_t)p.root_repeat;
+    Ctl* ctl = sq.ctl;
+    const uint32_t epoch = ctl->epoch + 1;
+    Ctl z;
+    memset(&z, 0, sizeof(z));
+    z.tree = 1, z.tree_old = 0, z.iter = 1, z.goal_idx = kNone;
+    z.plan_idx = plan_base, z.max_iters = max_iters, z.stop_at_goal = stop_at_goal, z.epoch = epoch;
+    z.goal[0] = ig[p.S], z.goal[1] = ig[p.S + 1], z.goal[2] = ig[p.S + 2];
+    z.t_begin_ns = globaltimer();
+    *ctl = z;
+}
+
+__device__ __forceinline__ uint32_t resolve_repeat(const KParams& p, const TreeDev& t, const RegDev& rg, uint32_t i,
+                                                   uint32_t tree_old, uint32_t iter, uint32_t plan, float fa, float total,
+                                                   uint32_t ready)
+{
+    const uint32_t r0 = t.rep[i];
+    uint32_t r = r0;
+    if(r == 0u) {  // re-activation of the previous iteration (KPAX.cu:505-517)
+        if(i < tree_old) {
+            const float sc = region_score(rg.score[t.r1[i]], total, ready, p.eps);
+            if(reactivate_draw(p, plan, iter - 1u, i) <= __fadd_rn(sc, fa)) r = 1u;
+        }
+    } else if(r == kPending) {  // repeat of a node added last iteration (KPAX.cu:476-479)
+        r = rg.valid[t.r1[i]] < p.sparse_thr ? p.sparse_repeat : 1u;
+    }
+    if(r != r0) t.rep[i] = (uint8_t)r;
+    return r;
+}
+
+__global__ void __launch_bounds__(kFrontierBS) k_frontier_count(const QueryDev* __restrict__ qs, uint32_t* __restrict__ active)
+{
+    __shared__ QueryDev sq;
+    __shared__ uint32_t s_last, s_carry;
+    __shared__ uint32_t s_warp[kFrontierBS / 32];
+    load_query(qs, nullptr, sq);
+    const KParams& p = sq.p;
+    Ctl* ctl = sq.ctl;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if(ctl->done) return;
+    const uint32_t tree = ctl->tree, tree_old = ctl->tree_old, iter = ctl->iter, plan = ctl->plan_idx;
+    const uint32_t ready = ctl->scores_ready;
+    const float fa = ctl->faccept, total = ctl->score_total;
+    const uint32_t ntiles = (tree + kTile - 1) / kTile;
+    for(uint32_t b = blockIdx.x; b < ntiles; b += gridDim.x) {
+        uint32_t sum = 0;
+#pragma unroll
+        for(int j = 0; j < kItems; ++j) {
+            const uint32_t i = b * kTile + j * kFrontierBS + threadIdx.x;  // coalesced
+            if(i < tree) sum += resolve_repeat(p, sq.t, sq.rg, i, tree_old, iter, plan, fa, total, ready);
+        }
+#pragma unroll
+        for(int d = 16; d > 0; d >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, d);
+        if(lane == 0) s_warp[warp] = sum;
+        __syncthreads();
+        if(threadIdx.x == 0) {
+            uint32_t acc = 0;
+            for(int w = 0; w < kFrontierBS / 32; ++w) acc += s_warp[w];
+            sq.tiles[b] = acc;
+        }
+        __syncthreads();
+    }
+    __threadfence();
+    __syncthreads();
+    if(threadIdx.x == 0) s_last = atomicAdd(sq.farr, 1u) == gridDim.x - 1u;
+    __syncthreads();
+    if(!s_last) return;
+    __threadfence();
+    // exclusive scan of the tile sums in place, kFrontierBS at a time; total R
+    if(threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    volatile uint32_t* ts = sq.tiles;
+    for(uint32_t base = 0; base < ntiles; base += kFrontierBS) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t v = i < ntiles ? ts[i] : 0u;
+        uint32_t x = v;
+#pragma unroll
+        for(int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+            if(lane >= d) x += y;
+        }
+        if(lane == 31) s_warp[warp] = x;
+        __syncthreads();
+        uint32_t wex = 0;
+        for(int w = 0; w < warp; ++w) wex += s_warp[w];
+        const uint32_t excl = s_carry + wex + x - v;
+        if(i < ntiles) ts[i] = excl;
+        __syncthreads();
+        if(threadIdx.x == kFrontierBS - 1) s_carry = excl + v;
+        __syncthreads();
+    }
+    if(threadIdx.x == 0) {  // the budget of this iteration (KPAX.cu:323-350)
+        *sq.farr = 0u;
+        const uint64_t R = s_carry;
+        const uint32_t B = min(p.budget, p.cap - tree);
+        uint32_t k = p.per_entry, E = 0, n = 0;
+        if(B == 0) {
+            ctl->full = 1u;
+            finish_query(ctl, active);
+        } else if(R) {
+            if(R * k > B) {
+                k = (uint32_t)(B / R);
+                if(k == 0) k = 1;
+            }
+            E = (uint32_t)(R < (uint64_t)(B / k) ? R : (uint64_t)(B / k));
+            n = E * k;
+        }
+        ctl->R = (uint32_t)R;
+        ctl->k = k, ctl->E = E, ctl->n = n;
+    }
+}
+
+// Node i owns virtual entries [a, a + rep) with a from the tile scan.  Entry j of the E taken is
+// virtual entry floor(j*R/E): node i writes entries ceil(a*E/R) .. ceil((a+rep)*E/R) - 1 (all of
+// its entries when E == R).  Nodes with an entry taken leave the frontier.
+__global__ void __launch_bounds__(kFrontierBS) k_frontier_write(const QueryDev* __restrict__ qs)
+{
+    __shared__ QueryDev sq;
+    __shared__ uint32_t s_warp[kFrontierBS / 32];
+    load_query(qs, nullptr, sq);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    Ctl* ctl = sq.ctl;
+    if(ctl->done) return;
+    const uint32_t tree = ctl->tree, E = ctl->E;
+    const uint64_t R = ctl->R;
+    if(E == 0) return;
+    const uint32_t ntiles = (tree + kTile - 1) / kTile;
+    const TreeDev& t = sq.t;
+    for(uint32_t b = blockIdx.x; b < ntiles; b += gridDim.x) {
+        const uint32_t i0 = b * kTile + threadIdx.x * kItems;  // consecutive nodes per thread
+        uint32_t cnt[kItems], sum = 0;
+#pragma unroll
+        for(int j = 0; j < kItems; ++j) {
+            const uint32_t i = i0 + j;
+            cnt[j] = i < tree ? (uint32_t)t.rep[i] : 0u;
+            sum += cnt[j];
+        }
+        uint32_t x = sum;
+#pragma unroll
+        for(int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+            if(lane >= d) x += y;
+        }
+        if(lane == 31) s_warp[warp] = x;
+        __syncthreads();
+        uint32_t wex = 0;
+        for(int w = 0; w < warp; ++w) wex += s_warp[w];
+        uint64_t a = (uint64_t)sq.tiles[b] + wex + x - sum;
+#pragma unroll
+        for(int j = 0; j < kItems; ++j) {
+            if(!cnt[j]) continue;
+            const uint64_t bnd = a + cnt[j];
+            const uint64_t lo = (a * E + R - 1) / R, hi = (bnd * E + R - 1) / R;
+            for(uint64_t e = lo; e < hi; ++e) sq.entries[e] = i0 + j;
+            if(lo < hi) t.rep[i0 + j] = 0;
+            a = bnd;
+        }
+        __syncthreads();
+    }
+}
+
+template <int M>
+__global__ void __launch_bounds__(kExpandBS) k_expand(const QueryDev* __restrict__ qs, const uint32_t* __restrict__ qidx,
+                                                      uint32_t* __restrict__ active)
+{
+    constexpr int SD = ModelDims<M>::SD, CD = ModelDims<M>::CD, S = SD + CD + 1;
+    constexpr int NW = kExpandBS / 32;
+    __shared__ QueryDev sq;
+    __shared__ uint32_t s_excl, s_ok;
+    __shared__ uint32_t s_wn[NW], s_wv[NW], s_ws[NW];
+    load_query(qs, qidx, sq);
+    const KParams& p = sq.p;
+    Ctl* ctl = sq.ctl;
+    if(ctl->done) return;
+    const uint32_t n = ctl->n, k = ctl->k, tree = ctl->tree, iter = ctl->iter, plan = ctl->plan_idx, epoch = ctl->epoch;
+    const uint32_t ready = ctl->scores_ready;
+    const float total = ctl->score_total;
+    const uint32_t nblk = n ? (n + kExpandBS - 1) / kExpandBS : 1u, b = blockIdx.x;
+    if(b >= nblk) return;
+    const TreeDev& t = sq.t;
+    const RegDev& rg = sq.rg;
+    const uint32_t c = b * kExpandBS + threadIdx.x;
+    const bool active_child = c < n;
+    bool valid = false, next = false;
+    float s[SD], cc[4], rc[4], u[6];
+    uint32_t parent = 0;
+    int r1v = 0, r2v = 0, steps = 0, steps_done = 0;
+    if(active_child) {
+        parent = sq.entries[c / k];
+        load_state<SD>(t, parent, s);
+        child_draws(p, plan, iter, c, u);
+        steps = draw_controls(p, u, cc);
+        valid = propagate<M>(p, sq.g, s, cc, steps, steps_done);
+        r1v = region_r1(p, s);
+        r2v = region_r2(p, s, r1v);
+        atomicAdd(rg.counter + r1v, 1);
+        if(valid) {
+            atomicAdd(rg.valid + r1v, 1);
+            const uint32_t word = (uint32_t)r2v >> 5, bit = 1u << (r2v & 31);
+            const bool seen = (__ldg(rg.cur + word) & bit) != 0u;
+            next = (u[5] < region_score(__ldg(rg.score + r1v), total, ready, p.eps)) || !seen;
+            atomicOr(rg.nxt + word, bit);
+        }
+        row_controls<M>(cc, rc);
+        if(sq.cap.rows) {
+            float* dst = sq.cap.rows + (size_t)c * S;
+            for(int q = 0; q < SD; ++q) dst[q] = s[q];
+            for(int q = 0; q < CD; ++q) dst[SD + q] = rc[q];
+            dst[SD + CD] = __fmul_rn(p.h, (float)steps);
+            sq.cap.valid[c] = valid, sq.cap.r1[c] = r1v, sq.cap.r2[c] = r2v, sq.cap.next[c] = next;
+            sq.cap.parent[c] = (int32_t)parent;
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t mn = __ballot_sync(0xffffffffu, next), mv = __ballot_sync(0xffffffffu, valid);
+    const uint32_t rank = __popc(mn & ((1u << lane) - 1u));
+    uint32_t wsteps = active_child ? (uint32_t)steps_done : 0u;  // RK4 steps executed (algorithmic work)
+#pragma unroll
+    for(int d = 16; d > 0; d >>= 1) wsteps += __shfl_xor_sync(0xffffffffu, wsteps, d);
+    if(lane == 0) s_wn[warp] = __popc(mn), s_wv[warp] = __popc(mv), s_ws[warp] = wsteps;
+    __syncthreads();
+    if(warp == 0) {
+        uint32_t acc = 0, nv = 0;
+        unsigned long long ns = 0;
+        for(int w = 0; w < NW; ++w) acc += s_wn[w], nv += s_wv[w], ns += s_ws[w];
+        uint32_t excl = 0;
+        bool ok = true;
+        if(b == 0) {
+            if(lane == 0) lb_publish(sq.lb, epoch, 2u, acc);
+        } else {
+            if(lane == 0) lb_publish(sq.lb + b, epoch, 1u, acc);
+            ok = lb_exclusive(sq.lb, b, epoch, excl);
+            if(ok && lane == 0) lb_publish(sq.lb + b, epoch, 2u, excl + acc);
+        }
+        if(lane == 0) {
+            if(nv) atomicAdd(&ctl->n_valid, (unsigned long long)nv);
+            if(ns) atomicAdd(&ctl->n_steps, ns);
+            if(!ok) {
+                atomicOr(&ctl->error, kErrTimeout);
+                finish_query(ctl, active);
+            }
+            if(ok && b == nblk - 1) ctl->appended = excl + acc;
+            s_excl = excl;
+            s_ok = ok;
+        }
+    }
+    __syncthreads();
+    if(!next || !s_ok) return;
+    uint32_t wex = 0;  // accepted children of the lower warps of this block
+    for(int w = 0; w < warp; ++w) wex += s_wn[w];
+    const uint32_t slot = tree + s_excl + wex + rank;
+    if(slot >= p.cap) {
+        atomicOr(&ctl->error, kErrCapacity);
+        return;
+    }
+    store_state<SD>(t, slot, s);
+    t.ctl[slot] = make_float4(rc[0], rc[1], rc[2], rc[3]);
+    t.dur[slot] = __fmul_rn(p.h, (float)steps);
+    t.parent[slot] = (int32_t)parent;
+    const float d = goal_distance(s, ctl->goal);
+    t.cost[slot] = d;
+    t.r1[slot] = r1v;
+    t.rep[slot] = kPending;
+    if(d < p.goal_thresh) atomicMin(&ctl->goal_idx, slot);
+}
+
+// Region scores (Graph.cu:233-358): one warp per partial sum j, lane m scoring region j + 1024*m,
+// summed in ascending region order; the last CTA adds the 1024 partials with a fixed halving
+// tree, so the total (and every normalised score) is bit-identical to the oracle's.  Raw scores
+// are stored (negative = no valid sample) and normalised where they are read (region_score).
+__global__ void __launch_bounds__(kScoreBS) k_scores(const QueryDev* __restrict__ qs, uint32_t* __restrict__ active)
+{
+    __shared__ QueryDev sq;
+    __shared__ float s_part[kPartials];
+    __shared__ uint32_t s_last;
+    load_query(qs, nullptr, sq);
+    const KParams& p = sq.p;
+    const RegDev& rg = sq.rg;
+    Ctl* ctl = sq.ctl;
+    const int tid = threadIdx.x, lane = tid & 31;
+    if(ctl->done) return;
+    const uint32_t gtid = blockIdx.x * blockDim.x + tid, gsize = gridDim.x * blockDim.x;
+    for(uint32_t w = gtid; w < p.r2_words; w += gsize) rg.cur[w] = rg.nxt[w];
+    const int nwarps = gridDim.x * (kScoreBS / 32);
+    for(int j = blockIdx.x * (kScoreBS / 32) + (tid >> 5); j < kPartials; j += nwarps) {
+        float part = 0.0f;
+        for(int m0 = 0; j + kPartials * m0 < p.num_r1; m0 += 32) {
+            const int r = j + kPartials * (m0 + lane);
+            float contrib = 0.0f;
+            if(r < p.num_r1) {
+                const int nv = rg.valid[r];
+                float stored = -1.0f;  // region without valid samples: score 1
+                if(nv > 0) {           // Graph.cu:241-256, coverage from an exact R2 popcount
+                    const int cnt = rg.counter[r];
+                    const uint32_t pc = popcount_range(rg.nxt, (uint64_t)r * p.P, (uint64_t)(r + 1) * p.P);
+                    const float cov = __fdiv_rn((float)pc, (float)p.P);
+                    const float fnv = __fadd_rn(p.eps, (float)nv);
+                    const float fv = __fmul_rn(__fdiv_rn(fnv, __fadd_rn(fnv, (float)(cnt - nv))), p.vol);
+                    const float fv2 = __fmul_rn(fv, fv), fv4 = __fmul_rn(fv2, fv2), cf = (float)cnt;
+                    stored = contrib = __fdiv_rn(fv4, __fmul_rn(__fadd_rn(1.0f, cov), __fadd_rn(1.0f, __fmul_rn(cf, cf))));
+                }
+                rg.score[r] = stored;
+            }
+            for(int q = 0; q < 32; ++q) {
+                const float v = __shfl_sync(0xffffffffu, contrib, q);
+                if(j + kPartials * (m0 + q) < p.num_r1) part = __fadd_rn(part, v);
+            }
+        }
+        if(lane == 0) sq.partials[j] = part;
+    }
+    __threadfence();
+    __syncthreads();
+    if(tid == 0) s_last = atomicAdd(sq.sarr, 1u) == gridDim.x - 1u;
+    __syncthreads();
+    if(!s_last) return;
+    __threadfence();
+    for(int j = tid; j < kPartials; j += kScoreBS) s_part[j] = ((volatile float*)sq.partials)[j];
+    __syncthreads();
+    for(int s = kPartials / 2; s > 0; s >>= 1) {
+        for(int j = tid; j < s; j += kScoreBS) s_part[j] = __fadd_rn(s_part[j], s_part[j + s]);
+        __syncthreads();
+    }
+    if(tid == 0) {
+        *sq.sarr = 0u;
+        ctl->score_total = s_part[0];
+        ctl->scores_ready = 1u;
+        const uint32_t iter = ctl->iter, tree_old = ctl->tree, tree_new = tree_old + ctl->appended;
+        ctl->tree_old = tree_old;
+        ctl->tree = tree_new;
+        const float a = __fsub_rn(1.0f, __fdiv_rn((float)tree_new, (float)p.cap));  // KPAX.cu:527-528
+        const float a2 = __fmul_rn(a, a), a4 = __fmul_rn(a2, a2), a5 = __fmul_rn(a4, a);
+        ctl->faccept = __fmul_rn(__fmul_rn((float)iter, p.eps), a5);
+        ctl->n_exp += ctl->n;
+        ctl->iters_done = iter;
+        ctl->iter = iter + 1u;
+        ctl->epoch = ctl->epoch + 1u;
+        if((ctl->goal_idx != kNone && ctl->stop_at_goal) || iter >= ctl->max_iters) finish_query(ctl, active);
+    }
+}
+
+// Re-activation of the last iteration without a scan (makes exported frontier flags final).
+__global__ void k_reactivate(const QueryDev* __restrict__ qs)
+{
+    __shared__ QueryDev sq;
+    load_query(qs, nullptr, sq);
+    const KParams& p = sq.p;
+    const Ctl* ctl = sq.ctl;
+    const uint32_t tree_old = ctl->tree_old;
+    if(ctl->iters_done == 0u) return;
+    for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < tree_old; i += gridDim.x * blockDim.x) {
+        const float sc = region_score(sq.rg.score[sq.t.r1[i]], ctl->score_total, ctl->scores_ready, p.eps);
+        if(sq.t.rep[i] == 0 && reactivate_draw(p, ctl->plan_idx, ctl->iter - 1u, i) <= __fadd_rn(sc, ctl->faccept))
+            sq.t.rep[i] = 1;
+    }
+}
+
+// Goal-to-root walk (KPAX.cu:482-501), goal row first, root row last.
+__global__ void k_path(const QueryDev* __restrict__ qs)
+{
+    __shared__ QueryDev sq;
+    load_query(qs, nullptr, sq);
+    if(threadIdx.x != 0) return;
+    const KParams& p = sq.p;
+    const TreeDev& t = sq.t;
+    Ctl* ctl = sq.ctl;
+    int32_t node = ctl->goal_idx == kNone ? -1 : (int32_t)ctl->goal_idx;
+    uint32_t len = 0;
+    double cost = 0.0;
+    while(node >= 0 && len < sq.path_rows) {
+        float s[12] = {0};
+        if(p.sd == 12) load_state<12>(t, (uint32_t)node, s);
+        else load_state<6>(t, (uint32_t)node, s);
+        const float4 c = t.ctl[node];
+        const float cv[4] = {c.x, c.y, c.z, c.w};
+        float* dst = sq.path + (size_t)len * p.S;
+        for(int k = 0; k < p.sd; ++k) dst[k] = s[k];
+        for(int k = 0; k < p.cd; ++k) dst[p.sd + k] = cv[k];
+        dst[p.S - 1] = t.dur[node];
+        const int32_t par = t.parent[node];
+        if(par >= 0) cost += (double)t.dur[node];
+        ++len;
+        node = par;
+    }
+    ctl->path_len = len;
+    ctl->path_cost = cost;
+}
+
+}  // namespace plan
+}  // namespace kpax

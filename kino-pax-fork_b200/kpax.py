@@ -99,6 +99,11 @@ class Result(ctypes.Structure):
     ]
 
 
+class BatchStats(ctypes.Structure):
+    _fields_ = [("ms", ctypes.c_double), ("iters", ctypes.c_uint32), ("found", ctypes.c_uint32),
+                ("expansions", ctypes.c_uint64), ("valid_expansions", ctypes.c_uint64), ("steps", ctypes.c_uint64)]
+
+
 class IterTiming(ctypes.Structure):
     _fields_ = [("ms_total", ctypes.c_float), ("ms_frontier", ctypes.c_float), ("ms_expand", ctypes.c_float),
                 ("ms_scores", ctypes.c_float)]
@@ -134,6 +139,9 @@ _SIGNATURES = {
     "kpax_collide_batch": (_I32, [_VP, _VP, _VP, _U32, _VP, _VP]),
     "kpax_region_batch": (_I32, [ctypes.POINTER(Config), _VP, _U32, _VP, _VP, _VP]),
     "kpax_kernel_launches": (ctypes.c_uint64, []),
+    "kpax_batch_create": (_I32, [_VP, _U32, ctypes.POINTER(_VP)]),
+    "kpax_batch_destroy": (_I32, [_VP]),
+    "kpax_batch_plan": (_I32, [_VP, _VP, _VP, _U32, _VP, _VP, _VP, ctypes.POINTER(BatchStats)]),
     "kpax_test_sincos": (_I32, [_VP, _U32, _VP, _VP]),
 }
 
@@ -357,6 +365,55 @@ class KPAX:
     def close(self) -> None:
         if self._h:
             load().kpax_destroy(self._h)
+            self._h = _VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many independent queries planned together: every iteration stage is one launch per kernel
+    over all queries (models may differ between queries)."""
+
+    def __init__(self, cfgs):
+        self.cfgs = [c.copy() for c in cfgs]
+        arr = (Config * len(self.cfgs))(*self.cfgs)
+        self._h = _VP()
+        check(load().kpax_batch_create(ctypes.addressof(arr), len(self.cfgs), ctypes.byref(self._h)), "kpax_batch_create")
+        self.n = len(self.cfgs)
+        self.stride = max(c.sample_dim for c in self.cfgs)
+
+    def plan(self, starts, goals, d_obstacles, n_obs):
+        """starts/goals: per-query state vectors; d_obstacles: device pointers; n_obs: counts."""
+        S = self.stride
+        init = np.zeros((self.n, S), np.float32)
+        goal = np.zeros((self.n, S), np.float32)
+        for q in range(self.n):
+            a, b = np.asarray(starts[q], np.float32).ravel(), np.asarray(goals[q], np.float32).ravel()
+            init[q, : min(S, a.size)] = a[:S]
+            goal[q, : min(S, b.size)] = b[:S]
+        ptrs = (ctypes.c_void_p * self.n)(*[int(p) for p in d_obstacles])
+        counts = np.ascontiguousarray(n_obs, np.uint32)
+        res = (Result * self.n)()
+        stats = BatchStats()
+        check(load().kpax_batch_plan(self._h, _ptr(init), _ptr(goal), S, ctypes.addressof(ptrs), _ptr(counts),
+                                     ctypes.addressof(res), ctypes.byref(stats)), "kpax_batch_plan")
+        out = []
+        for q in range(self.n):
+            r = res[q]
+            sd = self.cfgs[q].sample_dim
+            path = (np.ctypeslib.as_array(r.h_path, shape=(r.path_len * sd,)).reshape(r.path_len, sd).copy()
+                    if r.path_len else np.zeros((0, sd), np.float32))
+            out.append({f: getattr(r, f) for f in ("found", "goal_idx", "path_len", "tree_size", "iters", "tree_full", "ms",
+                                                     "expansions", "valid_expansions", "path_cost")} | {"path": path})
+        return out, {f: getattr(stats, f) for f in ("ms", "iters", "found", "expansions", "valid_expansions", "steps")}
+
+    def close(self) -> None:
+        if self._h:
+            load().kpax_batch_destroy(self._h)
             self._h = _VP()
 
     def __del__(self):
