@@ -331,19 +331,98 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+def batch_configs(queries):
+    """One configuration per batched query: its model's preset with the query's tree budget."""
+    pre = {kpax.MODEL_DOUBLE_INTEGRATOR: kpax.PRESET_DI, kpax.MODEL_DUBINS_AIRPLANE: kpax.PRESET_DUBINS,
+           kpax.MODEL_QUADROTOR: kpax.PRESET_QUAD}
+    cfgs = []
+    for q, d in enumerate(queries):
+        c = kpax.preset(pre[d["model"]])
+        c.max_tree_size = d["tree"]
+        c.expansions_per_iter = min(c.expansions_per_iter, c.max_tree_size)
+        c.seed = c.seed + 7919 * q
+        cfgs.append(c)
+    return cfgs
+
+
+def run_batch(args) -> None:
+    """Many independent queries per launch: each step plans the whole batch once."""
+    import torch
+
+    ws, rank, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    queries = E.batch_queries(args.queries, seed=4 + 1000 * rank)
+    cfgs = batch_configs(queries)
+    sizes = [d["obstacles"].shape[0] for d in queries]
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    h_obs = torch.from_numpy(np.concatenate([d["obstacles"] for d in queries])).pin_memory()
+    d_obs = torch.empty_like(h_obs, device="cuda")
+    ptrs = [d_obs.data_ptr() + 24 * int(o) for o in offs[:-1]]
+    starts, goals = [d["start"] for d in queries], [d["goal"] for d in queries]
+    batch = kpax.Batch(cfgs)
+    d_obs.copy_(h_obs)
+    for _ in range(args.warmup):
+        batch.plan(starts, goals, ptrs, sizes)
+    launches0 = kpax.kernel_launches()
+    tot_ms, tot_valid, wall, tts, found, n_plans = 0.0, 0, 0.0, [], 0, 0
+    per_model = {m: [0, 0] for m in (1, 2, 3)}
+    with Clocks(local) as clk:
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            d_obs.copy_(h_obs, non_blocking=True)  # host -> device inside the timed region
+            res, st = batch.plan(starts, goals, ptrs, sizes)
+            wall += time.perf_counter() - t0
+            tot_ms += st["ms"]
+            tot_valid += st["valid_expansions"]
+            n_plans += len(res)
+            for d, r in zip(queries, res):
+                per_model[d["model"]][0] += 1
+                if r["found"]:
+                    found += 1
+                    per_model[d["model"]][1] += 1
+                    tts.append(r["ms"])
+    launches = kpax.kernel_launches() - launches0
+    batch.close()
+    value = tot_valid / (tot_ms / 1000.0)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": tot_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": f"batched: {args.queries} queries, 40/30/30 % double integrator / Dubins / quadrotor, "
+                               "obstacles log-U[10,5000], trees log-U[2^14,2^20], start/goal >= 50 apart, one launch per "
+                               "stage for all queries", "l2": "each step is a whole batch plan (~GB working set)",
+                   "parallelism": f"replicas x{ws}"},
+        "plans_per_s": n_plans / (tot_ms / 1000.0),
+        "success_rate": found / max(n_plans, 1),
+        "success_by_model": {{1: "double_integrator", 2: "dubins", 3: "quadrotor"}[m]: v[1] / max(v[0], 1)
+                             for m, v in per_model.items()},
+        "tts_ms_p50": float(np.percentile(tts, 50)) if tts else None,
+        "tts_ms_p95": float(np.percentile(tts, 95)) if tts else None,
+        "e2e": {"value": tot_valid / wall, "unit": UNIT, "h2d_bytes_per_step": int(h_obs.numel() * 4),
+                "d2h_bytes_per_step": 128 * args.queries},
+        "gpu_launches": launches, "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="quad")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch"], default="quad")
+    ap.add_argument("--queries", type=int, default=1024)
     ap.add_argument("--plans", type=int, default=8)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batch":
+        run_batch(args)
     else:
         run_ours(args)
 

@@ -149,3 +149,50 @@ def uniform_draws(n: int, seed: int) -> np.ndarray:
     rng = np.random.default_rng(seed)
     k = rng.integers(1, 1 << 24, (n, 6), endpoint=True)
     return (k.astype(np.float64) * 2.0 ** -24).astype(np.float32)
+
+
+def boxes_avoiding(rng: np.random.Generator, n: int, points, side=(5.0, 15.0)) -> np.ndarray:
+    """n boxes (centres U[0,100]^3, sides U[side]) none of which covers one of `points`."""
+    pts = np.asarray([np.asarray(p, np.float32)[:3] for p in points], np.float32).reshape(-1, 3)
+    out = np.zeros((0, 6), np.float32)
+    while out.shape[0] < n:
+        m = int((n - out.shape[0]) * 1.5) + 8
+        c = rng.uniform(W_MIN, W_MAX, (m, 3))
+        s = rng.uniform(side[0], side[1], (m, 3))
+        b = np.concatenate([c - s / 2, c + s / 2], axis=1).astype(np.float32)
+        cover = np.zeros(m, bool)
+        for p in pts:
+            cover |= np.all(b[:, :3] <= p, axis=1) & np.all(p <= b[:, 3:], axis=1)
+        out = np.concatenate([out, b[~cover]])
+    return out[:n]
+
+
+def batch_queries(n: int = 1024, seed: int = 4, mix=(0.4, 0.3, 0.3), obs_range=(10, 5000), tree_range=(1 << 14, 1 << 20),
+                  min_sep: float = 50.0):
+    """The batched benchmark: n queries, mixing double integrator / Dubins / quadrotor in `mix`
+    proportions; obstacle counts and tree budgets log-uniform in their ranges; start and goal
+    uniform in the workspace at least `min_sep` apart, with no box covering either.
+    Returns a list of dicts: model, n_obs, tree, obstacles, start, goal."""
+    rng = np.random.default_rng(seed)
+    counts = [int(round(n * f)) for f in mix]
+    counts[0] += n - sum(counts)
+    models = np.concatenate([np.full(c, m + 1) for m, c in enumerate(counts)])
+    rng.shuffle(models)
+    out = []
+    for q in range(n):
+        model = int(models[q])
+        n_obs = int(round(math.exp(rng.uniform(math.log(obs_range[0]), math.log(obs_range[1])))))
+        tree = int(round(2.0 ** rng.uniform(math.log2(tree_range[0]), math.log2(tree_range[1]))))
+        while True:
+            a, b = rng.uniform(W_MIN, W_MAX, 3), rng.uniform(W_MIN, W_MAX, 3)
+            if np.linalg.norm(a - b) >= min_sep:
+                break
+        sd = 12 if model == 3 else 6
+        start, goal = np.zeros(sd, np.float32), np.zeros(sd, np.float32)
+        start[:3], goal[:3] = a, b
+        if model == 2:
+            start[3] = rng.uniform(-math.pi, math.pi)
+            start[5] = 1.0
+        out.append({"model": model, "n_obs": n_obs, "tree": tree, "start": start, "goal": goal,
+                    "obstacles": boxes_avoiding(rng, n_obs, (a, b))})
+    return out
