@@ -250,6 +250,71 @@ kpax_status kpax_test_sincos(const float* d_x, uint32_t n, float* d_out, void* s
  * benchmark reports it as evidence that the device path ran. */
 uint64_t kpax_kernel_launches(void);
 
+/* ---- learned proposal (no counterpart in the reference) ----------------------------------
+ * The reference draws every control and duration uniformly (statePropagatorSpatialHash.cu,
+ * propagateAndCheck).  A proposal network reshapes those draws for the quadrotor: an MLP
+ * 51 -> 256 -> 256 -> 88 (SiLU) maps (state, goal - state, occupancy of the 3x3x3 R1 workspace
+ * cells around the state) to an 8-component Gaussian mixture over the logits of the five draw
+ * uniforms (4 controls, duration).  A fraction epsilon of the draws stays uniform and every
+ * segment is still propagated and collision-checked exactly.
+ * Layouts: features n x 64 floats (51 used), network outputs n x 96 floats (88 used), mixture
+ * records n x 88 floats (8 cumulative weights, 8x5 means, 8x5 sigmas), logit targets n x 5. */
+typedef struct kpax_mlp kpax_mlp;
+#define KPAX_MLP_FEATURES 64
+#define KPAX_MLP_OUTPUTS 96
+#define KPAX_MLP_MIX 88
+#define KPAX_MLP_HIDDEN 256
+
+/* A network with buffers for training batches of up to max_batch rows; parameters start at 0. */
+kpax_status kpax_mlp_create(uint32_t max_batch, kpax_mlp** out);
+kpax_status kpax_mlp_destroy(kpax_mlp* net);
+/* Number of FP32 parameters (W1[256][64], b1, W2[256][256], b2, W3[96][256], b3). */
+uint32_t kpax_mlp_num_params(void);
+/* Sets the FP32 parameters, clears the Adam state and packs the BF16 inference image. */
+kpax_status kpax_mlp_set_params(kpax_mlp* net, const float* h_params, void* stream);
+kpax_status kpax_mlp_get_params(kpax_mlp* net, float* h_params, void* stream);
+/* Weights of the five target dimensions in the loss (default 1; 0 drops a dimension, e.g. the
+ * duration of fixed-step models). */
+kpax_status kpax_mlp_set_loss_mask(kpax_mlp* net, const float* h_mask5, void* stream);
+/* Re-packs the BF16 inference image from the FP32 parameters (after training). */
+kpax_status kpax_mlp_pack(kpax_mlp* net, void* stream);
+/* FP32 forward pass (training kernels): d_x n x 64 -> d_out n x 96. */
+kpax_status kpax_mlp_forward(kpax_mlp* net, const float* d_x, uint32_t n, float* d_out, void* stream);
+/* Mean loss (h_loss, synchronises) and its gradient (d_grad, num_params floats; may be NULL)
+ * of n rows of features d_x and logit targets d_y. */
+kpax_status kpax_mlp_loss_grad(kpax_mlp* net, const float* d_x, const float* d_y, uint32_t n,
+                               float* h_loss, float* d_grad, void* stream);
+/* One Adam step (beta 0.9/0.999, eps 1e-8) on the rows d_idx[0..batch) of (d_x, d_y).
+ * h_loss (may be NULL: no synchronisation) receives the batch's mean loss. */
+kpax_status kpax_mlp_train_step(kpax_mlp* net, const float* d_x, const float* d_y,
+                                const uint32_t* d_idx, uint32_t batch, float lr, float* h_loss,
+                                void* stream);
+/* Adam moments (num_params floats each, may be NULL) and step count. */
+kpax_status kpax_mlp_adam_state(kpax_mlp* net, float* h_m, float* h_v, uint64_t* step,
+                                void* stream);
+/* Occupancy bits of the env's R1 workspace cells (W1^3 bits, cell (x,y,z) at bit
+ * (z*W1 + y)*W1 + x): blocked when >= 32 of a 4x4x4 point lattice lie inside obstacles. */
+kpax_status kpax_env_occupancy(kpax_env* env, uint32_t* d_words, void* stream);
+/* Features of n states (row stride `stride` floats) with goals d_goals (n x 3). */
+kpax_status kpax_mlp_features(kpax_env* env, const float* d_states, uint32_t stride,
+                              const float* d_goals, uint32_t n, float* d_x, void* stream);
+/* Tensor-core (BF16, FP32 accumulate) forward pass of n states to mixture records d_mix.
+ * Optional dumps: d_out (n x 96 outputs), d_h1 / d_h2 (n x 256 BF16 hidden activations).
+ * Synchronises `stream`; KPAX_ETIMEOUT if a pipeline wait expired. */
+kpax_status kpax_mlp_propose(kpax_mlp* net, kpax_env* env, const float* d_states, uint32_t stride,
+                             const float* d_goals, uint32_t n, float* d_mix, float* d_out,
+                             uint16_t* d_h1, uint16_t* d_h2, void* stream);
+/* Turns the learned proposal on (net != NULL) or off for the planner's quadrotor plans.  The
+ * packed image is copied, so the network may be trained further or destroyed afterwards. */
+kpax_status kpax_set_proposal(kpax_planner* planner, kpax_mlp* net, float epsilon);
+/* Mixture records (88 floats each) of the frontier entries of the last iteration; child c of
+ * that iteration drew from record c / k with k = children / entries. */
+kpax_status kpax_export_proposal(kpax_planner* planner, float* h_mix, uint32_t max_entries,
+                                 uint32_t* n_entries);
+/* The same for the quadrotor queries of a batch; enable: one byte per query (NULL = all). */
+kpax_status kpax_batch_set_proposal(kpax_batch* batch, kpax_mlp* net, float epsilon,
+                                    const uint8_t* enable);
+
 #ifdef __cplusplus
 }
 #endif

@@ -303,6 +303,7 @@ kpax_status kpax_env_destroy(kpax_env* e)
 {
     if(!e) return KPAX_OK;
     e->env.release();
+    if(e->d_occ) cudaFree(e->d_occ);
     delete e;
     return KPAX_OK;
 }

@@ -48,9 +48,18 @@ struct Env {
 kpax_status launch_propagate(const KParams& p, const Grid& g, const float* parents, const float* draws, uint32_t stream_id,
                              uint32_t n, float* rows, uint8_t* valid, int32_t* steps, cudaStream_t stream);
 
+// Learned proposal (kpax_learn.cu): occupancy bits of the R1 workspace cells (W1^3 bits, zeroed
+// and filled on `stream`) and the packed tensor-core image of a network (null until packed).
+kpax_status launch_occupancy(const KParams& p, const Grid& g, uint32_t* d_words, cudaStream_t stream);
+
 }  // namespace kpax
 
 struct kpax_env {
     kpax::KParams params;
     kpax::Env env;
+    uint32_t* d_occ = nullptr;  // occupancy bits, computed on first use by the learned proposal
 };
+
+namespace kpax {
+const uint8_t* mlp_image(const kpax_mlp* n);
+}

@@ -20,6 +20,7 @@
 #include <stdint.h>
 
 #include "kpax_device.cuh"
+#include "kpax_mlp_tc.cuh"
 
 namespace kpax {
 namespace plan {
@@ -30,7 +31,7 @@ constexpr int kFrontierBS = 256, kItems = 4, kTile = kFrontierBS * kItems;
 constexpr int kExpandBS = 448;  // 2^16 children over 148 SMs: one 14-warp block per SM
 constexpr int kScoreBS = 256, kPartials = 1024;
 constexpr uint32_t kSpinLimit = 1u << 22;  // ~4 s of polling before a wait gives up
-constexpr uint32_t kErrTimeout = 1u, kErrCapacity = 2u;
+constexpr uint32_t kErrTimeout = 1u, kErrCapacity = 2u, kErrProposal = mlp::tc::kErrWait;
 
 struct TreeDev {
     float4* s[3];  // state planes: floats 4k..4k+3 of every node
@@ -87,7 +88,12 @@ struct alignas(16) QueryDev {
     uint32_t* sarr;       // arrival counter of k_scores
     float* path;
     const float* init_goal;  // init row then goal row, S floats each
-    uint32_t path_rows, pad[3];
+    // learned proposal (quadrotor queries that enabled it; null otherwise)
+    const uint8_t* mlp_img;  // packed BF16 network image
+    float* mix;              // one mixture record per frontier entry
+    const uint32_t* occ;     // occupancy bits of the R1 workspace cells
+    float prop_eps;          // fraction of draws kept uniform
+    uint32_t path_rows, pad[2];
 };
 
 __device__ __forceinline__ unsigned long long globaltimer()
@@ -430,6 +436,9 @@ __global__ void __launch_bounds__(kExpandBS) k_expand(const QueryDev* __restrict
         parent = sq.entries[c / k];
         load_state<SD>(t, parent, s);
         child_draws(p, plan, iter, c, u);
+        if constexpr(M == KPAX_MODEL_QUADROTOR) {
+            if(sq.mix) mlp::mixture_draws(p, sq.mix + (size_t)(c / k) * mlp::kMixFloats, sq.prop_eps, plan, iter, c, u);
+        }
         steps = draw_controls(p, u, cc);
         valid = propagate<M>(p, sq.g, s, cc, steps, steps_done);
         r1v = region_r1(p, s);
@@ -580,6 +589,39 @@ __global__ void __launch_bounds__(kScoreBS) k_scores(const QueryDev* __restrict_
 }
 
 // Re-activation of the last iteration without a scan (makes exported frontier flags final).
+// Rows of the proposal pass: the frontier entries of the iteration (k_frontier_write).
+struct EntrySrc {
+    static constexpr bool kDebug = false;
+    const QueryDev* q;
+    uint32_t E;
+    __device__ uint32_t count() const { return E; }
+    __device__ void row_features(uint32_t row, float x[mlp::kInPad]) const
+    {
+        float s[12];
+        load_state<12>(q->t, q->entries[row], s);
+        const float g[3] = {q->ctl->goal[0], q->ctl->goal[1], q->ctl->goal[2]};
+        mlp::features(q->p, q->occ, s, g, x);
+    }
+    __device__ void store(uint32_t row, const float o[mlp::kOutPad]) const
+    {
+        mlp::mixture_record(o, q->mix + (size_t)row * mlp::kMixFloats);
+    }
+    __device__ void dump_h(int, uint32_t, const uint8_t*, uint32_t) const {}
+};
+
+// Learned proposal of the quadrotor queries in qidx: one mixture record per frontier entry,
+// from the BF16 tensor-core forward pass of the entry's node.  Runs between k_frontier_write
+// and k_expand, which samples each child's draws from its entry's record.
+__global__ void __launch_bounds__(mlp::tc::kThreads, 1) k_propose(const QueryDev* __restrict__ qs, const uint32_t* __restrict__ qidx)
+{
+    extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ QueryDev sq;
+    load_query(qs, qidx, sq);
+    if(sq.ctl->done || !sq.mix) return;
+    EntrySrc src{&sq, sq.ctl->E};
+    mlp::tc::forward(src, sq.mlp_img, smem, &sq.ctl->error);
+}
+
 __global__ void k_reactivate(const QueryDev* __restrict__ qs)
 {
     __shared__ QueryDev sq;

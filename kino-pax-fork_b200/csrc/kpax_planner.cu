@@ -70,6 +70,11 @@ struct PlanBatch {
     void* d_flush = nullptr;
     uint64_t flush_cap = 0;
     std::vector<cudaEvent_t> tev;
+    // learned proposal
+    uint8_t* d_img = nullptr;        // copy of the packed network image
+    char* d_learn = nullptr;         // mixture records and occupancy bits of the learned queries
+    uint32_t* d_learned = nullptr;   // indices of the learned queries
+    uint32_t n_learned = 0, gx_prop = 1;
 
     kpax_status init(const kpax_config* cfgs, uint32_t n)
     {
@@ -185,7 +190,7 @@ struct PlanBatch {
         for(Env& e : env) e.release();
         for(int m = 0; m < 3; ++m)
             if(d_groups[m]) cudaFree(d_groups[m]);
-        void* dev[] = {pool, dq, d_ctl, d_active, d_ig, d_path, d_flush};
+        void* dev[] = {pool, dq, d_ctl, d_active, d_ig, d_path, d_flush, d_img, d_learn, d_learned};
         for(void* p : dev)
             if(p) cudaFree(p);
         void* host[] = {h_ctl, h_active, h_ig, h_path};
@@ -256,6 +261,8 @@ struct PlanBatch {
                 cudaStreamWaitEvent(s, ev_fork, 0);
             }
             const dim3 grid(expand_gx[m], (uint32_t)groups[m].size());
+            if(m == 2 && n_learned)
+                k_propose<<<dim3(gx_prop, n_learned), mlp::tc::kThreads, mlp::tc::kSmemBytes, s>>>(dq, d_learned);
             if(m == 0) k_expand<KPAX_MODEL_DOUBLE_INTEGRATOR><<<grid, kExpandBS, 0, s>>>(dq, d_groups[m], d_active);
             else if(m == 1) k_expand<KPAX_MODEL_DUBINS_AIRPLANE><<<grid, kExpandBS, 0, s>>>(dq, d_groups[m], d_active);
             else k_expand<KPAX_MODEL_QUADROTOR><<<grid, kExpandBS, 0, s>>>(dq, d_groups[m], d_active);
@@ -267,9 +274,72 @@ struct PlanBatch {
         if(ev) cudaEventRecord(ev[3], stream);
     }
 
+    // Learned proposal for the quadrotor queries with enable[q] != 0 (all when enable is null);
+    // net == nullptr turns it off.
+    kpax_status set_proposal(const kpax_mlp* net, float eps, const uint8_t* enable)
+    {
+        if(net && !mlp_image(net)) return set_error("set_proposal: network not packed"), KPAX_EINVAL;
+        if(!(eps >= 0.0f && eps <= 1.0f)) return set_error("set_proposal: epsilon %g not in [0,1]", (double)eps), KPAX_EINVAL;
+        std::vector<uint32_t> sel;
+        for(uint32_t q = 0; net && q < nq; ++q) {
+            const bool want = enable ? enable[q] != 0 : prm[q].model == KPAX_MODEL_QUADROTOR;
+            if(!want) continue;
+            if(prm[q].model != KPAX_MODEL_QUADROTOR)
+                return set_error("set_proposal: query %u is not a quadrotor query", q), KPAX_EINVAL;
+            sel.push_back(q);
+        }
+        KPAX_CUDA(cudaStreamSynchronize(stream));
+        if(graph) cudaGraphExecDestroy(graph), graph = nullptr;
+        graph_key.clear();
+        for(void* p : {(void*)d_img, (void*)d_learn, (void*)d_learned})
+            if(p) cudaFree(p);
+        d_img = nullptr, d_learn = nullptr, d_learned = nullptr;
+        n_learned = 0;
+        for(QueryDev& d : hq) d.mlp_img = nullptr, d.mix = nullptr, d.occ = nullptr, d.prop_eps = 1.0f;
+        if(!sel.empty()) {
+            KPAX_CUDA(cudaMalloc(&d_img, mlp::kImgBytes));
+            KPAX_CUDA(cudaMemcpyAsync(d_img, mlp_image(net), mlp::kImgBytes, cudaMemcpyDeviceToDevice, stream));
+            size_t bytes = 0;
+            for(uint32_t q : sel) {
+                const uint32_t words = (uint32_t)((prm[q].W1 * prm[q].W1 * prm[q].W1 + 31) / 32);
+                bytes += ((size_t)prm[q].budget * mlp::kMixFloats * 4 + (size_t)words * 4 + kAlign - 1) / kAlign * kAlign;
+            }
+            KPAX_CUDA(cudaMalloc(&d_learn, bytes));
+            size_t off = 0;
+            uint32_t max_tiles = 1;
+            for(uint32_t q : sel) {
+                QueryDev& d = hq[q];
+                const uint32_t words = (uint32_t)((prm[q].W1 * prm[q].W1 * prm[q].W1 + 31) / 32);
+                d.mix = reinterpret_cast<float*>(d_learn + off);
+                d.occ = reinterpret_cast<uint32_t*>(d_learn + off + (size_t)prm[q].budget * mlp::kMixFloats * 4);
+                d.mlp_img = d_img;
+                d.prop_eps = eps;
+                off += ((size_t)prm[q].budget * mlp::kMixFloats * 4 + (size_t)words * 4 + kAlign - 1) / kAlign * kAlign;
+                max_tiles = std::max<uint32_t>(max_tiles, (prm[q].budget + mlp::tc::kRows - 1) / mlp::tc::kRows);
+            }
+            KPAX_CUDA(cudaMalloc(&d_learned, sizeof(uint32_t) * sel.size()));
+            KPAX_CUDA(cudaMemcpyAsync(d_learned, sel.data(), sizeof(uint32_t) * sel.size(), cudaMemcpyHostToDevice, stream));
+            n_learned = (uint32_t)sel.size();
+            int dev = 0, sms = 148;
+            KPAX_CUDA(cudaGetDevice(&dev));
+            KPAX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            gx_prop = std::max<uint32_t>(1, std::min<uint32_t>(max_tiles, (2u * (uint32_t)sms + n_learned - 1) / n_learned));
+            KPAX_CUDA(cudaFuncSetAttribute(k_propose, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp::tc::kSmemBytes));
+            if(begun)  // a plan in progress: occupancy of the current environments
+                for(uint32_t q : sel) {
+                    kpax_status st = launch_occupancy(prm[q], env[q].view(), const_cast<uint32_t*>(hq[q].occ), stream);
+                    if(st != KPAX_OK) return st;
+                }
+        }
+        kpax_status st = upload_descriptors();
+        if(st != KPAX_OK) return st;
+        KPAX_CUDA(cudaStreamSynchronize(stream));
+        return begun ? ensure_graph() : KPAX_OK;
+    }
+
     uint64_t kernels_per_iteration() const
     {
-        uint64_t k = 3;  // two frontier passes and the score pass
+        uint64_t k = n_learned ? 4 : 3;  // two frontier passes, the score pass, the proposal pass
         for(int m = 0; m < 3; ++m) k += groups[m].empty() ? 0 : 1;
         return k;
     }
@@ -304,6 +374,10 @@ struct PlanBatch {
             kpax_status st = env[q].build(prm[q], d_obstacles[q], n_obs[q], stream);
             if(st != KPAX_OK) return st;
             hq[q].g = env[q].view();
+            if(hq[q].occ) {
+                st = launch_occupancy(prm[q], hq[q].g, const_cast<uint32_t*>(hq[q].occ), stream);
+                if(st != KPAX_OK) return st;
+            }
             const uint32_t S = (uint32_t)prm[q].S;
             memcpy(h_ig + (size_t)q * 2 * s_max, h_init + (size_t)q * stride, sizeof(float) * S);
             memcpy(h_ig + (size_t)q * 2 * s_max + S, h_goal + (size_t)q * stride, sizeof(float) * S);
@@ -344,6 +418,8 @@ struct PlanBatch {
         for(uint32_t q = 0; q < nq; ++q) {
             if(h_ctl[q].error & kErrTimeout) return set_error("query %u: a device-side wait gave up", q), KPAX_ETIMEOUT;
             if(h_ctl[q].error & kErrCapacity) return set_error("query %u: tree capacity exceeded", q), KPAX_ECAPACITY;
+            if(h_ctl[q].error & kErrProposal)
+                return set_error("query %u: a wait of the proposal pass expired", q), KPAX_ETIMEOUT;
         }
         return KPAX_OK;
     }
@@ -667,6 +743,20 @@ kpax_status kpax_export_children(kpax_planner* pl, float* h_rows, uint8_t* h_val
     return KPAX_OK;
 }
 
+kpax_status kpax_export_proposal(kpax_planner* pl, float* h_mix, uint32_t max_entries, uint32_t* n_entries)
+{
+    if(!pl || !pl->b.hq[0].mix) return set_error("kpax_export_proposal: the learned proposal is off"), KPAX_EINVAL;
+    PlanBatch& b = pl->b;
+    kpax_status st = b.sync_ctl();
+    if(st != KPAX_OK) return st;
+    const uint32_t n = std::min(b.h_ctl[0].E, max_entries);
+    if(n_entries) *n_entries = n;
+    if(n && h_mix)
+        KPAX_CUDA(cudaMemcpyAsync(h_mix, b.hq[0].mix, sizeof(float) * n * mlp::kMixFloats, cudaMemcpyDeviceToHost, b.stream));
+    KPAX_CUDA(cudaStreamSynchronize(b.stream));
+    return KPAX_OK;
+}
+
 // ---------------------------------------------------------------- batches of queries
 
 kpax_status kpax_batch_create(const kpax_config* cfgs, uint32_t n, kpax_batch** out)
@@ -690,6 +780,20 @@ kpax_status kpax_batch_destroy(kpax_batch* b)
     b->b.release();
     delete b;
     return KPAX_OK;
+}
+
+kpax_status kpax_set_proposal(kpax_planner* pl, kpax_mlp* net, float epsilon)
+{
+    if(!pl) return set_error("kpax_set_proposal: null planner"), KPAX_EINVAL;
+    if(net && pl->b.prm[0].model != KPAX_MODEL_QUADROTOR)
+        return set_error("kpax_set_proposal: the proposal network is defined for the quadrotor"), KPAX_EINVAL;
+    return pl->b.set_proposal(net, epsilon, nullptr);
+}
+
+kpax_status kpax_batch_set_proposal(kpax_batch* bt, kpax_mlp* net, float epsilon, const uint8_t* enable)
+{
+    if(!bt) return set_error("kpax_batch_set_proposal: null batch"), KPAX_EINVAL;
+    return bt->b.set_proposal(net, epsilon, enable);
 }
 
 kpax_status kpax_batch_plan(kpax_batch* bt, const float* h_inits, const float* h_goals, uint32_t row_stride,

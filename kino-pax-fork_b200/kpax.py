@@ -143,7 +143,26 @@ _SIGNATURES = {
     "kpax_batch_destroy": (_I32, [_VP]),
     "kpax_batch_plan": (_I32, [_VP, _VP, _VP, _U32, _VP, _VP, _VP, ctypes.POINTER(BatchStats)]),
     "kpax_test_sincos": (_I32, [_VP, _U32, _VP, _VP]),
+    "kpax_mlp_create": (_I32, [_U32, ctypes.POINTER(_VP)]),
+    "kpax_mlp_destroy": (_I32, [_VP]),
+    "kpax_mlp_num_params": (_U32, []),
+    "kpax_mlp_set_params": (_I32, [_VP, _VP, _VP]),
+    "kpax_mlp_get_params": (_I32, [_VP, _VP, _VP]),
+    "kpax_mlp_set_loss_mask": (_I32, [_VP, _VP, _VP]),
+    "kpax_mlp_pack": (_I32, [_VP, _VP]),
+    "kpax_mlp_forward": (_I32, [_VP, _VP, _U32, _VP, _VP]),
+    "kpax_mlp_loss_grad": (_I32, [_VP, _VP, _VP, _U32, _VP, _VP, _VP]),
+    "kpax_mlp_train_step": (_I32, [_VP, _VP, _VP, _VP, _U32, ctypes.c_float, _VP, _VP]),
+    "kpax_mlp_adam_state": (_I32, [_VP, _VP, _VP, _VP, _VP]),
+    "kpax_env_occupancy": (_I32, [_VP, _VP, _VP]),
+    "kpax_mlp_features": (_I32, [_VP, _VP, _U32, _VP, _U32, _VP, _VP]),
+    "kpax_mlp_propose": (_I32, [_VP, _VP, _VP, _U32, _VP, _U32, _VP, _VP, _VP, _VP, _VP]),
+    "kpax_set_proposal": (_I32, [_VP, _VP, ctypes.c_float]),
+    "kpax_export_proposal": (_I32, [_VP, _VP, _U32, _VP]),
+    "kpax_batch_set_proposal": (_I32, [_VP, _VP, ctypes.c_float, _VP]),
 }
+
+MLP_FEATURES, MLP_OUTPUTS, MLP_MIX, MLP_HIDDEN = 64, 96, 88, 256
 
 _lib = None
 
@@ -345,6 +364,17 @@ class KPAX:
         check(load().kpax_export_frontier(self._h, _ptr(rep), _ptr(r1), n), "kpax_export_frontier")
         return rep, r1
 
+    def set_proposal(self, net: "MLP | None", epsilon: float = 0.2) -> None:
+        """Learned proposal on (net) or off (None) for this quadrotor planner."""
+        check(load().kpax_set_proposal(self._h, net.handle if net else None, float(epsilon)), "kpax_set_proposal")
+
+    def export_proposal(self) -> np.ndarray:
+        """Mixture records of the last iteration's frontier entries (E x 88)."""
+        mix = np.zeros((self.cfg.expansions_per_iter, MLP_MIX), np.float32)
+        n = ctypes.c_uint32()
+        check(load().kpax_export_proposal(self._h, _ptr(mix), mix.shape[0], ctypes.byref(n)), "kpax_export_proposal")
+        return mix[: n.value]
+
     def debug_capture(self, on: bool = True) -> None:
         check(load().kpax_debug_capture(self._h, int(on)), "kpax_debug_capture")
 
@@ -386,6 +416,13 @@ class Batch:
         self.n = len(self.cfgs)
         self.stride = max(c.sample_dim for c in self.cfgs)
 
+    def set_proposal(self, net: "MLP | None", epsilon: float = 0.2, enable=None) -> None:
+        """Learned proposal for the quadrotor queries (enable: per-query flags, None = all)."""
+        en = None if enable is None else np.ascontiguousarray(enable, np.uint8)
+        check(load().kpax_batch_set_proposal(self._h, net.handle if net else None, float(epsilon),
+                                             None if en is None else _ptr(en)), "kpax_batch_set_proposal")
+        self._enable = en
+
     def plan(self, starts, goals, d_obstacles, n_obs):
         """starts/goals: per-query state vectors; d_obstacles: device pointers; n_obs: counts."""
         S = self.stride
@@ -421,3 +458,83 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+class MLP:
+    """The learned proposal network: FP32 parameters trained by the library's SIMT kernels and a
+    packed BF16 image for the tensor-core inference pass.  Device buffers are integer pointers."""
+
+    def __init__(self, max_batch: int = 4096, stream: int = 0):
+        self._h = _VP()
+        self.stream = stream
+        self.max_batch = max_batch
+        check(load().kpax_mlp_create(max_batch, ctypes.byref(self._h)), "kpax_mlp_create")
+        self.num_params = int(load().kpax_mlp_num_params())
+
+    @property
+    def handle(self) -> int:
+        return self._h.value
+
+    def set_params(self, params: np.ndarray) -> None:
+        w = np.ascontiguousarray(params, np.float32).ravel()
+        if w.size != self.num_params:
+            raise ValueError(f"expected {self.num_params} parameters, got {w.size}")
+        check(load().kpax_mlp_set_params(self._h, _ptr(w), self.stream), "kpax_mlp_set_params")
+
+    def get_params(self) -> np.ndarray:
+        w = np.zeros(self.num_params, np.float32)
+        check(load().kpax_mlp_get_params(self._h, _ptr(w), self.stream), "kpax_mlp_get_params")
+        return w
+
+    def set_loss_mask(self, mask) -> None:
+        m = np.ascontiguousarray(mask, np.float32).ravel()
+        check(load().kpax_mlp_set_loss_mask(self._h, _ptr(m), self.stream), "kpax_mlp_set_loss_mask")
+
+    def pack(self) -> None:
+        check(load().kpax_mlp_pack(self._h, self.stream), "kpax_mlp_pack")
+
+    def forward(self, d_x: int, n: int, d_out: int) -> None:
+        check(load().kpax_mlp_forward(self._h, d_x, n, d_out, self.stream), "kpax_mlp_forward")
+
+    def loss_grad(self, d_x: int, d_y: int, n: int, d_grad: int | None = None) -> float:
+        loss = ctypes.c_float()
+        check(load().kpax_mlp_loss_grad(self._h, d_x, d_y, n, ctypes.byref(loss), d_grad or None, self.stream),
+              "kpax_mlp_loss_grad")
+        return float(loss.value)
+
+    def train_step(self, d_x: int, d_y: int, d_idx: int, batch: int, lr: float, want_loss: bool = False) -> float | None:
+        loss = ctypes.c_float()
+        check(load().kpax_mlp_train_step(self._h, d_x, d_y, d_idx, batch, float(lr),
+                                         ctypes.byref(loss) if want_loss else None, self.stream), "kpax_mlp_train_step")
+        return float(loss.value) if want_loss else None
+
+    def adam_state(self):
+        m = np.zeros(self.num_params, np.float32)
+        v = np.zeros(self.num_params, np.float32)
+        step = ctypes.c_uint64()
+        check(load().kpax_mlp_adam_state(self._h, _ptr(m), _ptr(v), ctypes.byref(step), self.stream), "kpax_mlp_adam_state")
+        return m, v, int(step.value)
+
+    def propose(self, env: Env, d_states: int, stride: int, d_goals: int, n: int, d_mix: int, d_out: int | None = None,
+                d_h1: int | None = None, d_h2: int | None = None) -> None:
+        check(load().kpax_mlp_propose(self._h, env.handle, d_states, stride, d_goals, n, d_mix, d_out or None, d_h1 or None,
+                                      d_h2 or None, self.stream), "kpax_mlp_propose")
+
+    def close(self) -> None:
+        if self._h:
+            load().kpax_mlp_destroy(self._h)
+            self._h = _VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def env_occupancy(env: Env, d_words: int, stream: int = 0) -> None:
+    check(load().kpax_env_occupancy(env.handle, d_words, stream), "kpax_env_occupancy")
+
+
+def mlp_features(env: Env, d_states: int, stride: int, d_goals: int, n: int, d_x: int, stream: int = 0) -> None:
+    check(load().kpax_mlp_features(env.handle, d_states, stride, d_goals, n, d_x, stream), "kpax_mlp_features")
