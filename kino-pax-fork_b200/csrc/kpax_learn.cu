@@ -258,6 +258,7 @@ struct ArraySrc {
     uint16_t* h1;
     uint16_t* h2;
     __device__ uint32_t count() const { return n; }
+    __device__ float* records() const { return mix; }
     __device__ void row_features(uint32_t row, float x[kInPad]) const
     {
         float s[12], g[3];
@@ -265,21 +266,16 @@ struct ArraySrc {
         for(int d = 0; d < 3; ++d) g[d] = goals[(size_t)row * 3 + d];
         features(p, occ, s, g, x);
     }
-    __device__ void store(uint32_t row, const float o[kOutPad]) const
-    {
-        if(out)
-            for(int i = 0; i < kOutPad; ++i) out[(size_t)row * kOutPad + i] = o[i];
-        float rec[kMixFloats];
-        mixture_record(o, rec);
-        for(int i = 0; i < kMixFloats; ++i) mix[(size_t)row * kMixFloats + i] = rec[i];
-    }
-    __device__ void dump_h(int layer, uint32_t row, const uint8_t* slabs, uint32_t r) const
+    __device__ void dump_h(int layer, uint32_t row, uint32_t col0, const uint4 bits[2]) const
     {
         uint16_t* dst = layer == 1 ? h1 : h2;
         if(!dst) return;
-        for(uint32_t c = 0; c < (uint32_t)kH; ++c)
-            dst[(size_t)row * kH + c] =
-              *reinterpret_cast<const uint16_t*>(slabs + (c >> 6) * (tc::kRows * kSlabRowBytes) + swz(r, c & 63));
+        uint4* d = reinterpret_cast<uint4*>(dst + (size_t)row * kH + col0);
+        d[0] = bits[0], d[1] = bits[1];
+    }
+    __device__ void dump_out(uint32_t row, uint32_t col, float v) const
+    {
+        if(out) out[(size_t)row * kOutPad + col] = v;
     }
 };
 

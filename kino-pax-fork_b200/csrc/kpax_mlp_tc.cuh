@@ -1,19 +1,19 @@
-// kpax_mlp_tc.cuh — device side of the learned proposal: input features, obstacle occupancy of
-// the R1 workspace cells, the mixture record, the mixture sampler, and the BF16 tensor-core
-// forward pass (tcgen05, FP32 accumulators in tensor memory).
+// kpax_mlp_tc.cuh — device side of the learned proposal: input features, the mixture record,
+// the mixture sampler, and the BF16 tensor-core forward pass (tcgen05, FP32 accumulators in
+// tensor memory).
 //
-// Forward pass, one CTA of 512 threads per SM, persistent over tiles of 128 rows:
-//   features   threads 0..127 build one row each and store it as BF16 into the swizzled X slab
-//   layer 1    D1[128x256] = X W1^T           (4 MMAs of K=16, N=256; TMEM columns 0..255)
-//   epilogue   H = SiLU(D1 + b1) as BF16 into four swizzled slabs (16 warps, 64 columns each)
-//   layer 2    D2[128x256] = H W2^T           (16 MMAs; TMEM columns 256..511)
-//   epilogue   H = SiLU(D2 + b2)
-//   layer 3    D3[128x96]  = H W3^T           (16 MMAs, N=96; TMEM columns 0..95)
-//   epilogue   threads 0..127 turn their row's 88 outputs (+ b3) into a mixture record
-// Weights stream from the global image through a two-slot ring of 32 KB shared-memory buffers
-// by bulk copies (no tensor map, no multicast); one thread issues the copies and the MMAs and
-// tracks both with mbarriers.  Every wait is bounded in time: on expiry the kernel records an
-// error bit, waits (bounded) for its copies and MMAs, frees its tensor memory and returns.
+// Forward pass: one CTA of 20 warps per SM, persistent over tiles of 128 rows, with roles:
+//   warp 0      issues the MMAs (one thread) and owns the tensor-memory allocation
+//   warp 1      streams the weights from the global image through a 3-slot ring of 32 KB
+//               shared-memory buffers by bulk copies (no tensor map, no multicast)
+//   warps 2-3   build the input features of the next tiles into a double-buffered X slab
+//   warps 4-19  epilogues: TMEM -> bias + SiLU -> BF16 H slabs, and the mixture records
+// Per tile: D1[128x256] = X W1^T (TMEM columns 0..255), H = SiLU(D1 + b1); D2 = H W2^T (columns
+// 256..511), H = SiLU(D2 + b2); D3[128x96] = H W3^T (columns 0..95) -> records.  The MMAs of
+// K-slab j of layers 2 and 3 start as soon as the epilogue has written H slab j, so epilogues
+// overlap the tensor cores.  Operands are K-major with the 128-byte swizzle; every handoff is an
+// mbarrier, and every wait is bounded in time: on expiry the kernel records an error bit, lets
+// its copies and MMAs drain (bounded), frees its tensor memory and returns.
 #pragma once
 #include <cuda_bf16.h>
 #include <stdint.h>
@@ -122,14 +122,21 @@ __device__ __forceinline__ void mixture_draws(const KParams& p, const float* __r
 
 namespace tc {
 
-constexpr int kThreads = 512, kRows = 128;
-constexpr uint32_t kRingBytes = 32768;
-constexpr uint32_t kSmX = 0, kSmH = 16384, kSmRing = kSmH + 65536, kSmBias = kSmRing + 2 * kRingBytes;
-constexpr uint32_t kSmBar = kSmBias + (kH + kH + kOutPad) * 4, kSmTmem = kSmBar + 8 * 8, kSmUsed = kSmTmem + 16;
+constexpr int kThreads = 640, kRows = 128, kStages = 3, kEpiThreads = 512, kFeatThreads = 64;
+constexpr uint32_t kRingBytes = 32768, kSlabBytes = kRows * kSlabRowBytes;  // 16 KB: 128 rows x 64 BF16
+constexpr uint32_t kSmX = 0, kSmH = kSmX + 2 * kSlabBytes, kSmRing = kSmH + 4 * kSlabBytes;
+constexpr uint32_t kSmBias = kSmRing + kStages * kRingBytes;
+constexpr uint32_t kRecStride = kMixFloats + 1;  // staging row stride (odd: conflict-free)
+// mbarriers: ring full / empty, X full / empty, layer accumulators, H slabs of layers 1 and 2,
+// tensor memory free (end of a tile's record epilogue), drain
+constexpr int kBarRF = 0, kBarRE = 3, kBarXF = 6, kBarXE = 8, kBarD1 = 10, kBarD2 = 11, kBarD3 = 12, kBarHF = 13, kBarGF = 17,
+              kBarTF = 21, kBarFin = 22, kNumBars = 23;
+constexpr uint32_t kSmBar = kSmBias + (kH + kH + kOutPad) * 4, kSmTmem = kSmBar + kNumBars * 8, kSmUsed = kSmTmem + 16;
 constexpr uint32_t kSmemBytes = kSmUsed + 1024;  // slack for the 1024-byte alignment of the slabs
 constexpr int kChunks = 9;                       // W1, 4 slabs of W2, 4 slabs of W3
 constexpr unsigned long long kWaitNs = 2000000000ull;
 constexpr uint32_t kErrWait = 4u;
+static_assert(kRows * kRecStride * 4 <= 4 * kSlabBytes, "record staging must fit in the H slabs");
 
 __host__ __device__ constexpr uint32_t chunk_src(int c)
 {
@@ -185,6 +192,11 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
     return true;
 }
 
+__device__ __forceinline__ void mbar_arrive(uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
 __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar)
 {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
@@ -224,6 +236,13 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16])
     for(int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ float tmem_ld1(uint32_t taddr)
+{
+    uint32_t r;
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(taddr));
+    return __uint_as_float(r);
+}
+
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b)
@@ -232,22 +251,47 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b)
     return *reinterpret_cast<const uint32_t*>(&h);
 }
 
-__device__ __forceinline__ float silu(float x) { return __fdividef(x, 1.0f + __expf(-x)); }
+// SiLU(x) = x * sigmoid(x) = 0.5 x (1 + tanh(x / 2)), one MUFU operation (tanh.approx.f32,
+// absolute error below 2^-10.9); the result is rounded to BF16 afterwards.
+__device__ __forceinline__ float silu(float x)
+{
+    const float hx = 0.5f * x;
+    float t;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(hx));
+    return fmaf(hx, t, hx);
+}
+
+// Named barrier of the 512 epilogue threads; the OR form returns a value uniform across them.
+__device__ __forceinline__ void epi_sync() { asm volatile("bar.sync 1, 512;" ::: "memory"); }
+__device__ __forceinline__ bool epi_sync_or(bool v)
+{
+    uint32_t r;
+    asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 q, %1, 0;\n\t"
+      "bar.red.or.pred p, 1, 512, q;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)v)
+      : "memory");
+    return r != 0u;
+}
 
 // Stores 16 consecutive columns (col0 a multiple of 16) of row r into the swizzled slabs at base.
-__device__ __forceinline__ void store_row16(uint8_t* base, uint32_t r, uint32_t col0, const float v[16])
+__device__ __forceinline__ void store_row16(uint8_t* base, uint32_t r, uint32_t col0, const float v[16], uint4* packed = nullptr)
 {
-    uint8_t* slab = base + (col0 >> 6) * (kRows * kSlabRowBytes);
+    uint8_t* slab = base + (col0 >> 6) * kSlabBytes;
     const uint32_t k = col0 & 63u;
     const uint4 lo = make_uint4(pack_bf16(v[0], v[1]), pack_bf16(v[2], v[3]), pack_bf16(v[4], v[5]), pack_bf16(v[6], v[7]));
     const uint4 hi = make_uint4(pack_bf16(v[8], v[9]), pack_bf16(v[10], v[11]), pack_bf16(v[12], v[13]), pack_bf16(v[14], v[15]));
     *reinterpret_cast<uint4*>(slab + swz(r, k)) = lo;
     *reinterpret_cast<uint4*>(slab + swz(r, k + 8)) = hi;
+    if(packed) packed[0] = lo, packed[1] = hi;
 }
 
 // Source of rows: `uint32_t count()`, `void row_features(uint32_t row, float x[64])`,
-// `void store(uint32_t row, const float o[96])`, and for debug dumps `kDebug` with
-// `dump_h(layer, row, const uint8_t* slabs, uint32_t r)`.
+// `float* records()` (count() records of kMixFloats floats), and for debug dumps `kDebug` with
+// `dump_h(layer, row, col0, const uint4 bits[2])` (16 BF16 values) and `dump_out(row, col, v)`.
 template <class Src>
 __device__ void forward(Src& src, const uint8_t* __restrict__ img, uint8_t* smem_raw, uint32_t* __restrict__ err)
 {
@@ -256,24 +300,25 @@ __device__ void forward(Src& src, const uint8_t* __restrict__ img, uint8_t* smem
     const uint32_t ntiles = (n + kRows - 1) / kRows;
     if(blockIdx.x >= ntiles) return;
     const uint32_t my_tiles = (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x;
-    const uint32_t total = my_tiles * kChunks;
     const uint32_t raw = (uint32_t)__cvta_generic_to_shared(smem_raw);
     const uint32_t pad = ((raw + 1023u) & ~1023u) - raw;
     uint8_t* sm = smem_raw + pad;
-    const uint32_t sbase = raw + pad;
+    const uint32_t sb = raw + pad;
     const float* bias = reinterpret_cast<const float*>(sm + kSmBias);
-    const uint32_t bar_full = sbase + kSmBar, bar_empty = bar_full + 16, bar_done = bar_full + 32;
+    auto bar = [&](int i) { return sb + kSmBar + 8u * (uint32_t)i; };
     uint32_t* s_tmem = reinterpret_cast<uint32_t*>(sm + kSmTmem);
     volatile uint32_t* s_err = s_tmem + 1;
 
     if(warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + kSmTmem), "r"(512u)
-                     : "memory");
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sb + kSmTmem), "r"(512u) : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    if(tid == 0) {
-        for(int i = 0; i < 2; ++i) mbar_init(bar_full + 8 * i, 1), mbar_init(bar_empty + 8 * i, 1);
-        mbar_init(bar_done, 1);
+    if(tid == 32) {
+        for(int s = 0; s < kStages; ++s) mbar_init(bar(kBarRF + s), 1), mbar_init(bar(kBarRE + s), 1);
+        for(int b = 0; b < 2; ++b) mbar_init(bar(kBarXF + b), kFeatThreads), mbar_init(bar(kBarXE + b), 1);
+        mbar_init(bar(kBarD1), 1), mbar_init(bar(kBarD2), 1), mbar_init(bar(kBarD3), 1);
+        for(int j = 0; j < 4; ++j) mbar_init(bar(kBarHF + j), 128), mbar_init(bar(kBarGF + j), 128);
+        mbar_init(bar(kBarTF), kEpiThreads), mbar_init(bar(kBarFin), 1);
         *s_err = 0u;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -283,135 +328,188 @@ __device__ void forward(Src& src, const uint8_t* __restrict__ img, uint8_t* smem
     __syncthreads();
     fence_after();
     const uint32_t tmem = *s_tmem;
-
-    // chunk g of this CTA's sequence lands in ring slot g & 1; its phases have parity (g >> 1) & 1
-    uint32_t issued = 0, consumed = 0, done_cnt = 0;
-    auto issue = [&]() {
-        const uint32_t slot = issued & 1u;
-        const int c = (int)(issued % kChunks);
-        bulk_load(sbase + kSmRing + slot * kRingBytes, img + chunk_src(c), chunk_bytes(c), bar_full + 8 * slot);
-        ++issued;
-    };
-    auto fail = [&]() { atomicOr(err, kErrWait), *s_err = 1u; };
-    if(tid == 0)
-        while(issued < total && issued < 2) issue();
-
-    // MMAs of one chunk: A = the K slab at a_addr (K = 64), B = the ring slot; accumulate after
-    // the first K step when `acc`.  Issued by thread 0 only.
-    auto run_chunk = [&](uint32_t a_addr, uint32_t d_col, uint32_t nn, bool acc, bool last) -> bool {
-        const uint32_t slot = consumed & 1u, par = (consumed >> 1) & 1u;
-        if(!mbar_wait(bar_full + 8 * slot, par)) return false;
-        fence_after();
-        const uint32_t b_addr = sbase + kSmRing + slot * kRingBytes;
-#pragma unroll
-        for(uint32_t kk = 0; kk < 4; ++kk)
-            mma(tmem + d_col, sdesc(a_addr + 32u * kk), sdesc(b_addr + 32u * kk), idesc(nn), (acc || kk) ? 1u : 0u);
-        commit(bar_empty + 8 * slot);
-        if(last) commit(bar_done);
-        ++consumed;
-        if(!mbar_wait(bar_empty + 8 * slot, par)) return false;  // slot free: refill it
-        if(issued < total) issue();
-        return true;
-    };
-    // Epilogue of layers 1 and 2: 16 warps, warp w reads TMEM lanes 32*(w%4).. and 64 columns.
-    auto hidden_epilogue = [&](uint32_t d_col, const float* b) {
-        const uint32_t q = warp & 3u, cg = warp >> 2, r = 32u * q + lane;
-        float v[4][16];
-#pragma unroll
-        for(int cc = 0; cc < 4; ++cc) tmem_ld16(tmem + ((32u * q) << 16) + d_col + cg * 64u + 16u * cc, v[cc]);
-        tmem_wait_ld();
-#pragma unroll
-        for(int cc = 0; cc < 4; ++cc) {
-            const uint32_t col0 = cg * 64u + 16u * cc;
-#pragma unroll
-            for(int i = 0; i < 16; ++i) v[cc][i] = silu(v[cc][i] + b[col0 + i]);
-            store_row16(sm + kSmH, r, col0, v[cc]);
-        }
-    };
-    // All threads wait for the layer's MMAs; returns a CTA-uniform verdict so that the warp-wide
-    // TMEM loads that follow are executed by whole warps or not at all.
-    auto layer_sync = [&]() -> bool {
-        bool ok = true;
-        if(!*s_err) ok = mbar_wait(bar_done, done_cnt & 1u);
-        ++done_cnt;
-        fence_after();
-        const bool bad = __syncthreads_or(!ok || *s_err) != 0;
-        if(bad && tid == 0) fail();
-        return !bad;
-    };
-    auto publish_smem = [&]() {  // generic-proxy writes -> visible to the MMA; TMEM reads ordered
-        fence_async_smem();
-        fence_before();
-        __syncthreads();
+    auto fail = [&]() {
+        atomicOr(err, kErrWait);
+        *s_err = 1u;
     };
 
-    for(uint32_t t = 0; t < my_tiles; ++t) {
-        const uint32_t tile = blockIdx.x + t * gridDim.x;
-        if(tid < (uint32_t)kRows) {
-            const uint32_t row = tile * kRows + tid;
-            float x[kInPad];
-            if(row < n) src.row_features(row, x);
-            else
+    if(warp == 0) {
+        // ---------------------------------------------------------------- MMA issuer
+        if(lane == 0) {
+            uint32_t g = 0;  // chunk sequence number
+            auto chunk = [&](uint32_t a_addr, uint32_t d_col, uint32_t nn, bool acc) -> bool {
+                const uint32_t s = g % kStages;
+                if(!mbar_wait(bar(kBarRF + s), (g / kStages) & 1u)) return false;
+                fence_after();
+                const uint32_t b_addr = sb + kSmRing + s * kRingBytes;
 #pragma unroll
-                for(int i = 0; i < kInPad; ++i) x[i] = 0.0f;
-#pragma unroll
-            for(int c = 0; c < kInPad; c += 16) store_row16(sm + kSmX, tid, (uint32_t)c, x + c);
-        }
-        publish_smem();
-        if(tid == 0) {
-            fence_after();
-            if(!run_chunk(sbase + kSmX, 0u, kH, false, true)) fail();
-        }
-        if(!layer_sync()) break;
-        hidden_epilogue(0u, bias);
-        publish_smem();
-        if constexpr(Src::kDebug) {
-            if(tid < (uint32_t)kRows && tile * kRows + tid < n) src.dump_h(1, tile * kRows + tid, sm + kSmH, tid);
-        }
-        if(tid == 0) {
-            fence_after();
-            for(uint32_t j = 0; j < 4; ++j)
-                if(!run_chunk(sbase + kSmH + j * (kRows * kSlabRowBytes), 256u, kH, j > 0, j == 3)) {
+                for(uint32_t kk = 0; kk < 4; ++kk)
+                    mma(tmem + d_col, sdesc(a_addr + 32u * kk), sdesc(b_addr + 32u * kk), idesc(nn), (acc || kk) ? 1u : 0u);
+                commit(bar(kBarRE + s));
+                ++g;
+                return true;
+            };
+            for(uint32_t i = 0; i < my_tiles && !*s_err; ++i) {
+                const uint32_t b = i & 1u;
+                bool ok = mbar_wait(bar(kBarXF + b), (i >> 1) & 1u);
+                if(ok && i > 0) ok = mbar_wait(bar(kBarTF), (i - 1) & 1u);  // tile i-1 done with TMEM
+                if(ok) ok = chunk(sb + kSmX + b * kSlabBytes, 0u, kH, false);
+                if(!ok) {
                     fail();
                     break;
                 }
-        }
-        if(!layer_sync()) break;
-        // H is rewritten only after every layer-2 MMA has completed (bar_done)
-        hidden_epilogue(256u, bias + kH);
-        publish_smem();
-        if constexpr(Src::kDebug) {
-            if(tid < (uint32_t)kRows && tile * kRows + tid < n) src.dump_h(2, tile * kRows + tid, sm + kSmH, tid);
-        }
-        if(tid == 0) {
-            fence_after();
-            for(uint32_t j = 0; j < 4; ++j)
-                if(!run_chunk(sbase + kSmH + j * (kRows * kSlabRowBytes), 0u, kOutPad, j > 0, j == 3)) {
+                commit(bar(kBarXE + b));
+                commit(bar(kBarD1));
+                for(uint32_t j = 0; j < 4 && ok; ++j) {
+                    ok = mbar_wait(bar(kBarHF + j), i & 1u);
+                    if(ok) fence_after(), ok = chunk(sb + kSmH + j * kSlabBytes, 256u, kH, j > 0);
+                }
+                if(ok) commit(bar(kBarD2));
+                for(uint32_t j = 0; j < 4 && ok; ++j) {
+                    ok = mbar_wait(bar(kBarGF + j), i & 1u);
+                    if(ok) fence_after(), ok = chunk(sb + kSmH + j * kSlabBytes, 0u, kOutPad, j > 0);
+                }
+                if(!ok) {
                     fail();
                     break;
                 }
-        }
-        if(!layer_sync()) break;
-        if(warp < 4) {
-            const uint32_t r = 32u * warp + lane, row = tile * kRows + r;
-            float o[kOutPad];
-#pragma unroll
-            for(int cc = 0; cc < kOutPad / 16; ++cc) tmem_ld16(tmem + ((32u * warp) << 16) + 16u * cc, o + 16 * cc);
-            tmem_wait_ld();
-            if(row < n) {
-#pragma unroll
-                for(int i = 0; i < kOutPad; ++i) o[i] += bias[2 * kH + i];
-                src.store(row, o);
+                commit(bar(kBarD3));
             }
+            commit(bar(kBarFin));  // arrives once every MMA issued above has completed
+            mbar_wait(bar(kBarFin), 0u);
         }
-        fence_before();
-        __syncthreads();
-    }
-    // teardown: on an error, let copies and MMAs in flight finish (bounded) before freeing TMEM
-    if(tid == 0 && *s_err) {
-        for(uint32_t g = consumed; g < issued; ++g) mbar_wait(bar_full + 8 * (g & 1u), (g >> 1) & 1u);
-        commit(bar_empty);  // arrives on slot 0 once every MMA issued so far is complete
-        mbar_wait(bar_empty, ((consumed + 1u) >> 1) & 1u);
+        __syncwarp();
+    } else if(warp == 1) {
+        // ---------------------------------------------------------------- weight producer
+        if(lane == 0) {
+            const uint32_t total = my_tiles * kChunks;
+            uint32_t g = 0;
+            for(; g < total && !*s_err; ++g) {
+                const uint32_t s = g % kStages;
+                if(g >= (uint32_t)kStages && !mbar_wait(bar(kBarRE + s), (g / kStages - 1) & 1u)) {
+                    fail();
+                    break;
+                }
+                const int c = (int)(g % kChunks);
+                bulk_load(sb + kSmRing + s * kRingBytes, img + chunk_src(c), chunk_bytes(c), bar(kBarRF + s));
+            }
+            for(uint32_t h = g > (uint32_t)kStages ? g - kStages : 0u; h < g; ++h)  // drain copies in flight
+                mbar_wait(bar(kBarRF + h % kStages), (h / kStages) & 1u);
+        }
+        __syncwarp();
+    } else if(warp < 4) {
+        // ---------------------------------------------------------------- features
+        const uint32_t ft = tid - 64u;
+        for(uint32_t i = 0; i < my_tiles && !*s_err; ++i) {
+            const uint32_t b = i & 1u, tile = blockIdx.x + i * gridDim.x;
+            if(i >= 2 && !mbar_wait(bar(kBarXE + b), ((i >> 1) - 1) & 1u)) {
+                fail();
+                break;
+            }
+            for(uint32_t r = ft; r < (uint32_t)kRows; r += kFeatThreads) {
+                const uint32_t row = tile * kRows + r;
+                float x[kInPad];
+                if(row < n) src.row_features(row, x);
+                else
+#pragma unroll
+                    for(int c = 0; c < kInPad; ++c) x[c] = 0.0f;
+#pragma unroll
+                for(int c = 0; c < kInPad; c += 16) store_row16(sm + kSmX + b * kSlabBytes, r, (uint32_t)c, x + c);
+            }
+            fence_async_smem();
+            mbar_arrive(bar(kBarXF + b));
+        }
+    } else {
+        // ---------------------------------------------------------------- epilogues
+        const uint32_t q = warp & 3u, cg = (warp - 4u) >> 2, r = 32u * q + lane;
+        const uint32_t t_lane = tmem + ((32u * q) << 16);
+        float* stg = reinterpret_cast<float*>(sm + kSmH);
+        for(uint32_t i = 0; i < my_tiles; ++i) {
+            const uint32_t tile = blockIdx.x + i * gridDim.x, row = tile * kRows + r;
+            // hidden layers: D (columns d_col..) -> SiLU -> H slab cg; arrive `ready`
+            auto hidden = [&](int layer, int bar_d, uint32_t d_col, const float* b, int bar_ready) -> bool {
+                const bool ok = mbar_wait(bar(bar_d), i & 1u);
+                if(epi_sync_or(!ok || *s_err)) return false;
+                fence_after();
+#pragma unroll
+                for(int half = 0; half < 2; ++half) {
+                    float v[2][16];
+#pragma unroll
+                    for(int cc = 0; cc < 2; ++cc) tmem_ld16(t_lane + d_col + cg * 64u + 32u * half + 16u * cc, v[cc]);
+                    tmem_wait_ld();
+#pragma unroll
+                    for(int cc = 0; cc < 2; ++cc) {
+                        const uint32_t col0 = cg * 64u + 32u * half + 16u * cc;
+#pragma unroll
+                        for(int k = 0; k < 16; ++k) v[cc][k] = silu(v[cc][k] + b[col0 + k]);
+                        uint4 bits[2];
+                        store_row16(sm + kSmH, r, col0, v[cc], bits);
+                        if constexpr(Src::kDebug) {
+                            if(row < n) src.dump_h(layer, row, col0, bits);
+                        }
+                    }
+                }
+                fence_async_smem();
+                fence_before();
+                mbar_arrive(bar(bar_ready + (int)cg));
+                return true;
+            };
+            if(!hidden(1, kBarD1, 0u, bias, kBarHF)) break;
+            if(!hidden(2, kBarD2, 256u, bias + kH, kBarGF)) break;
+            // records: warp group cg handles components 2cg and 2cg + 1, and (cg 0) the weights
+            const bool ok = mbar_wait(bar(kBarD3), i & 1u);
+            if(epi_sync_or(!ok || *s_err)) break;
+            fence_after();
+            float lg[kComp], o[2 * kCompStride];
+#pragma unroll
+            for(int k = 0; k < kComp; ++k) lg[k] = tmem_ld1(t_lane + (uint32_t)(k * kCompStride));
+#pragma unroll
+            for(int c = 0; c < 2 * kCompStride; ++c) o[c] = tmem_ld1(t_lane + cg * 2u * kCompStride + (uint32_t)c);
+            tmem_wait_ld();
+            fence_before();
+            mbar_arrive(bar(kBarTF));
+            const float* b3 = bias + 2 * kH;
+#pragma unroll
+            for(int k = 0; k < kComp; ++k) lg[k] += b3[k * kCompStride];
+#pragma unroll
+            for(int c = 0; c < 2 * kCompStride; ++c) o[c] += b3[cg * 2 * kCompStride + c];
+            float* rec = stg + r * kRecStride;
+            if(cg == 0) {
+                float mx = lg[0];
+#pragma unroll
+                for(int k = 1; k < kComp; ++k) mx = fmaxf(mx, lg[k]);
+                float e[kComp], tot = 0.0f;
+#pragma unroll
+                for(int k = 0; k < kComp; ++k) e[k] = expf(lg[k] - mx), tot += e[k];
+                float acc = 0.0f;
+#pragma unroll
+                for(int k = 0; k < kComp; ++k) {
+                    acc += e[k];
+                    rec[kMixCdf + k] = k == kComp - 1 ? 1.0f : acc / tot;
+                }
+            }
+#pragma unroll
+            for(int h = 0; h < 2; ++h) {
+                const int k = 2 * (int)cg + h;
+#pragma unroll
+                for(int d = 0; d < kDim; ++d) {
+                    rec[kMixMu + k * kDim + d] = o[h * kCompStride + 1 + d];
+                    const float sg = kSigMid + kSigHalf * tanhf(o[h * kCompStride + 1 + kDim + d] * (1.0f / kSigHalf));
+                    rec[kMixSigma + k * kDim + d] = expf(sg);
+                }
+            }
+            if constexpr(Src::kDebug) {
+                if(row < n)
+                    for(int c = 0; c < 2 * kCompStride; ++c) src.dump_out(row, cg * 2u * kCompStride + (uint32_t)c, o[c]);
+            }
+            epi_sync();
+            // coalesced copy of the tile's records (contiguous rows) to global memory
+            const uint32_t valid = min((uint32_t)kRows, n - tile * kRows);
+            float* dst = src.records() + (size_t)tile * kRows * kMixFloats;
+            for(uint32_t f = tid - 128u; f < valid * (uint32_t)kMixFloats; f += (uint32_t)kEpiThreads)
+                dst[f] = stg[(f / kMixFloats) * kRecStride + f % kMixFloats];
+            epi_sync();  // staging read before the next tile's epilogue rewrites H
+        }
     }
     fence_before();
     __syncthreads();

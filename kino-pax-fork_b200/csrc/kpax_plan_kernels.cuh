@@ -595,6 +595,7 @@ struct EntrySrc {
     const QueryDev* q;
     uint32_t E;
     __device__ uint32_t count() const { return E; }
+    __device__ float* records() const { return q->mix; }
     __device__ void row_features(uint32_t row, float x[mlp::kInPad]) const
     {
         float s[12];
@@ -602,11 +603,8 @@ struct EntrySrc {
         const float g[3] = {q->ctl->goal[0], q->ctl->goal[1], q->ctl->goal[2]};
         mlp::features(q->p, q->occ, s, g, x);
     }
-    __device__ void store(uint32_t row, const float o[mlp::kOutPad]) const
-    {
-        mlp::mixture_record(o, q->mix + (size_t)row * mlp::kMixFloats);
-    }
-    __device__ void dump_h(int, uint32_t, const uint8_t*, uint32_t) const {}
+    __device__ void dump_h(int, uint32_t, uint32_t, const uint4*) const {}
+    __device__ void dump_out(uint32_t, uint32_t, float) const {}
 };
 
 // Learned proposal of the quadrotor queries in qidx: one mixture record per frontier entry,

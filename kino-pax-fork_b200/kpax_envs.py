@@ -196,3 +196,23 @@ def batch_queries(n: int = 1024, seed: int = 4, mix=(0.4, 0.3, 0.3), obs_range=(
         out.append({"model": model, "n_obs": n_obs, "tree": tree, "start": start, "goal": goal,
                     "obstacles": boxes_avoiding(rng, n_obs, (a, b))})
     return out
+
+
+def learned_family(seed: int, obs_range=(200, 2000), min_sep: float = 25.0, max_sep: float = 45.0, fixed: bool = False):
+    """The learned-proposal family of the 12D quadrotor: a 'building' scene (windowed wall at
+    x = 50 plus random boxes) with a seeded obstacle count uniform in obs_range.  Start and goal
+    are uniform in [5, 95]^3, min_sep..max_sep apart (within the reach of a 2^20-node plain tree
+    under the +-0.1 torque limits) and off the wall, or with `fixed` the benchmark pair
+    (10, 8, 5) -> (80, 95, 90).  Returns (obstacles, start, goal)."""
+    rng = np.random.default_rng(seed)
+    n_total = int(rng.integers(obs_range[0], obs_range[1], endpoint=True))
+    if fixed:
+        return quad_scene(seed=seed, n_total=n_total)
+    while True:
+        a, b = rng.uniform(5.0, 95.0, 3), rng.uniform(5.0, 95.0, 3)
+        off_wall = abs(a[0] - WALL_X) > 2.0 and abs(b[0] - WALL_X) > 2.0
+        if off_wall and min_sep <= np.linalg.norm(a - b) <= max_sep:
+            break
+    start, goal = np.zeros(12, np.float32), np.zeros(12, np.float32)
+    start[:3], goal[:3] = a, b
+    return building(n_total, seed, start[:3], goal[:3]), start, goal

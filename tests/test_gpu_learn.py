@@ -182,28 +182,30 @@ def tc_check(scene, n, seed):
     out, mix = d_out.cpu().numpy(), d_mix.cpu().numpy()
     W1, b1, W2, b2, W3, b3 = M.unpack(w)
     x = M.features(s, g, occ)
-    # layer by layer, each from the GPU's own input: BF16 activations within one BF16 ulp, or,
-    # where the sum cancels to near zero, within the FP32 accumulation error 1e-6 * sum |terms|
+    # layer by layer, each from the GPU's own input: BF16 activations within one BF16 ulp plus the
+    # error of the kernel's SiLU (0.5 z (1 + tanh.approx(z / 2)), |tanh error| < 2^-10.9, so
+    # |error| < 2^-11.9 |z|) and the FP32 accumulation error 1e-6 * sum |terms|
     for name, h_in, W, b, h_gpu in (("h1", x, W1, b1, h1), ("h2", h1, W2, b2, h2)):
-        act, _ = M.layer_bf16(h_in, W, b, act=True)
+        act, z = M.layer_bf16(h_in, W, b, act=True)
         want = M.bf16(act)
         bound = np.abs(M.bf16(h_in).astype(np.float64)) @ np.abs(M.bf16(W).astype(np.float64)).T
         diff = np.abs(h_gpu.astype(np.float64) - want)
-        assert np.all(diff <= _ulp_bf16(want) * 1.01 + 1e-6 * bound), (name, float(diff.max()))
-        frac = np.mean(diff > 0)
-        assert frac < 0.02, (name, frac)
+        tol = _ulp_bf16(want) * 1.01 + 2.0 ** -11.9 * np.abs(z) + 1e-6 * bound
+        assert np.all(diff <= tol), (name, float((diff - tol).max()))
+        assert np.mean(diff) <= 0.5 * np.mean(_ulp_bf16(want)), name
     # outputs: FP32 sums of exact BF16 products
     z = M.bf16(h2).astype(np.float64) @ M.bf16(W3).astype(np.float64).T
     bound = np.abs(M.bf16(h2).astype(np.float64)) @ np.abs(M.bf16(W3).astype(np.float64)).T
     want = z + b3
-    assert np.all(np.abs(out - want) <= 1e-5 * bound + 1e-5 * np.abs(b3) + 1e-6)
-    rec = M.mixture_record(out[:, : M.OUT])
+    out = out[:, : M.OUT]
+    assert np.all(np.abs(out - want[:, : M.OUT]) <= 1e-5 * bound[:, : M.OUT] + 1e-5 * np.abs(b3[: M.OUT]) + 1e-6)
+    rec = M.mixture_record(out)
     assert np.max(np.abs(mix[:, : M.COMP] - rec[:, : M.COMP])) <= 1e-6
     rel = np.abs(mix[:, M.COMP:] - rec[:, M.COMP:]) / np.maximum(np.abs(rec[:, M.COMP:]), 1e-3)
     assert rel.max() <= 1e-5, rel.max()
     # end to end against the oracle's own BF16 pass (no teacher forcing): small drift only
     _, _, o_ref = M.forward_bf16(w, x)
-    assert np.max(np.abs(out - o_ref)) <= 0.02 * max(1.0, np.max(np.abs(o_ref)))
+    assert np.max(np.abs(out - o_ref[:, : M.OUT])) <= 0.02 * max(1.0, np.max(np.abs(o_ref)))
     return out
 
 
