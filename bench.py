@@ -360,6 +360,12 @@ def run_batch(args) -> None:
     ptrs = [d_obs.data_ptr() + 24 * int(o) for o in offs[:-1]]
     starts, goals = [d["start"] for d in queries], [d["goal"] for d in queries]
     batch = kpax.Batch(cfgs)
+    net = None
+    if args.proposal == "on":
+        import kpax_learn as L
+
+        net = L.load_network(L.DEFAULT_WEIGHTS)
+        batch.set_proposal(net, args.eps)
     d_obs.copy_(h_obs)
     for _ in range(args.warmup):
         batch.plan(starts, goals, ptrs, sizes)
@@ -392,6 +398,7 @@ def run_batch(args) -> None:
         "config": {"workload": f"batched: {args.queries} queries, 40/30/30 % double integrator / Dubins / quadrotor, "
                                "obstacles log-U[10,5000], trees log-U[2^14,2^20], start/goal >= 50 apart, one launch per "
                                "stage for all queries", "l2": "each step is a whole batch plan (~GB working set)",
+                   "learned_proposal": f"quadrotor queries, epsilon {args.eps}" if net is not None else "off",
                    "parallelism": f"replicas x{ws}"},
         "plans_per_s": n_plans / (tot_ms / 1000.0),
         "success_rate": found / max(n_plans, 1),
@@ -407,13 +414,104 @@ def run_batch(args) -> None:
         print(json.dumps(line), flush=True)
 
 
+def run_learned(args) -> None:
+    """Learned proposal on the 12D quadrotor: the shipped network (trained on the GPU by the
+    library's kernels) against the plain uniform sampler on held-out scenes of the learned
+    family, with the same random streams; plus the tensor-core proposal pass and the training
+    step measured on their own."""
+    import torch
+
+    import kpax_learn as L
+
+    ws, rank, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    cfg = L.quad_config()
+    w, meta = L.load_params(L.DEFAULT_WEIGHTS)
+    net = kpax.MLP(max_batch=4096)
+    net.set_params(w)
+    seeds = [L.EVAL_SEED0 + 1_000_000 * rank + i for i in range(args.seeds)]
+    L.evaluate(seeds[:2], cfg), L.evaluate(seeds[:2], cfg, net, args.eps)  # warm-up
+    launches0 = kpax.kernel_launches()
+    with Clocks(local) as clk:
+        t0 = time.perf_counter()
+        plain = L.evaluate(seeds, cfg, progress=True)
+        t1 = time.perf_counter()
+        learned = L.evaluate(seeds, cfg, net, args.eps, progress=True)
+        t2 = time.perf_counter()
+    launches = kpax.kernel_launches() - launches0
+    sp, sl = L.summarize(plain), L.summarize(learned)
+    # tensor-core proposal pass: 2^16 frontier entries (the quadrotor budget), device-timed
+    obs, start, goal = E.learned_family(seeds[0])
+    d_obs = torch.from_numpy(obs).cuda()
+    env = kpax.Env(cfg, d_obs.data_ptr(), obs.shape[0])
+    n = 1 << 16
+    g = torch.Generator(device="cuda").manual_seed(0)
+    st = (torch.rand((n, 12), device="cuda", generator=g) * 100).contiguous()
+    go = (torch.rand((n, 3), device="cuda", generator=g) * 100).contiguous()
+    mix = torch.zeros((n, kpax.MLP_MIX), device="cuda")
+    for _ in range(3):
+        net.propose(env, st.data_ptr(), 12, go.data_ptr(), n, mix.data_ptr())
+    ms = []
+    for _ in range(max(args.steps, 5)):
+        net.propose(env, st.data_ptr(), 12, go.data_ptr(), n, mix.data_ptr())
+        ms.append(net.last_propose_ms())
+    prop_ms = statistics.mean(ms)
+    flop = n * 202240
+    peaks = load_peaks()
+    peak_tf = float(peaks.get("bf16_tflops", 1590.0))
+    # training step: batch 4096, FP32 kernels (forward + backward ~ 3x the forward's FLOP)
+    X = torch.randn((1 << 16, kpax.MLP_FEATURES), device="cuda", generator=g)
+    Y = torch.randn((1 << 16, 5), device="cuda", generator=g)
+    idx = torch.randint(0, 1 << 16, (4096,), device="cuda", dtype=torch.int32, generator=g)
+    tnet = kpax.MLP(max_batch=4096)
+    tnet.set_params(L.init_params(1))
+    for _ in range(5):
+        tnet.train_step(X.data_ptr(), Y.data_ptr(), idx.data_ptr(), 4096, 1e-4)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(50):
+        tnet.train_step(X.data_ptr(), Y.data_ptr(), idx.data_ptr(), 4096, 1e-4)
+    e1.record()
+    torch.cuda.synchronize()
+    train_ms = e0.elapsed_time(e1) / 50
+    line = {
+        "metric": "p50 time-to-solution of solved plans, learned proposal (quadrotor)", "value": sl["p50_ms_solved"],
+        "unit": "ms", "n_gpus": ws, "steps": len(seeds), "warmup": 2, "ms_per_step": (t2 - t1) * 1e3 / len(seeds),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "bf16 inference / fp32 training",
+        "data": "synthetic",
+        "config": {"workload": f"learned proposal: {len(seeds)} held-out building scenes (200-2000 AABBs incl. windowed "
+                               "wall), start/goal 25-45 m apart, 12D quadrotor preset (2^16 expansions/iteration, 2^20 "
+                               f"nodes, 300 iterations), epsilon {args.eps}", "parallelism": f"replicas x{ws}",
+                   "network": "51-256-256-88 SiLU, 8-component mixture", "training": meta},
+        "plain": sp, "learned": sl,
+        "success_gain": sl["success"] - sp["success"],
+        "proposal_pass": {"rows": n, "ms": prop_ms, "tflops": flop / (prop_ms * 1e-3) / 1e12},
+        "roofline": {"bound": "tensor", "achieved": flop / (prop_ms * 1e-3) / 1e12, "peak": peak_tf, "unit": "TFLOP/s",
+                     "frac": flop / (prop_ms * 1e-3) / 1e12 / peak_tf, "traffic": None,
+                     "kernel": "k_forward_tc (tensor-core proposal pass, 202240 FLOP per row)",
+                     "peak_source": "measured bf16 burst" if "fallback" not in peaks else "fallback"},
+        "training_step": {"batch": 4096, "ms": train_ms, "samples_per_s": 4096 / (train_ms * 1e-3),
+                          "tflops": 3 * 202240 * 4096 / (train_ms * 1e-3) / 1e12},
+        "e2e": {"value": len(seeds) / (t2 - t1), "unit": "plans/s (learned arm, wall clock, obstacles copied per plan)",
+                "h2d_bytes_per_step": int(np.mean([E.learned_family(s)[0].nbytes for s in seeds[:8]])),
+                "d2h_bytes_per_step": 0},
+        "plain_plans_per_s_wall": len(seeds) / (t1 - t0),
+        "gpu_launches": launches, "clocks": clk.summary(),
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch"], default="quad")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "learned"], default="quad")
+    ap.add_argument("--seeds", type=int, default=256, help="held-out scenes of the learned workload")
+    ap.add_argument("--eps", type=float, default=0.2, help="uniform fraction of the learned proposal")
+    ap.add_argument("--proposal", choices=["on", "off"], default="on", help="learned proposal for batched quadrotor queries")
     ap.add_argument("--queries", type=int, default=1024)
     ap.add_argument("--plans", type=int, default=8)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
@@ -423,6 +521,8 @@ def main() -> None:
         run_reference(args)
     elif args.workload == "batch":
         run_batch(args)
+    elif args.workload == "learned":
+        run_learned(args)
     else:
         run_ours(args)
 

@@ -304,6 +304,8 @@ kpax_status kpax_mlp_features(kpax_env* env, const float* d_states, uint32_t str
 kpax_status kpax_mlp_propose(kpax_mlp* net, kpax_env* env, const float* d_states, uint32_t stride,
                              const float* d_goals, uint32_t n, float* d_mix, float* d_out,
                              uint16_t* d_h1, uint16_t* d_h2, void* stream);
+/* Device time (CUDA events on `stream`) of the tensor-core kernel of the last kpax_mlp_propose. */
+float kpax_mlp_last_propose_ms(const kpax_mlp* net);
 /* Turns the learned proposal on (net != NULL) or off for the planner's quadrotor plans.  The
  * packed image is copied, so the network may be trained further or destroyed afterwards. */
 kpax_status kpax_set_proposal(kpax_planner* planner, kpax_mlp* net, float epsilon);

@@ -334,6 +334,8 @@ struct kpax_mlp {
     float *d_o = nullptr, *d_a = nullptr, *d_z = nullptr, *ls = nullptr;
     uint64_t step = 0;
     bool packed = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // around the last tensor-core pass
+    float last_ms = 0.0f;
 };
 
 namespace kpax {
@@ -449,6 +451,8 @@ kpax_status kpax_mlp_create(uint32_t max_batch, kpax_mlp** out)
     KPAX_MLP_ALLOC(n->ls, B * 4);
 #undef KPAX_MLP_ALLOC
     if(cudaMallocHost(&n->h_loss, 4) != cudaSuccess) return set_error("kpax_mlp_create: pinned alloc"), fail(KPAX_ENOMEM);
+    if(cudaEventCreate(&n->ev0) != cudaSuccess || cudaEventCreate(&n->ev1) != cudaSuccess)
+        return set_error("kpax_mlp_create: event creation failed"), fail(KPAX_ECUDA);
     if(cudaMemset(n->w, 0, P * 4) != cudaSuccess || cudaMemset(n->m, 0, P * 4) != cudaSuccess ||
        cudaMemset(n->v, 0, P * 4) != cudaSuccess || cudaMemset(n->err, 0, 4) != cudaSuccess ||
        cudaMemset(n->img, 0, kImgBytes) != cudaSuccess)
@@ -467,11 +471,15 @@ kpax_status kpax_mlp_destroy(kpax_mlp* n)
     for(void* p : dev)
         if(p) cudaFree(p);
     if(n->h_loss) cudaFreeHost(n->h_loss);
+    if(n->ev0) cudaEventDestroy(n->ev0);
+    if(n->ev1) cudaEventDestroy(n->ev1);
     delete n;
     return KPAX_OK;
 }
 
 uint32_t kpax_mlp_num_params(void) { return (uint32_t)kNumParams; }
+
+float kpax_mlp_last_propose_ms(const kpax_mlp* n) { return n ? n->last_ms : 0.0f; }
 
 kpax_status kpax_mlp_set_params(kpax_mlp* n, const float* h_params, void* stream)
 {
@@ -624,12 +632,15 @@ kpax_status kpax_mlp_propose(kpax_mlp* net, kpax_env* e, const float* d_states, 
     const uint32_t tiles = (n + tc::kRows - 1) / tc::kRows;
     ArraySrc src{e->params, e->d_occ, d_states, d_goals, stride, n, d_mix, d_out, d_h1, d_h2};
     KPAX_CUDA(cudaMemsetAsync(net->err, 0, 4, st));
+    KPAX_CUDA(cudaEventRecord(net->ev0, st));
     k_forward_tc<<<std::min<uint32_t>(tiles, (uint32_t)sms), tc::kThreads, tc::kSmemBytes, st>>>(src, net->img, net->err);
     count_launch();
     KPAX_CHECK_LAUNCH();
+    KPAX_CUDA(cudaEventRecord(net->ev1, st));
     uint32_t h_err = 0;
     KPAX_CUDA(cudaMemcpyAsync(&h_err, net->err, 4, cudaMemcpyDeviceToHost, st));
     KPAX_CUDA(cudaStreamSynchronize(st));
+    KPAX_CUDA(cudaEventElapsedTime(&net->last_ms, net->ev0, net->ev1));
     if(h_err) return set_error("kpax_mlp_propose: a tensor-core pipeline wait expired (code %u)", h_err), KPAX_ETIMEOUT;
     return KPAX_OK;
 }

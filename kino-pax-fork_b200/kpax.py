@@ -157,6 +157,7 @@ _SIGNATURES = {
     "kpax_env_occupancy": (_I32, [_VP, _VP, _VP]),
     "kpax_mlp_features": (_I32, [_VP, _VP, _U32, _VP, _U32, _VP, _VP]),
     "kpax_mlp_propose": (_I32, [_VP, _VP, _VP, _U32, _VP, _U32, _VP, _VP, _VP, _VP, _VP]),
+    "kpax_mlp_last_propose_ms": (ctypes.c_float, [_VP]),
     "kpax_set_proposal": (_I32, [_VP, _VP, ctypes.c_float]),
     "kpax_export_proposal": (_I32, [_VP, _VP, _U32, _VP]),
     "kpax_batch_set_proposal": (_I32, [_VP, _VP, ctypes.c_float, _VP]),
@@ -519,6 +520,9 @@ class MLP:
                 d_h1: int | None = None, d_h2: int | None = None) -> None:
         check(load().kpax_mlp_propose(self._h, env.handle, d_states, stride, d_goals, n, d_mix, d_out or None, d_h1 or None,
                                       d_h2 or None, self.stream), "kpax_mlp_propose")
+
+    def last_propose_ms(self) -> float:
+        return float(load().kpax_mlp_last_propose_ms(self._h))
 
     def close(self) -> None:
         if self._h:
