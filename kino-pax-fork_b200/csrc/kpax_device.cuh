@@ -82,6 +82,21 @@ __device__ __forceinline__ void sincos_checked(float x, float* sn, float* cs)
     if(!(fabsf(x) <= kTrigFastMax)) sincosf(x, sn, cs);  // huge or non-finite arguments
 }
 
+// sin and cos of a0 + d from s0 = sin(a0), c0 = cos(a0) by the angle-sum identity, with the
+// Taylor series of sin(d) to d^7 and cos(d) - 1 to d^8: for |d| <= kShiftMax the truncation error
+// is below 2e-11, so the result is within a few ulp of sin/cos of the rounded sum a0 + d.  The RK4
+// stages evaluate the attitude at a0 + (h/2) k and a0 + h k; this replaces three of every four
+// full evaluations per angle and step.
+constexpr float kShiftMax = 0.25f;
+__device__ __forceinline__ void sincos_shift(float s0, float c0, float d, float* sn, float* cs)
+{
+    const float d2 = d * d;
+    const float sd = fmaf(d * d2, fmaf(d2, fmaf(d2, -1.0f / 5040.0f, 1.0f / 120.0f), -1.0f / 6.0f), d);
+    const float cm = d2 * fmaf(d2, fmaf(d2, fmaf(d2, 1.0f / 40320.0f, -1.0f / 720.0f), 1.0f / 24.0f), -0.5f);
+    *sn = fmaf(s0, cm, fmaf(c0, sd, s0));
+    *cs = fmaf(c0, cm, fmaf(-s0, sd, c0));
+}
+
 // float -> int with the reference's device semantics (saturating, NaN -> 0).
 __device__ __forceinline__ int f2i(float x) { return __float2int_rz(x); }
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
@@ -304,22 +319,18 @@ __device__ __forceinline__ bool prop_dubins(const KParams& p, const Grid& g, flo
         const float p0[3] = {s[0], s[1], s[2]};
         const float yaw = s[3], pitch = s[4], v = s[5];
         float sp0, cp0, sy0, cy0, sp1, cp1, sy1, cy1, sp2, cp2, sy2, cy2;
-        const float p1 = pitch + hh * pr, y1 = yaw + hh * yr, p2 = pitch + h * pr, y2 = yaw + h * yr;
-        sincos_fast(pitch, &sp0, &cp0);
-        sincos_fast(yaw, &sy0, &cy0);
-        sincos_fast(p1, &sp1, &cp1);
-        sincos_fast(y1, &sy1, &cy1);
-        sincos_fast(p2, &sp2, &cp2);
-        sincos_fast(y2, &sy2, &cy2);
-        if(!(fmaxf(fmaxf(fabsf(yaw), fabsf(y1)), fabsf(y2)) <= kTrigFastMax)) {
-            sincosf(yaw, &sy0, &cy0);
-            sincosf(y1, &sy1, &cy1);
-            sincosf(y2, &sy2, &cy2);
-        }
-        if(!(fmaxf(fmaxf(fabsf(pitch), fabsf(p1)), fabsf(p2)) <= kTrigFastMax)) {
-            sincosf(pitch, &sp0, &cp0);
-            sincosf(p1, &sp1, &cp1);
-            sincosf(p2, &sp2, &cp2);
+        sincos_checked(pitch, &sp0, &cp0);
+        sincos_checked(yaw, &sy0, &cy0);
+        if(fmaxf(fabsf(h * pr), fabsf(h * yr)) <= kShiftMax) {
+            sincos_shift(sp0, cp0, hh * pr, &sp1, &cp1);
+            sincos_shift(sy0, cy0, hh * yr, &sy1, &cy1);
+            sincos_shift(sp0, cp0, h * pr, &sp2, &cp2);
+            sincos_shift(sy0, cy0, h * yr, &sy2, &cy2);
+        } else {
+            sincos_checked(pitch + hh * pr, &sp1, &cp1);
+            sincos_checked(yaw + hh * yr, &sy1, &cy1);
+            sincos_checked(pitch + h * pr, &sp2, &cp2);
+            sincos_checked(yaw + h * yr, &sy2, &cy2);
         }
         const float vm = v + hh * a, ve = v + h * a;
         const float mx = vm * cp1 * cy1, my = vm * cp1 * sy1, mz = vm * sp1;
@@ -348,20 +359,23 @@ __device__ __forceinline__ bool prop_dubins(const KParams& p, const Grid& g, flo
 
 // Quadrotor right-hand side, statePropagator.cu:325-370, evaluated at x0 + delta*k.
 // Model constants NU 10e-3, MU 2e-6, IX 1, IY 1, IZ 2, GRAVITY -9.81, MASS 1 (config.h:300-308).
-__device__ __forceinline__ void quad_rhs(float* xd, const float* x0, const float* k, float delta, const float* c)  // xd may alias k
+// trig0: (sin, cos) of the three Euler angles of x0.
+__device__ __forceinline__ void quad_rhs(float* xd, const float* x0, const float* k, float delta, const float* c,
+                                         const float* trig0)  // xd may alias k
 {
     const float NU = 10e-3f, MU = 2e-6f, G = -9.81f;
-    const float phi = x0[3] + delta * k[3], theta = x0[4] + delta * k[4], psi = x0[5] + delta * k[5];
     const float u = x0[6] + delta * k[6], v = x0[7] + delta * k[7], w = x0[8] + delta * k[8];
     const float pp = x0[9] + delta * k[9], q = x0[10] + delta * k[10], r = x0[11] + delta * k[11];
     float sf, cf, st, ct, sp, cp;
-    sincos_fast(phi, &sf, &cf);
-    sincos_fast(theta, &st, &ct);
-    sincos_fast(psi, &sp, &cp);
-    if(!(fmaxf(fabsf(phi), fmaxf(fabsf(theta), fabsf(psi))) <= kTrigFastMax)) {
-        sincosf(phi, &sf, &cf);
-        sincosf(theta, &st, &ct);
-        sincosf(psi, &sp, &cp);
+    const float d0 = delta * k[3], d1 = delta * k[4], d2 = delta * k[5];
+    if(fmaxf(fabsf(d0), fmaxf(fabsf(d1), fabsf(d2))) <= kShiftMax) {
+        sincos_shift(trig0[0], trig0[1], d0, &sf, &cf);
+        sincos_shift(trig0[2], trig0[3], d1, &st, &ct);
+        sincos_shift(trig0[4], trig0[5], d2, &sp, &cp);
+    } else {  // large attitude increments or non-finite values: evaluate at the rounded angles
+        sincos_checked(x0[3] + d0, &sf, &cf);
+        sincos_checked(x0[4] + d1, &st, &ct);
+        sincos_checked(x0[5] + d2, &sp, &cp);
     }
     const float sec = __frcp_rn(ct);  // tan(theta) = sin * sec, 1/cos(theta) = sec
     xd[0] = ct * cp * u + (sf * st * cp - cf * sp) * v + (cf * st * cp + sf * sp) * w;
@@ -391,13 +405,16 @@ __device__ __forceinline__ bool prop_quad(const KParams& p, const Grid& g, float
     int i = 0;
     for(; i < steps; ++i) {
         const float p0[3] = {s[0], s[1], s[2]};
-        float k[12], acc[12];
+        float k[12], acc[12], trig0[6];
+        sincos_checked(s[3], &trig0[0], &trig0[1]);
+        sincos_checked(s[4], &trig0[2], &trig0[3]);
+        sincos_checked(s[5], &trig0[4], &trig0[5]);
 #pragma unroll
         for(int j = 0; j < 12; ++j) k[j] = 0.0f;
 #pragma unroll 1
         for(int stage = 0; stage < 4; ++stage) {
             const float delta = stage == 0 ? 1.0f : (stage == 3 ? h : hh);
-            quad_rhs(k, s, k, delta, c);
+            quad_rhs(k, s, k, delta, c, trig0);
             if(stage == 0) {
 #pragma unroll
                 for(int j = 0; j < 12; ++j) acc[j] = k[j];

@@ -326,7 +326,29 @@ def main(argv=None):
     e.add_argument("--seeds", type=int, default=256)
     e.add_argument("--eps", type=float, default=0.2)
     e.add_argument("--max-iter", type=int, default=0)
+    pp = sub.add_parser("propose", help="time the tensor-core proposal pass on random states")
+    pp.add_argument("--weights", type=Path, default=DEFAULT_WEIGHTS)
+    pp.add_argument("--rows", type=int, default=1 << 16)
+    pp.add_argument("--reps", type=int, default=10)
     a = ap.parse_args(argv)
+    if a.cmd == "propose":
+        import torch
+
+        net = load_network(a.weights)
+        obs, _, _ = E.learned_family(EVAL_SEED0)
+        d_obs = torch.from_numpy(obs).cuda()
+        env = kpax.Env(quad_config(), d_obs.data_ptr(), obs.shape[0])
+        g = torch.Generator(device="cuda").manual_seed(0)
+        st = (torch.rand((a.rows, 12), device="cuda", generator=g) * 100).contiguous()
+        go = (torch.rand((a.rows, 3), device="cuda", generator=g) * 100).contiguous()
+        mix = torch.zeros((a.rows, kpax.MLP_MIX), device="cuda")
+        ms = []
+        for _ in range(a.reps):
+            net.propose(env, st.data_ptr(), 12, go.data_ptr(), a.rows, mix.data_ptr())
+            ms.append(net.last_propose_ms())
+        t = float(np.median(ms))
+        print(json.dumps({"rows": a.rows, "ms_median": t, "tflops": a.rows * 202240 / (t * 1e-3) / 1e12}))
+        return
     cfg = quad_config(a.max_iter or None)
     if a.cmd == "train":
         seeds = [TRAIN_SEED0 + i for i in range(a.envs)]
