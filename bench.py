@@ -249,6 +249,11 @@ def run_ours(args) -> None:
     cfg = kpax.preset(pre)
     cfg.seed = cfg.seed + 1000003 * rank
     obs, start, goal = scene()
+    tuning = None
+    if not args.no_tune:  # launch parameters from the autotuner's cache (plans are unchanged)
+        import kpax_autotune
+
+        cfg, tuning = kpax_autotune.tuned(cfg, obs.shape[0])
     d_obs = torch.from_numpy(obs).cuda()
     pl = kpax.KPAX(cfg)
     stream = torch.cuda.ExternalStream(pl.stream)
@@ -318,6 +323,9 @@ def run_ours(args) -> None:
             "ms_per_step": 1000 * t_s / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "fp32", "data": "synthetic",
             "config": {"workload": desc, "expansions_per_iter": cfg.expansions_per_iter,
+                       "launch": {"block_size": cfg.block_size or 448, "samples_per_thread": cfg.samples_per_thread or 1,
+                                  "hash_cell_size": cfg.hash_cell_size,
+                                  "source": "autotuner cache" if tuning else "defaults"},
                        "children_per_step": tot["children"] // args.steps, "l2": "flushed before each timed iteration "
                        "(256 MiB write, outside the events)", "parallelism": f"replicas x{ws}"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
@@ -353,6 +361,17 @@ def run_batch(args) -> None:
     torch.cuda.set_device(local)
     queries = E.batch_queries(args.queries, seed=4 + 1000 * rank)
     cfgs = batch_configs(queries)
+    tuned_models = {}
+    if not args.no_tune:  # per model: the cached parameters of its single-query workload
+        import kpax_autotune
+
+        for name, m in (("quad", kpax.MODEL_QUADROTOR), ("dubins", kpax.MODEL_DUBINS_AIRPLANE),
+                        ("di", kpax.MODEL_DOUBLE_INTEGRATOR)):
+            pre, scene, _ = WORKLOADS[name]
+            _, best = kpax_autotune.tuned(kpax.preset(pre), scene()[0].shape[0])
+            if best:
+                tuned_models[m] = best
+        cfgs = [kpax_autotune.apply(c, tuned_models[c.model]) if c.model in tuned_models else c for c in cfgs]
     sizes = [d["obstacles"].shape[0] for d in queries]
     offs = np.concatenate([[0], np.cumsum(sizes)])
     h_obs = torch.from_numpy(np.concatenate([d["obstacles"] for d in queries])).pin_memory()
@@ -399,6 +418,7 @@ def run_batch(args) -> None:
                                "obstacles log-U[10,5000], trees log-U[2^14,2^20], start/goal >= 50 apart, one launch per "
                                "stage for all queries", "l2": "each step is a whole batch plan (~GB working set)",
                    "learned_proposal": f"quadrotor queries, epsilon {args.eps}" if net is not None else "off",
+                   "launch": {str(m): v for m, v in tuned_models.items()} or "defaults",
                    "parallelism": f"replicas x{ws}"},
         "plans_per_s": n_plans / (tot_ms / 1000.0),
         "success_rate": found / max(n_plans, 1),
@@ -516,6 +536,7 @@ def main() -> None:
     ap.add_argument("--plans", type=int, default=8)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="ignore the autotuner's cached launch parameters")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -90,9 +90,10 @@ typedef struct kpax_config {
     uint32_t sparse_repeat;         /* repeat of a new node in a sparse region (15, KPAX.cu:477) */
     int32_t sparse_valid_threshold; /* region is sparse if valid count < this (10, KPAX.cu:476) */
     uint64_t seed;                  /* Philox4x32-10 key (the reference seeds cuRAND from the clock) */
-    int32_t block_size;             /* threads per CTA for the expansion kernel (0 = default) */
+    int32_t block_size;             /* threads per CTA of the expansion kernel: 0 (= 448), 128, 256, 448, 512 */
     int32_t unroll_iters;           /* planner iterations per captured CUDA graph (0 = default) */
-    int32_t reserved[8];
+    int32_t samples_per_thread;     /* children per expansion thread, 0 (= 1) .. 8 (grid-stride rounds) */
+    int32_t reserved[7];
 } kpax_config;
 
 /* Result of kpax_plan (the reference exposes these as public fields h_pathToGoal_, h_itr_,

@@ -279,8 +279,10 @@ kpax_status kpax_config_validate(const kpax_config* c)
     KPAX_REQ(c->root_repeat >= 1 && c->root_repeat <= 254, "root_repeat in [1,254]");
     KPAX_REQ(c->sparse_repeat >= 1 && c->sparse_repeat <= 254, "sparse_repeat in [1,254]");
     KPAX_REQ(c->epsilon > 0.0f, "epsilon must be positive");
-    KPAX_REQ(c->block_size == 0 || (c->block_size >= 32 && c->block_size <= 1024 && c->block_size % 32 == 0),
-             "block_size must be a multiple of 32 in [32,1024]");
+    KPAX_REQ(c->block_size == 0 || c->block_size == 128 || c->block_size == 256 || c->block_size == 448 ||
+               c->block_size == 512,
+             "block_size must be 0 (default), 128, 256, 448 or 512");
+    KPAX_REQ(c->samples_per_thread >= 0 && c->samples_per_thread <= 8, "samples_per_thread in [0,8]");
     KPAX_REQ(c->unroll_iters >= 0 && c->unroll_iters <= 64, "unroll_iters in [0,64]");
 #undef KPAX_REQ
     return KPAX_OK;

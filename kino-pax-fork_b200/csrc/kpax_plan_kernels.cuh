@@ -28,7 +28,8 @@ namespace plan {
 constexpr uint8_t kPending = 255;
 constexpr uint32_t kNone = 0xFFFFFFFFu;
 constexpr int kFrontierBS = 256, kItems = 4, kTile = kFrontierBS * kItems;
-constexpr int kExpandBS = 448;  // 2^16 children over 148 SMs: one 14-warp block per SM
+constexpr int kExpandBS = 448;  // default: 2^16 children over 148 SMs, one 14-warp block per SM
+constexpr int kExpandBSMin = 128;  // smallest expansion block (sizes the look-back status array)
 constexpr int kScoreBS = 256, kPartials = 1024;
 constexpr uint32_t kSpinLimit = 1u << 22;  // ~4 s of polling before a wait gives up
 constexpr uint32_t kErrTimeout = 1u, kErrCapacity = 2u, kErrProposal = mlp::tc::kErrWait;
@@ -406,12 +407,15 @@ __global__ void __launch_bounds__(kFrontierBS) k_frontier_write(const QueryDev* 
     }
 }
 
-template <int M>
-__global__ void __launch_bounds__(kExpandBS) k_expand(const QueryDev* __restrict__ qs, const uint32_t* __restrict__ qidx,
-                                                      uint32_t* __restrict__ active)
+// Expansion of the children of one query (blockIdx.y).  Children form look-back tiles of BS
+// consecutive children; a block processes `spt` tiles in grid-stride rounds (tile = round *
+// gridDim.x + blockIdx.x), so every block's round r only waits on tiles of round r or earlier.
+template <int M, int BS>
+__global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_expand(const QueryDev* __restrict__ qs, const uint32_t* __restrict__ qidx,
+                                               uint32_t* __restrict__ active)
 {
     constexpr int SD = ModelDims<M>::SD, CD = ModelDims<M>::CD, S = SD + CD + 1;
-    constexpr int NW = kExpandBS / 32;
+    constexpr int NW = BS / 32;
     __shared__ QueryDev sq;
     __shared__ uint32_t s_excl, s_ok;
     __shared__ uint32_t s_wn[NW], s_wv[NW], s_ws[NW];
@@ -422,96 +426,101 @@ __global__ void __launch_bounds__(kExpandBS) k_expand(const QueryDev* __restrict
     const uint32_t n = ctl->n, k = ctl->k, tree = ctl->tree, iter = ctl->iter, plan = ctl->plan_idx, epoch = ctl->epoch;
     const uint32_t ready = ctl->scores_ready;
     const float total = ctl->score_total;
-    const uint32_t nblk = n ? (n + kExpandBS - 1) / kExpandBS : 1u, b = blockIdx.x;
-    if(b >= nblk) return;
+    const uint32_t ntile = n ? (n + BS - 1) / BS : 1u;
     const TreeDev& t = sq.t;
     const RegDev& rg = sq.rg;
-    const uint32_t c = b * kExpandBS + threadIdx.x;
-    const bool active_child = c < n;
-    bool valid = false, next = false;
-    float s[SD], cc[4], rc[4], u[6];
-    uint32_t parent = 0;
-    int r1v = 0, r2v = 0, steps = 0, steps_done = 0;
-    if(active_child) {
-        parent = sq.entries[c / k];
-        load_state<SD>(t, parent, s);
-        child_draws(p, plan, iter, c, u);
-        if constexpr(M == KPAX_MODEL_QUADROTOR) {
-            if(sq.mix) mlp::mixture_draws(p, sq.mix + (size_t)(c / k) * mlp::kMixFloats, sq.prop_eps, plan, iter, c, u);
-        }
-        steps = draw_controls(p, u, cc);
-        valid = propagate<M>(p, sq.g, s, cc, steps, steps_done);
-        r1v = region_r1(p, s);
-        r2v = region_r2(p, s, r1v);
-        atomicAdd(rg.counter + r1v, 1);
-        if(valid) {
-            atomicAdd(rg.valid + r1v, 1);
-            const uint32_t word = (uint32_t)r2v >> 5, bit = 1u << (r2v & 31);
-            const bool seen = (__ldg(rg.cur + word) & bit) != 0u;
-            next = (u[5] < region_score(__ldg(rg.score + r1v), total, ready, p.eps)) || !seen;
-            atomicOr(rg.nxt + word, bit);
-        }
-        row_controls<M>(cc, rc);
-        if(sq.cap.rows) {
-            float* dst = sq.cap.rows + (size_t)c * S;
-            for(int q = 0; q < SD; ++q) dst[q] = s[q];
-            for(int q = 0; q < CD; ++q) dst[SD + q] = rc[q];
-            dst[SD + CD] = __fmul_rn(p.h, (float)steps);
-            sq.cap.valid[c] = valid, sq.cap.r1[c] = r1v, sq.cap.r2[c] = r2v, sq.cap.next[c] = next;
-            sq.cap.parent[c] = (int32_t)parent;
-        }
-    }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t mn = __ballot_sync(0xffffffffu, next), mv = __ballot_sync(0xffffffffu, valid);
-    const uint32_t rank = __popc(mn & ((1u << lane) - 1u));
-    uint32_t wsteps = active_child ? (uint32_t)steps_done : 0u;  // RK4 steps executed (algorithmic work)
-#pragma unroll
-    for(int d = 16; d > 0; d >>= 1) wsteps += __shfl_xor_sync(0xffffffffu, wsteps, d);
-    if(lane == 0) s_wn[warp] = __popc(mn), s_wv[warp] = __popc(mv), s_ws[warp] = wsteps;
-    __syncthreads();
-    if(warp == 0) {
-        uint32_t acc = 0, nv = 0;
-        unsigned long long ns = 0;
-        for(int w = 0; w < NW; ++w) acc += s_wn[w], nv += s_wv[w], ns += s_ws[w];
-        uint32_t excl = 0;
-        bool ok = true;
-        if(b == 0) {
-            if(lane == 0) lb_publish(sq.lb, epoch, 2u, acc);
-        } else {
-            if(lane == 0) lb_publish(sq.lb + b, epoch, 1u, acc);
-            ok = lb_exclusive(sq.lb, b, epoch, excl);
-            if(ok && lane == 0) lb_publish(sq.lb + b, epoch, 2u, excl + acc);
-        }
-        if(lane == 0) {
-            if(nv) atomicAdd(&ctl->n_valid, (unsigned long long)nv);
-            if(ns) atomicAdd(&ctl->n_steps, ns);
-            if(!ok) {
-                atomicOr(&ctl->error, kErrTimeout);
-                finish_query(ctl, active);
+    for(uint32_t b = blockIdx.x; b < ntile; b += gridDim.x) {
+        const uint32_t c = b * BS + threadIdx.x;
+        const bool active_child = c < n;
+        bool valid = false, next = false;
+        float s[SD], cc[4], rc[4], u[6];
+        uint32_t parent = 0;
+        int r1v = 0, r2v = 0, steps = 0, steps_done = 0;
+        if(active_child) {
+            parent = sq.entries[c / k];
+            load_state<SD>(t, parent, s);
+            child_draws(p, plan, iter, c, u);
+            if constexpr(M == KPAX_MODEL_QUADROTOR) {
+                if(sq.mix) mlp::mixture_draws(p, sq.mix + (size_t)(c / k) * mlp::kMixFloats, sq.prop_eps, plan, iter, c, u);
             }
-            if(ok && b == nblk - 1) ctl->appended = excl + acc;
-            s_excl = excl;
-            s_ok = ok;
+            steps = draw_controls(p, u, cc);
+            valid = propagate<M>(p, sq.g, s, cc, steps, steps_done);
+            r1v = region_r1(p, s);
+            r2v = region_r2(p, s, r1v);
+            atomicAdd(rg.counter + r1v, 1);
+            if(valid) {
+                atomicAdd(rg.valid + r1v, 1);
+                const uint32_t word = (uint32_t)r2v >> 5, bit = 1u << (r2v & 31);
+                const bool seen = (__ldg(rg.cur + word) & bit) != 0u;
+                next = (u[5] < region_score(__ldg(rg.score + r1v), total, ready, p.eps)) || !seen;
+                atomicOr(rg.nxt + word, bit);
+            }
+            row_controls<M>(cc, rc);
+            if(sq.cap.rows) {
+                float* dst = sq.cap.rows + (size_t)c * S;
+                for(int q = 0; q < SD; ++q) dst[q] = s[q];
+                for(int q = 0; q < CD; ++q) dst[SD + q] = rc[q];
+                dst[SD + CD] = __fmul_rn(p.h, (float)steps);
+                sq.cap.valid[c] = valid, sq.cap.r1[c] = r1v, sq.cap.r2[c] = r2v, sq.cap.next[c] = next;
+                sq.cap.parent[c] = (int32_t)parent;
+            }
         }
+        const uint32_t mn = __ballot_sync(0xffffffffu, next), mv = __ballot_sync(0xffffffffu, valid);
+        const uint32_t rank = __popc(mn & ((1u << lane) - 1u));
+        uint32_t wsteps = active_child ? (uint32_t)steps_done : 0u;  // RK4 steps executed (algorithmic work)
+#pragma unroll
+        for(int d = 16; d > 0; d >>= 1) wsteps += __shfl_xor_sync(0xffffffffu, wsteps, d);
+        if(lane == 0) s_wn[warp] = __popc(mn), s_wv[warp] = __popc(mv), s_ws[warp] = wsteps;
+        __syncthreads();
+        if(warp == 0) {
+            uint32_t acc = 0, nv = 0;
+            unsigned long long ns = 0;
+            for(int w = 0; w < NW; ++w) acc += s_wn[w], nv += s_wv[w], ns += s_ws[w];
+            uint32_t excl = 0;
+            bool ok = true;
+            if(b == 0) {
+                if(lane == 0) lb_publish(sq.lb, epoch, 2u, acc);
+            } else {
+                if(lane == 0) lb_publish(sq.lb + b, epoch, 1u, acc);
+                ok = lb_exclusive(sq.lb, b, epoch, excl);
+                if(ok && lane == 0) lb_publish(sq.lb + b, epoch, 2u, excl + acc);
+            }
+            if(lane == 0) {
+                if(nv) atomicAdd(&ctl->n_valid, (unsigned long long)nv);
+                if(ns) atomicAdd(&ctl->n_steps, ns);
+                if(!ok) {
+                    atomicOr(&ctl->error, kErrTimeout);
+                    finish_query(ctl, active);
+                }
+                if(ok && b == ntile - 1) ctl->appended = excl + acc;
+                s_excl = excl;
+                s_ok = ok;
+            }
+        }
+        __syncthreads();
+        const bool block_ok = s_ok != 0u;
+        if(next && block_ok) {
+            uint32_t wex = 0;  // accepted children of the lower warps of this tile
+            for(int w = 0; w < warp; ++w) wex += s_wn[w];
+            const uint32_t slot = tree + s_excl + wex + rank;
+            if(slot >= p.cap) {
+                atomicOr(&ctl->error, kErrCapacity);
+            } else {
+                store_state<SD>(t, slot, s);
+                t.ctl[slot] = make_float4(rc[0], rc[1], rc[2], rc[3]);
+                t.dur[slot] = __fmul_rn(p.h, (float)steps);
+                t.parent[slot] = (int32_t)parent;
+                const float d = goal_distance(s, ctl->goal);
+                t.cost[slot] = d;
+                t.r1[slot] = r1v;
+                t.rep[slot] = kPending;
+                if(d < p.goal_thresh) atomicMin(&ctl->goal_idx, slot);
+            }
+        }
+        if(!block_ok) return;
+        __syncthreads();  // s_wn / s_excl are rewritten by the next round
     }
-    __syncthreads();
-    if(!next || !s_ok) return;
-    uint32_t wex = 0;  // accepted children of the lower warps of this block
-    for(int w = 0; w < warp; ++w) wex += s_wn[w];
-    const uint32_t slot = tree + s_excl + wex + rank;
-    if(slot >= p.cap) {
-        atomicOr(&ctl->error, kErrCapacity);
-        return;
-    }
-    store_state<SD>(t, slot, s);
-    t.ctl[slot] = make_float4(rc[0], rc[1], rc[2], rc[3]);
-    t.dur[slot] = __fmul_rn(p.h, (float)steps);
-    t.parent[slot] = (int32_t)parent;
-    const float d = goal_distance(s, ctl->goal);
-    t.cost[slot] = d;
-    t.r1[slot] = r1v;
-    t.rep[slot] = kPending;
-    if(d < p.goal_thresh) atomicMin(&ctl->goal_idx, slot);
 }
 
 // Region scores (Graph.cu:233-358): one warp per partial sum j, lane m scoring region j + 1024*m,

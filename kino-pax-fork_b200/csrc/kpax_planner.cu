@@ -33,6 +33,18 @@ struct Carver {
     }
 };
 
+// The expansion kernel at one of its block sizes (validated by kpax_config_validate).
+template <int M>
+void launch_expand(int bs, dim3 grid, cudaStream_t s, const QueryDev* dq, const uint32_t* qidx, uint32_t* active)
+{
+    switch(bs) {
+        case 128: k_expand<M, 128><<<grid, 128, 0, s>>>(dq, qidx, active); break;
+        case 256: k_expand<M, 256><<<grid, 256, 0, s>>>(dq, qidx, active); break;
+        case 512: k_expand<M, 512><<<grid, 512, 0, s>>>(dq, qidx, active); break;
+        default: k_expand<M, kExpandBS><<<grid, kExpandBS, 0, s>>>(dq, qidx, active); break;
+    }
+}
+
 struct PlanBatch {
     uint32_t nq = 0;
     std::vector<kpax_config> cfg;
@@ -46,6 +58,7 @@ struct PlanBatch {
     std::vector<uint32_t> groups[3];      // query indices per model (DI, Dubins, quad)
     uint32_t* d_groups[3] = {nullptr, nullptr, nullptr};
     uint32_t expand_gx[3] = {0, 0, 0};
+    int expand_bs[3] = {kExpandBS, kExpandBS, kExpandBS};  // block size per model group (its first query's)
     uint32_t gx_front = 1, gx_score = 1;
     Ctl* d_ctl = nullptr;
     Ctl* h_ctl = nullptr;
@@ -114,7 +127,7 @@ struct PlanBatch {
                 d.t.rep = cv.take<uint8_t>(cap_n);
                 d.entries = cv.take<uint32_t>(p.budget);
                 d.tiles = cv.take<uint32_t>((cap_n + kTile - 1) / kTile + 1);
-                d.lb = cv.take<unsigned long long>((p.budget + kExpandBS - 1) / kExpandBS + 1);
+                d.lb = cv.take<unsigned long long>((p.budget + kExpandBSMin - 1) / kExpandBSMin + 1);
                 d.partials = cv.take<float>(kPartials);
                 d.farr = cv.take<uint32_t>(1);
                 d.sarr = cv.take<uint32_t>(1);
@@ -163,8 +176,11 @@ struct PlanBatch {
         uint32_t max_tiles = 1;
         for(uint32_t q = 0; q < n; ++q) {
             const int m = prm[q].model - 1;
+            if(groups[m].empty()) expand_bs[m] = cfg[q].block_size > 0 ? cfg[q].block_size : kExpandBS;
             groups[m].push_back(q);
-            expand_gx[m] = std::max<uint32_t>(expand_gx[m], (prm[q].budget + kExpandBS - 1) / kExpandBS);
+            const uint32_t bs = (uint32_t)expand_bs[m], spt = cfg[q].samples_per_thread > 0 ? cfg[q].samples_per_thread : 1;
+            const uint32_t tiles = (prm[q].budget + bs - 1) / bs;
+            expand_gx[m] = std::max<uint32_t>(expand_gx[m], (tiles + spt - 1) / spt);
             max_tiles = std::max<uint32_t>(max_tiles, (prm[q].cap + kTile - 1) / kTile);
         }
         for(int m = 0; m < 3; ++m) {
@@ -263,9 +279,9 @@ struct PlanBatch {
             const dim3 grid(expand_gx[m], (uint32_t)groups[m].size());
             if(m == 2 && n_learned)
                 k_propose<<<dim3(gx_prop, n_learned), mlp::tc::kThreads, mlp::tc::kSmemBytes, s>>>(dq, d_learned);
-            if(m == 0) k_expand<KPAX_MODEL_DOUBLE_INTEGRATOR><<<grid, kExpandBS, 0, s>>>(dq, d_groups[m], d_active);
-            else if(m == 1) k_expand<KPAX_MODEL_DUBINS_AIRPLANE><<<grid, kExpandBS, 0, s>>>(dq, d_groups[m], d_active);
-            else k_expand<KPAX_MODEL_QUADROTOR><<<grid, kExpandBS, 0, s>>>(dq, d_groups[m], d_active);
+            if(m == 0) launch_expand<KPAX_MODEL_DOUBLE_INTEGRATOR>(expand_bs[m], grid, s, dq, d_groups[m], d_active);
+            else if(m == 1) launch_expand<KPAX_MODEL_DUBINS_AIRPLANE>(expand_bs[m], grid, s, dq, d_groups[m], d_active);
+            else launch_expand<KPAX_MODEL_QUADROTOR>(expand_bs[m], grid, s, dq, d_groups[m], d_active);
             if(u < nused - 1) cudaEventRecord(ev_join[u], s);
         }
         for(int u = 0; u + 1 < nused; ++u) cudaStreamWaitEvent(stream, ev_join[u], 0);

@@ -70,7 +70,8 @@ class Config(ctypes.Structure):
         ("seed", ctypes.c_uint64),
         ("block_size", ctypes.c_int32),
         ("unroll_iters", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 8),
+        ("samples_per_thread", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 7),
     ]
 
     @property

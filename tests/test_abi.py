@@ -59,7 +59,8 @@ def test_preset_values_follow_benchmark_configs():
 @pytest.mark.parametrize(
     "field,value",
     [("model", 7), ("state_dim", 5), ("max_tree_size", 1), ("step_size", 0.0), ("w_max", -1.0), ("c_r1_length", 40),
-     ("hash_cell_size", 0.0), ("children_per_entry", 0), ("expansions_per_iter", 0), ("c_dim", 9), ("block_size", 33)],
+     ("hash_cell_size", 0.0), ("children_per_entry", 0), ("expansions_per_iter", 0), ("c_dim", 9), ("block_size", 33),
+     ("block_size", 384), ("samples_per_thread", 9), ("samples_per_thread", -1)],
 )
 def test_invalid_configs_are_rejected_with_a_message(field, value):
     cfg = kpax.preset(kpax.PRESET_QUAD)
