@@ -251,6 +251,16 @@ kpax_status kpax_test_sincos(const float* d_x, uint32_t n, float* d_out, void* s
  * benchmark reports it as evidence that the device path ran. */
 uint64_t kpax_kernel_launches(void);
 
+/* ---- solution output (copyAndWriteVectorToCSV / writeVectorToCSV, helper.cuh:56-93) ------
+ * Rows of `cols` floats as CSV, each value printed "%.6f" (std::fixed, setprecision 6) and
+ * separated by commas, one row per line; append = 1 appends as the reference's append mode. */
+kpax_status kpax_write_rows_csv(const float* h_rows, uint32_t rows, uint32_t cols,
+                                const char* filename, int32_t append);
+/* The last plan's solution (KPAX.cu:621-627, controlPathToGoal.csv): SAMPLE_DIM columns, the goal
+ * node first and the root last (every row; the reference writes h_itr_ rows, Q12).  No file
+ * content is written when no path was found (an empty file unless appending). */
+kpax_status kpax_write_solution_csv(kpax_planner* planner, const char* filename, int32_t append);
+
 /* ---- learned proposal (no counterpart in the reference) ----------------------------------
  * The reference draws every control and duration uniformly (statePropagatorSpatialHash.cu,
  * propagateAndCheck).  A proposal network reshapes those draws for the quadrotor: an MLP

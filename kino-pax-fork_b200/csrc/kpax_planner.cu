@@ -650,6 +650,35 @@ kpax_status kpax_plan_iterate_timed(kpax_planner* pl, uint32_t n_iters, uint64_t
     return pl->b.iterate_timed(n_iters, flush_bytes, h_times, h_totals);
 }
 
+kpax_status kpax_write_rows_csv(const float* h_rows, uint32_t rows, uint32_t cols, const char* filename, int32_t append)
+{
+    if((!h_rows && rows) || !cols || !filename) return set_error("kpax_write_rows_csv: bad arguments"), KPAX_EINVAL;
+    FILE* f = fopen(filename, append ? "a" : "w");
+    if(!f) return set_error("kpax_write_rows_csv: cannot open %s", filename), KPAX_EINVAL;
+    char buf[64];
+    for(uint32_t i = 0; i < rows; ++i) {
+        for(uint32_t j = 0; j < cols; ++j) {  // std::fixed with 6 digits, as writeVectorToCSV (helper.cuh:56-80)
+            snprintf(buf, sizeof(buf), "%.6f", (double)h_rows[(size_t)i * cols + j]);
+            fputs(buf, f);
+            if(j + 1 < cols) fputc(',', f);
+        }
+        fputc('\n', f);
+    }
+    const bool ok = fflush(f) == 0;
+    fclose(f);
+    if(!ok) return set_error("kpax_write_rows_csv: write to %s failed", filename), KPAX_EINVAL;
+    return KPAX_OK;
+}
+
+kpax_status kpax_write_solution_csv(kpax_planner* pl, const char* filename, int32_t append)
+{
+    if(!pl || !pl->b.begun) return set_error("kpax_write_solution_csv: no plan"), KPAX_EINVAL;
+    kpax_result r{};
+    kpax_status st = pl->b.finish(&r);
+    if(st != KPAX_OK) return st;
+    return kpax_write_rows_csv(r.h_path, r.path_len, (uint32_t)pl->b.prm[0].S, filename, append);
+}
+
 kpax_status kpax_plan_result(kpax_planner* pl, kpax_result* out)
 {
     if(!pl || !pl->b.begun) return set_error("kpax_plan_result: no plan"), KPAX_EINVAL;

@@ -160,6 +160,8 @@ _SIGNATURES = {
     "kpax_mlp_propose": (_I32, [_VP, _VP, _VP, _U32, _VP, _U32, _VP, _VP, _VP, _VP, _VP]),
     "kpax_mlp_last_propose_ms": (ctypes.c_float, [_VP]),
     "kpax_set_proposal": (_I32, [_VP, _VP, ctypes.c_float]),
+    "kpax_write_rows_csv": (_I32, [_VP, _U32, _U32, ctypes.c_char_p, _I32]),
+    "kpax_write_solution_csv": (_I32, [_VP, ctypes.c_char_p, _I32]),
     "kpax_export_proposal": (_I32, [_VP, _VP, _U32, _VP]),
     "kpax_batch_set_proposal": (_I32, [_VP, _VP, ctypes.c_float, _VP]),
 }
@@ -370,6 +372,10 @@ class KPAX:
         """Learned proposal on (net) or off (None) for this quadrotor planner."""
         check(load().kpax_set_proposal(self._h, net.handle if net else None, float(epsilon)), "kpax_set_proposal")
 
+    def write_solution_csv(self, filename, append: bool = False) -> None:
+        """The last plan's path (goal first, root last) in the reference's controlPathToGoal.csv format."""
+        check(load().kpax_write_solution_csv(self._h, os.fsencode(filename), int(append)), "kpax_write_solution_csv")
+
     def export_proposal(self) -> np.ndarray:
         """Mixture records of the last iteration's frontier entries (E x 88)."""
         mix = np.zeros((self.cfg.expansions_per_iter, MLP_MIX), np.float32)
@@ -535,6 +541,15 @@ class MLP:
             self.close()
         except Exception:
             pass
+
+
+def write_rows_csv(rows: np.ndarray, filename, append: bool = False) -> None:
+    """Rows as CSV in the reference's format (6 decimals, comma-separated)."""
+    a = np.ascontiguousarray(rows, np.float32)
+    if a.ndim == 1:
+        a = a.reshape(1, -1)
+    check(load().kpax_write_rows_csv(_ptr(a), a.shape[0], a.shape[1], os.fsencode(filename), int(append)),
+          "kpax_write_rows_csv")
 
 
 def env_occupancy(env: Env, d_words: int, stream: int = 0) -> None:

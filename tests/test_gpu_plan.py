@@ -73,7 +73,7 @@ def test_di_plan_bit_exact_until_tree_full(cuda):
     assert_plans_equal(g, o)
 
 
-def test_di_plan_bit_exact_goal_found(cuda):
+def test_di_plan_bit_exact_goal_found(cuda, tmp_path):
     import torch
 
     cfg = small_di(fast=True)
@@ -87,6 +87,11 @@ def test_di_plan_bit_exact_goal_found(cuda):
     path = g["path"]
     assert np.linalg.norm(path[0, :3] - goal[:3]) < cfg.goal_thresh
     assert np.array_equal(path[-1, :6], s[:6])
+    # the solution file: controlPathToGoal.csv rows (goal first, root last), "%.6f" values
+    f = tmp_path / "controlPathToGoal.csv"
+    pl.write_solution_csv(f)
+    want = "".join(",".join(f"{float(v):.6f}" for v in r) + "\n" for r in path)
+    assert f.read_text() == want
     # a second plan on the same planner draws a new random stream (plan index 1)
     g2, _ = gpu_plan(torch, cfg, s, goal, obs, planner=pl)
     o2 = O.plan(cfg, s, goal, obs, plan_idx=1)
