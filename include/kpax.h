@@ -269,7 +269,9 @@ kpax_status kpax_write_solution_csv(kpax_planner* planner, const char* filename,
  * uniforms (4 controls, duration).  A fraction epsilon of the draws stays uniform and every
  * segment is still propagated and collision-checked exactly.
  * Layouts: features n x 64 floats (51 used), network outputs n x 96 floats (88 used), mixture
- * records n x 88 floats (8 cumulative weights, 8x5 means, 8x5 sigmas), logit targets n x 5. */
+ * records n x 88 floats (the outputs with biases: component k's logit at 11k, its 5 means at
+ * 11k+1.., its 5 raw log-sigmas at 11k+6.., sigma = exp(-2 + 5 tanh(raw / 5))), logit targets
+ * n x 5. */
 typedef struct kpax_mlp kpax_mlp;
 #define KPAX_MLP_FEATURES 64
 #define KPAX_MLP_OUTPUTS 96
@@ -320,7 +322,7 @@ float kpax_mlp_last_propose_ms(const kpax_mlp* net);
 /* Turns the learned proposal on (net != NULL) or off for the planner's quadrotor plans.  The
  * packed image is copied, so the network may be trained further or destroyed afterwards. */
 kpax_status kpax_set_proposal(kpax_planner* planner, kpax_mlp* net, float epsilon);
-/* Mixture records (88 floats each) of the frontier entries of the last iteration; child c of
+/* Mixture records (88 outputs each) of the frontier entries of the last iteration; child c of
  * that iteration drew from record c / k with k = children / entries. */
 kpax_status kpax_export_proposal(kpax_planner* planner, float* h_mix, uint32_t max_entries,
                                  uint32_t* n_entries);

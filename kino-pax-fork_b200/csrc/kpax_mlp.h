@@ -33,8 +33,9 @@ constexpr float kSigMid = -2.0f, kSigHalf = 5.0f;
 // Logit targets are clamped to +-kLogitClamp (u in [1e-4, 1 - 1e-4]).
 constexpr float kLogitClamp = 9.21024f;
 
-// Per-entry mixture record written by the proposal kernel: cumulative weights, means, sigmas.
-constexpr int kMixCdf = 0, kMixMu = kComp, kMixSigma = kComp + kComp * kDim, kMixFloats = kComp * (1 + 2 * kDim);
+// Per-entry mixture record written by the proposal pass: the network's 88 outputs with biases,
+// component k at [11k] (logit), [11k+1 .. 11k+5] (means), [11k+6 .. 11k+10] (raw log-sigmas).
+constexpr int kMixFloats = kOut;
 
 // BF16 image: slabs of 64 K-columns, each row 128 bytes, rows grouped by 8 into 1024-byte atoms,
 // the 16-byte chunk j of row r stored at chunk position j ^ (r & 7).

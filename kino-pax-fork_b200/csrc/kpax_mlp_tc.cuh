@@ -59,47 +59,35 @@ __device__ __forceinline__ void features(const KParams& p, const uint32_t* __res
     for(int i = kIn; i < kInPad; ++i) x[i] = 0.0f;
 }
 
-// Mixture record from the 88 network outputs (biases included): cumulative component weights
-// (softmax in component order, last entry exactly 1), means, sigmas = exp(s) with
-// s = kSigMid + kSigHalf * tanh(raw * (1 / kSigHalf)).
-__device__ __forceinline__ void mixture_record(const float* o, float* __restrict__ rec)
-{
-    float mx = o[0];
-#pragma unroll
-    for(int k = 1; k < kComp; ++k) mx = fmaxf(mx, o[k * kCompStride]);
-    float e[kComp], tot = 0.0f;
-#pragma unroll
-    for(int k = 0; k < kComp; ++k) e[k] = expf(o[k * kCompStride] - mx), tot += e[k];
-    float acc = 0.0f;
-#pragma unroll
-    for(int k = 0; k < kComp; ++k) {
-        acc += e[k];
-        rec[kMixCdf + k] = k == kComp - 1 ? 1.0f : acc / tot;
-    }
-#pragma unroll
-    for(int k = 0; k < kComp; ++k)
-#pragma unroll
-        for(int d = 0; d < kDim; ++d) {
-            rec[kMixMu + k * kDim + d] = o[k * kCompStride + 1 + d];
-            const float s = kSigMid + kSigHalf * tanhf(o[k * kCompStride + 1 + kDim + d] * (1.0f / kSigHalf));
-            rec[kMixSigma + k * kDim + d] = expf(s);
-        }
-}
-
-// Draws of child `index` from the mixture record of its entry.  u[] holds the plain uniform
-// draws on entry; they are kept when the Philox stream-3 uniform is <= eps (probability eps), else u[0..4] are
-// replaced by sigmoid(mu + sigma * n) of a component picked by the cumulative weights, with
-// Box-Muller normals from Philox streams 3 and 4.  u[5] (frontier acceptance) is never changed.
+// Draws of child `index` from the mixture record (network outputs) of its entry.  u[] holds the
+// plain uniform draws on entry; they are kept when the Philox stream-3 uniform is <= eps
+// (probability eps), else u[0..4] are replaced by sigmoid(mu + sigma * n): the component is the
+// first whose cumulative softmax weight reaches a stream-3 uniform (the last one if none), sigma
+// = exp(kSigMid + kSigHalf * tanh(raw / kSigHalf)), and n are Box-Muller normals from streams 3
+// and 4.  Only the drawn component's sigmas are evaluated.  u[5] (frontier acceptance) is never
+// changed.
 __device__ __forceinline__ void mixture_draws(const KParams& p, const float* __restrict__ rec, float eps, uint32_t stream,
                                               uint32_t iter, uint32_t index, float u[6])
 {
     const U4 a = philox(index, iter, 3u, stream, p.seed_lo, p.seed_hi);
     if(u01(a.x) <= eps) return;
     const U4 b = philox(index, iter, 4u, stream, p.seed_lo, p.seed_hi);
-    const float uc = u01(a.y);
-    int k = 0;
+    float lg[kComp], mx = -INFINITY;
 #pragma unroll
-    for(int j = 0; j < kComp - 1; ++j) k += __ldg(rec + kMixCdf + j) < uc ? 1 : 0;
+    for(int j = 0; j < kComp; ++j) lg[j] = __ldg(rec + j * kCompStride), mx = fmaxf(mx, lg[j]);
+    float e[kComp], tot = 0.0f;
+#pragma unroll
+    for(int j = 0; j < kComp; ++j) e[j] = expf(lg[j] - mx), tot += e[j];
+    const float target = u01(a.y) * tot;  // component: first with cumulative weight sum >= target
+    float acc = 0.0f;
+    int k = kComp - 1;
+    for(int j = 0; j < kComp - 1; ++j) {
+        acc += e[j];
+        if(acc >= target) {
+            k = j;
+            break;
+        }
+    }
     const uint32_t bm[6] = {a.z, a.w, b.x, b.y, b.z, b.w};
     float n[6];
 #pragma unroll
@@ -109,9 +97,11 @@ __device__ __forceinline__ void mixture_draws(const KParams& p, const float* __r
         sincospif(2.0f * u01(bm[2 * i + 1]), &sn, &cs);
         n[2 * i] = r * cs, n[2 * i + 1] = r * sn;
     }
+    const float* c = rec + k * kCompStride;
 #pragma unroll
     for(int d = 0; d < kDim; ++d) {
-        const float z = __ldg(rec + kMixMu + k * kDim + d) + __ldg(rec + kMixSigma + k * kDim + d) * n[d];
+        const float sg = expf(kSigMid + kSigHalf * tanhf(__ldg(c + 1 + kDim + d) * (1.0f / kSigHalf)));
+        const float z = __ldg(c + 1 + d) + sg * n[d];
         const float v = 1.0f / (1.0f + expf(-z));
         u[d] = fminf(fmaxf(v, 5.9604645e-8f), 1.0f);
     }
@@ -251,14 +241,18 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b)
     return *reinterpret_cast<const uint32_t*>(&h);
 }
 
-// SiLU(x) = x * sigmoid(x) = 0.5 x (1 + tanh(x / 2)), one MUFU operation (tanh.approx.f32,
-// absolute error below 2^-10.9); the result is rounded to BF16 afterwards.
-__device__ __forceinline__ float silu(float x)
+// SiLU of two values: x * sigmoid(x) = h + h * tanh(h) with h = x / 2, the tanh of both halves
+// in one MUFU operation (tanh.approx.bf16x2: h rounded to BF16, tanh returned in BF16), so
+// |error| < 2^-8 |x| before the result is rounded to BF16.
+__device__ __forceinline__ void silu2(float& x0, float& x1)
 {
-    const float hx = 0.5f * x;
-    float t;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(hx));
-    return fmaf(hx, t, hx);
+    const float h0 = 0.5f * x0, h1 = 0.5f * x1;
+    const __nv_bfloat162 hb = __floats2bfloat162_rn(h0, h1);
+    uint32_t tin = *reinterpret_cast<const uint32_t*>(&hb), tout;
+    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(tout) : "r"(tin));
+    const __nv_bfloat162 tb = *reinterpret_cast<const __nv_bfloat162*>(&tout);
+    x0 = fmaf(h0, __low2float(tb), h0);
+    x1 = fmaf(h1, __high2float(tb), h1);
 }
 
 // Named barrier of the 512 epilogue threads; the OR form returns a value uniform across them.
@@ -441,7 +435,10 @@ __device__ void forward(Src& src, const uint8_t* __restrict__ img, uint8_t* smem
                     for(int cc = 0; cc < 2; ++cc) {
                         const uint32_t col0 = cg * 64u + 32u * half + 16u * cc;
 #pragma unroll
-                        for(int k = 0; k < 16; ++k) v[cc][k] = silu(v[cc][k] + b[col0 + k]);
+                        for(int k = 0; k < 16; k += 2) {
+                            v[cc][k] += b[col0 + k], v[cc][k + 1] += b[col0 + k + 1];
+                            silu2(v[cc][k], v[cc][k + 1]);
+                        }
                         uint4 bits[2];
                         store_row16(sm + kSmH, r, col0, v[cc], bits);
                         if constexpr(Src::kDebug) {
@@ -456,51 +453,24 @@ __device__ void forward(Src& src, const uint8_t* __restrict__ img, uint8_t* smem
             };
             if(!hidden(1, kBarD1, 0u, bias, kBarHF)) break;
             if(!hidden(2, kBarD2, 256u, bias + kH, kBarGF)) break;
-            // records: warp group cg handles components 2cg and 2cg + 1, and (cg 0) the weights
+            // records: the outputs plus biases; warp group cg stages columns 22cg .. 22cg + 21
             const bool ok = mbar_wait(bar(kBarD3), i & 1u);
             if(epi_sync_or(!ok || *s_err)) break;
             fence_after();
-            float lg[kComp], o[2 * kCompStride];
+            constexpr int kCols = kOut / 4;
+            float o[kCols];
 #pragma unroll
-            for(int k = 0; k < kComp; ++k) lg[k] = tmem_ld1(t_lane + (uint32_t)(k * kCompStride));
-#pragma unroll
-            for(int c = 0; c < 2 * kCompStride; ++c) o[c] = tmem_ld1(t_lane + cg * 2u * kCompStride + (uint32_t)c);
+            for(int c = 0; c < kCols; ++c) o[c] = tmem_ld1(t_lane + cg * (uint32_t)kCols + (uint32_t)c);
             tmem_wait_ld();
             fence_before();
             mbar_arrive(bar(kBarTF));
-            const float* b3 = bias + 2 * kH;
+            const float* b3 = bias + 2 * kH + cg * kCols;
+            float* rec = stg + r * kRecStride + cg * kCols;
 #pragma unroll
-            for(int k = 0; k < kComp; ++k) lg[k] += b3[k * kCompStride];
-#pragma unroll
-            for(int c = 0; c < 2 * kCompStride; ++c) o[c] += b3[cg * 2 * kCompStride + c];
-            float* rec = stg + r * kRecStride;
-            if(cg == 0) {
-                float mx = lg[0];
-#pragma unroll
-                for(int k = 1; k < kComp; ++k) mx = fmaxf(mx, lg[k]);
-                float e[kComp], tot = 0.0f;
-#pragma unroll
-                for(int k = 0; k < kComp; ++k) e[k] = expf(lg[k] - mx), tot += e[k];
-                float acc = 0.0f;
-#pragma unroll
-                for(int k = 0; k < kComp; ++k) {
-                    acc += e[k];
-                    rec[kMixCdf + k] = k == kComp - 1 ? 1.0f : acc / tot;
-                }
-            }
-#pragma unroll
-            for(int h = 0; h < 2; ++h) {
-                const int k = 2 * (int)cg + h;
-#pragma unroll
-                for(int d = 0; d < kDim; ++d) {
-                    rec[kMixMu + k * kDim + d] = o[h * kCompStride + 1 + d];
-                    const float sg = kSigMid + kSigHalf * tanhf(o[h * kCompStride + 1 + kDim + d] * (1.0f / kSigHalf));
-                    rec[kMixSigma + k * kDim + d] = expf(sg);
-                }
-            }
+            for(int c = 0; c < kCols; ++c) rec[c] = o[c] + b3[c];
             if constexpr(Src::kDebug) {
                 if(row < n)
-                    for(int c = 0; c < 2 * kCompStride; ++c) src.dump_out(row, cg * 2u * kCompStride + (uint32_t)c, o[c]);
+                    for(int c = 0; c < kCols; ++c) src.dump_out(row, cg * (uint32_t)kCols + (uint32_t)c, o[c] + b3[c]);
             }
             epi_sync();
             // coalesced copy of the tile's records (contiguous rows) to global memory

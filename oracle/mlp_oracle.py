@@ -241,27 +241,24 @@ def layer_bf16(h_in: np.ndarray, W: np.ndarray, b: np.ndarray, act: bool):
     return (silu(z.astype(np.float64)).astype(np.float32) if act else z), z
 
 
-def mixture_record(o: np.ndarray) -> np.ndarray:
-    """Cumulative weights (last exactly 1), means and sigmas of each row of outputs (float64)."""
+def mixture_parts(o: np.ndarray):
+    """Softmax weights (n x 8), means and sigmas (n x 8 x 5) of rows of outputs (float64)."""
     o = np.asarray(o, np.float64)
-    n = o.shape[0]
     a = o[:, 0:OUT:CSTRIDE]
     e = np.exp(a - a.max(1, keepdims=True))
-    cdf = np.cumsum(e, 1) / e.sum(1, keepdims=True)
-    cdf[:, -1] = 1.0
-    rec = np.zeros((n, MIX))
-    rec[:, :COMP] = cdf
-    for k in range(COMP):
-        rec[:, COMP + k * DIM:COMP + (k + 1) * DIM] = o[:, k * CSTRIDE + 1:k * CSTRIDE + 1 + DIM]
-        raw = o[:, k * CSTRIDE + 1 + DIM:k * CSTRIDE + 1 + 2 * DIM]
-        rec[:, COMP + COMP * DIM + k * DIM:COMP + COMP * DIM + (k + 1) * DIM] = np.exp(SIG_MID + SIG_HALF * np.tanh(raw / SIG_HALF))
-    return rec
+    w = e / e.sum(1, keepdims=True)
+    mu = np.stack([o[:, k * CSTRIDE + 1:k * CSTRIDE + 1 + DIM] for k in range(COMP)], 1)
+    raw = np.stack([o[:, k * CSTRIDE + 1 + DIM:k * CSTRIDE + 1 + 2 * DIM] for k in range(COMP)], 1)
+    return w, mu, np.exp(SIG_MID + SIG_HALF * np.tanh(raw / SIG_HALF))
 
 
 def mixture_draws(rec: np.ndarray, u_plain: np.ndarray, eps: float, seed: int, stream: int, it: int, index: np.ndarray):
-    """Draws of children `index` (one mixture record row each) in float64: Philox stream 3 keeps
-    the plain draws with probability eps, else component by cumulative weight and Box-Muller
-    normals (streams 3 and 4); returns (u (n x 6), learned mask, component)."""
+    """Draws of children `index` from the records (network outputs, one row per child) in float64:
+    Philox stream 3 keeps the plain draws when its uniform is <= eps; otherwise the component is
+    the first whose cumulative softmax weight reaches a stream-3 uniform (the last if none) and
+    u = sigmoid(mu + sigma n) with Box-Muller normals from streams 3 and 4.  Returns (u (n x 6),
+    learned mask, component, distance of the component uniform from the nearest cumulative
+    weight)."""
     index = np.asarray(index, np.uint32)
     k0, k1 = seed & 0xFFFFFFFF, seed >> 32
     a = philox_vec(index, it, 3, stream, k0, k1)
@@ -269,17 +266,18 @@ def mixture_draws(rec: np.ndarray, u_plain: np.ndarray, eps: float, seed: int, s
     ua = u01(a).astype(np.float64)
     ub = u01(b).astype(np.float64)
     keep = ua[:, 0] <= np.float32(eps)
-    comp = (rec[:, :COMP - 1] < ua[:, 1:2]).sum(1)
+    w, mu_all, sg_all = mixture_parts(rec)
+    cdf = np.cumsum(w, 1)
+    comp = np.minimum((cdf[:, : COMP - 1] < ua[:, 1:2]).sum(1), COMP - 1)
+    margin = np.abs(cdf[:, : COMP - 1] - ua[:, 1:2]).min(1)
     bm = np.concatenate([ua[:, 2:4], ub], 1)            # 6 uniforms: pairs (0,1), (2,3), (4,5)
     r = np.sqrt(-2.0 * np.log(bm[:, 0::2]))
     th = 2.0 * np.pi * bm[:, 1::2]
     nrm = np.stack([r[:, 0] * np.cos(th[:, 0]), r[:, 0] * np.sin(th[:, 0]), r[:, 1] * np.cos(th[:, 1]),
                     r[:, 1] * np.sin(th[:, 1]), r[:, 2] * np.cos(th[:, 2])], 1)
     rows = np.arange(rec.shape[0])
-    mu = np.stack([rec[rows, COMP + comp * DIM + d] for d in range(DIM)], 1)
-    sg = np.stack([rec[rows, COMP + COMP * DIM + comp * DIM + d] for d in range(DIM)], 1)
-    z = mu + sg * nrm
+    z = mu_all[rows, comp] + sg_all[rows, comp] * nrm
     u_l = np.clip(1.0 / (1.0 + np.exp(-z)), 5.9604645e-8, 1.0)
     u = np.asarray(u_plain, np.float64).copy()
     u[~keep, :DIM] = u_l[~keep]
-    return u, ~keep, comp
+    return u, ~keep, comp, margin

@@ -183,14 +183,14 @@ def tc_check(scene, n, seed):
     W1, b1, W2, b2, W3, b3 = M.unpack(w)
     x = M.features(s, g, occ)
     # layer by layer, each from the GPU's own input: BF16 activations within one BF16 ulp plus the
-    # error of the kernel's SiLU (0.5 z (1 + tanh.approx(z / 2)), |tanh error| < 2^-10.9, so
-    # |error| < 2^-11.9 |z|) and the FP32 accumulation error 1e-6 * sum |terms|
+    # error of the kernel's SiLU (h + h tanh(h), h = z / 2, tanh of h in BF16 by
+    # tanh.approx.bf16x2: |error| < 2^-8 |z|) and the FP32 accumulation error 1e-6 * sum |terms|
     for name, h_in, W, b, h_gpu in (("h1", x, W1, b1, h1), ("h2", h1, W2, b2, h2)):
         act, z = M.layer_bf16(h_in, W, b, act=True)
         want = M.bf16(act)
         bound = np.abs(M.bf16(h_in).astype(np.float64)) @ np.abs(M.bf16(W).astype(np.float64)).T
         diff = np.abs(h_gpu.astype(np.float64) - want)
-        tol = _ulp_bf16(want) * 1.01 + 2.0 ** -11.9 * np.abs(z) + 1e-6 * bound
+        tol = _ulp_bf16(want) * 1.01 + 2.0 ** -8 * np.abs(z) + 1e-6 * bound
         assert np.all(diff <= tol), (name, float((diff - tol).max()))
         assert np.mean(diff) <= 0.5 * np.mean(_ulp_bf16(want)), name
     # outputs: FP32 sums of exact BF16 products
@@ -199,10 +199,8 @@ def tc_check(scene, n, seed):
     want = z + b3
     out = out[:, : M.OUT]
     assert np.all(np.abs(out - want[:, : M.OUT]) <= 1e-5 * bound[:, : M.OUT] + 1e-5 * np.abs(b3[: M.OUT]) + 1e-6)
-    rec = M.mixture_record(out)
-    assert np.max(np.abs(mix[:, : M.COMP] - rec[:, : M.COMP])) <= 1e-6
-    rel = np.abs(mix[:, M.COMP:] - rec[:, M.COMP:]) / np.maximum(np.abs(rec[:, M.COMP:]), 1e-3)
-    assert rel.max() <= 1e-5, rel.max()
+    # the records are the outputs (biases included)
+    assert np.array_equal(mix.view(np.uint32), np.ascontiguousarray(out).view(np.uint32))
     # end to end against the oracle's own BF16 pass (no teacher forcing): small drift only
     _, _, o_ref = M.forward_bf16(w, x)
     assert np.max(np.abs(out - o_ref[:, : M.OUT])) <= 0.02 * max(1.0, np.max(np.abs(o_ref)))
@@ -282,14 +280,20 @@ def test_planner_draws_follow_the_mixture(scene):
         assert np.array_equal(d_mix.cpu().numpy().view(np.uint32), mix.view(np.uint32))
         # each child's controls: the oracle sampler on its entry's record
         plain = O.child_draws(cfg.seed, 0, it, n)
-        u, learned, _ = M.mixture_draws(mix[np.arange(n) // k].astype(np.float64), plain, eps, cfg.seed, 0, it,
-                                        np.arange(n))
+        u, learned, _, margin = M.mixture_draws(mix[np.arange(n) // k].astype(np.float64), plain, eps, cfg.seed, 0, it,
+                                                np.arange(n))
+        # children whose component uniform lies within 1e-6 of a cumulative weight may pick the
+        # neighbouring component (FP32 softmax on the GPU); they are counted and skipped
+        close = learned & (margin < 1e-6)
+        if close.any():
+            print(f"iteration {it}: {int(close.sum())} children at a component boundary")
+        learned_ok = learned & ~close
         clo = np.array(cfg.ctrl_min[:4], np.float32)
         crng = (np.array(cfg.ctrl_max[:4], np.float32) - clo).astype(np.float32)
         want = clo + u[:, :4].astype(np.float32) * crng
         got = c_rows[:, 12:16]
         assert np.array_equal(got[~learned].view(np.uint32), (clo + plain[~learned, :4] * crng).astype(np.float32).view(np.uint32))
-        assert np.all(np.abs(got[learned] - want[learned]) <= 1e-5 * crng + 1e-7)
+        assert np.all(np.abs(got[learned_ok] - want[learned_ok]) <= 1e-5 * crng + 1e-7)
         learned_total += int(learned.sum())
         assert abs((~learned).mean() - eps) < 0.05
     assert learned_total > 0

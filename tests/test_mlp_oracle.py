@@ -1,7 +1,7 @@
 """The network oracle pinned on the CPU: its Philox matches the C oracle's (itself checked against
 the published known-answer vectors), its float64 gradient matches central finite differences,
-its float32 gradient matches the float64 one, and the BF16 rounding, mixture record and mixture
-sampler behave as specified."""
+its float32 gradient matches the float64 one, and the BF16 rounding and the mixture sampler
+behave as specified."""
 import numpy as np
 import pytest
 
@@ -85,27 +85,24 @@ def test_bf16_rounding():
     assert np.all((r.view(np.uint32) & 0xFFFF) == 0)
 
 
-def test_mixture_record_and_sampler():
+def test_mixture_sampler():
     w = small_params(2)
     x, _ = batch(16, 4)
-    o = M.forward(w, x)[-1]
-    rec = M.mixture_record(o)
-    cdf = rec[:, : M.COMP]
-    assert np.all(np.diff(cdf, axis=1) >= 0) and np.all(cdf[:, -1] == 1.0)
-    sig = rec[:, M.COMP + M.COMP * M.DIM:]
+    o = M.forward(w, x)[-1][:, : M.OUT]
+    wts, mu, sig = M.mixture_parts(o)
+    assert np.allclose(wts.sum(1), 1.0)
     assert np.all(sig > np.exp(-7.0)) and np.all(sig < np.exp(3.0))
     n = 4096
-    rec_n = np.repeat(rec[:1], n, 0)
+    rec_n = np.repeat(o[:1], n, 0)
     plain = np.full((n, 6), 0.5)
-    u, learned, _ = M.mixture_draws(rec_n, plain, 1.0, 7, 0, 1, np.arange(n))
+    u, learned, _, _ = M.mixture_draws(rec_n, plain, 1.0, 7, 0, 1, np.arange(n))
     assert not learned.any() and np.array_equal(u, plain)
-    u, learned, comp = M.mixture_draws(rec_n, plain, 0.0, 7, 0, 1, np.arange(n))
+    u, learned, comp, _ = M.mixture_draws(rec_n, plain, 0.0, 7, 0, 1, np.arange(n))
     assert learned.all() and np.all((u[:, :5] > 0) & (u[:, :5] <= 1)) and np.all(u[:, 5] == 0.5)
     # component frequencies follow the mixture weights
-    wts = np.diff(np.concatenate([[0.0], rec[0, : M.COMP]]))
     freq = np.bincount(comp, minlength=M.COMP) / n
-    assert np.max(np.abs(freq - wts)) < 0.05
-    u, learned, _ = M.mixture_draws(rec_n, plain, 0.2, 7, 0, 1, np.arange(n))
+    assert np.max(np.abs(freq - wts[0])) < 0.05
+    u, learned, _, _ = M.mixture_draws(rec_n, plain, 0.2, 7, 0, 1, np.arange(n))
     assert abs((~learned).mean() - 0.2) < 0.03
 
 
