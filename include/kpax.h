@@ -93,7 +93,14 @@ typedef struct kpax_config {
     int32_t block_size;             /* threads per CTA of the expansion kernel: 0 (= 448), 128, 256, 448, 512 */
     int32_t unroll_iters;           /* planner iterations per captured CUDA graph (0 = default) */
     int32_t samples_per_thread;     /* children per expansion thread, 0 (= 1) .. 8 (grid-stride rounds) */
-    int32_t reserved[7];
+    /* PruneKPAX goal-progress pruning (PruneKPAX.cu:466-498): an accepted child is kept with
+     * probability clamp(exploration_bias + goal_bias * clamp(progress / progress_scale + 1/2, 0, 1),
+     * EPSILON, 1), progress = parent's distance to the goal - child's.  0 = off (KPAX). */
+    int32_t prune;
+    float prune_goal_bias;          /* h_goalBias_ (0.7, PruneKPAX.cu:36) */
+    float prune_exploration_bias;   /* h_explorationBias_ (0.3, PruneKPAX.cu:35) */
+    float prune_progress_scale;     /* h_progressScale_ (10, PruneKPAX.cu:34) */
+    int32_t reserved[3];
 } kpax_config;
 
 /* Result of kpax_plan (the reference exposes these as public fields h_pathToGoal_, h_itr_,

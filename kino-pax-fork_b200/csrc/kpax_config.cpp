@@ -155,6 +155,9 @@ kpax_status derive_params(const kpax_config& c, KParams* p)
     p->sparse_repeat = c.sparse_repeat;
     p->sparse_thr = c.sparse_valid_threshold;
     p->seed_lo = (uint32_t)c.seed;
+    p->prune = c.prune ? 1 : 0;
+    p->prune_goal_bias = c.prune_goal_bias, p->prune_expl_bias = c.prune_exploration_bias;
+    p->prune_scale = c.prune_progress_scale;
     p->seed_hi = (uint32_t)(c.seed >> 32);
     return KPAX_OK;
 }
@@ -188,6 +191,8 @@ kpax_status kpax_config_preset(int32_t preset, kpax_config* o)
     o->sparse_repeat = 15;
     o->sparse_valid_threshold = 10;
     o->seed = 0x4B504158ull;  // "KPAX"
+    o->prune = 0;  // PruneKPAX's defaults (PruneKPAX.cu:34-36) for when it is switched on
+    o->prune_goal_bias = 0.7f, o->prune_exploration_bias = 0.3f, o->prune_progress_scale = 10.0f;
     switch(preset) {
         case KPAX_PRESET_DI:  // 6D double integrator: h 0.1, U{1..10} steps, |v|<=1, a in [-1,1]^3
             o->model = KPAX_MODEL_DOUBLE_INTEGRATOR;
@@ -283,6 +288,9 @@ kpax_status kpax_config_validate(const kpax_config* c)
                c->block_size == 512,
              "block_size must be 0 (default), 128, 256, 448 or 512");
     KPAX_REQ(c->samples_per_thread >= 0 && c->samples_per_thread <= 8, "samples_per_thread in [0,8]");
+    KPAX_REQ(!c->prune || (c->prune_progress_scale > 0.0f && isfinite(c->prune_progress_scale) &&
+                           isfinite(c->prune_goal_bias) && isfinite(c->prune_exploration_bias)),
+             "pruning needs a positive progress scale and finite biases");
     KPAX_REQ(c->unroll_iters >= 0 && c->unroll_iters <= 64, "unroll_iters in [0,64]");
 #undef KPAX_REQ
     return KPAX_OK;

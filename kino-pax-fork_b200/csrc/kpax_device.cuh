@@ -51,6 +51,17 @@ __device__ __forceinline__ float reactivate_draw(const KParams& p, uint32_t stre
     return u01(philox(index, iter, 2u, stream, p.seed_lo, p.seed_hi).x);
 }
 
+// Goal-progress pruning of an accepted child (prune_updateFrontier_kernel, PruneKPAX.cu:466-498):
+// kept when the Philox stream-5 uniform is below clamp(explorationBias + goalBias *
+// clamp((d_parent - d_child) / progressScale + 1/2, 0, 1), EPSILON, 1).
+__device__ __forceinline__ bool prune_keep(const KParams& p, float d_parent, float d_child, uint32_t stream, uint32_t iter,
+                                           uint32_t index)
+{
+    const float prog = fminf(fmaxf(__fadd_rn(__fdiv_rn(__fsub_rn(d_parent, d_child), p.prune_scale), 0.5f), 0.0f), 1.0f);
+    const float prob = fminf(fmaxf(__fadd_rn(p.prune_expl_bias, __fmul_rn(p.prune_goal_bias, prog)), p.eps), 1.0f);
+    return u01(philox(index, iter, 5u, stream, p.seed_lo, p.seed_hi).x) < prob;
+}
+
 // ------------------------------------------------------------------ sine / cosine
 // Branch-free sin and cos of one argument for |x| <= kTrigFastMax: Cody-Waite reduction by pi/2
 // with pi/2 split in three parts (1.5703125 + 4.837512969970703125e-4 + 7.54978995489188216e-8),

@@ -40,6 +40,9 @@ struct KParams {
     uint32_t cap, budget, per_entry, root_repeat, sparse_repeat;
     int sparse_thr;
     uint32_t seed_lo, seed_hi;
+    // goal-progress pruning (PruneKPAX)
+    int prune;
+    float prune_goal_bias, prune_expl_bias, prune_scale;
 };
 
 // Derive parameters; returns KPAX_OK or KPAX_EINVAL with a message in kpax_last_error().

@@ -440,6 +440,7 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_expand(co
         if(active_child) {
             parent = sq.entries[c / k];
             load_state<SD>(t, parent, s);
+            const float d_parent = p.prune ? goal_distance(s, ctl->goal) : 0.0f;
             child_draws(p, plan, iter, c, u);
             if constexpr(M == KPAX_MODEL_QUADROTOR) {
                 if(sq.mix) mlp::mixture_draws(p, sq.mix + (size_t)(c / k) * mlp::kMixFloats, sq.prop_eps, plan, iter, c, u);
@@ -455,6 +456,7 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_expand(co
                 const bool seen = (__ldg(rg.cur + word) & bit) != 0u;
                 next = (u[5] < region_score(__ldg(rg.score + r1v), total, ready, p.eps)) || !seen;
                 atomicOr(rg.nxt + word, bit);
+                if(next && p.prune) next = prune_keep(p, d_parent, goal_distance(s, ctl->goal), plan, iter, c);
             }
             row_controls<M>(cc, rc);
             if(sq.cap.rows) {

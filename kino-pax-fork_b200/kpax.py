@@ -71,7 +71,11 @@ class Config(ctypes.Structure):
         ("block_size", ctypes.c_int32),
         ("unroll_iters", ctypes.c_int32),
         ("samples_per_thread", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 7),
+        ("prune", ctypes.c_int32),
+        ("prune_goal_bias", ctypes.c_float),
+        ("prune_exploration_bias", ctypes.c_float),
+        ("prune_progress_scale", ctypes.c_float),
+        ("reserved", ctypes.c_int32 * 3),
     ]
 
     @property

@@ -87,6 +87,15 @@ float ko_reactivate_draw(uint64_t seed, uint32_t stream, uint32_t iter, uint32_t
     return ko_u01(o[0]);
 }
 
+/* Goal-progress pruning draw (PruneKPAX.cu:488-489): Philox sub-stream 5. */
+float ko_prune_draw(uint64_t seed, uint32_t stream, uint32_t iter, uint32_t index)
+{
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    uint32_t c[4] = {index, iter, 5u, stream}, o[4];
+    ko_philox4x32_10(c, key, o);
+    return ko_u01(o[0]);
+}
+
 /* ---------------------------------------------------------------- sizes --------------- */
 
 int ko_sizes(const kpax_config* cfg, uint32_t* num_r1, uint32_t* r2_per_r1, uint32_t* sample_dim)
@@ -776,6 +785,13 @@ int ko_plan(const kpax_config* cfg, const float* init, const float* goal, const 
                 int seen = (cur[(uint32_t)b >> 5] >> (b & 31)) & 1;
                 if(u[5] < scores[a] || !seen) child_next[c] = 1;
                 nxt[(uint32_t)b >> 5] |= 1u << (b & 31);
+                if(child_next[c] && cfg->prune) { /* PruneKPAX.cu:474-492 (pruned children are not appended) */
+                    float prog = (goal_dist(x0, goal) - goal_dist(x1, goal)) / cfg->prune_progress_scale + 0.5f;
+                    prog = prog < 0.0f ? 0.0f : (prog > 1.0f ? 1.0f : prog);
+                    float prob = cfg->prune_exploration_bias + cfg->prune_goal_bias * prog;
+                    prob = prob < cfg->epsilon ? cfg->epsilon : (prob > 1.0f ? 1.0f : prob);
+                    if(!(ko_prune_draw(cfg->seed, plan_idx, it, c) < prob)) child_next[c] = 0;
+                }
             }
         }
         n_exp += n;

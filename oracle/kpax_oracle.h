@@ -38,6 +38,7 @@ float ko_u01(uint32_t x);
 void ko_child_draws(uint64_t seed, uint32_t stream, uint32_t iter, uint32_t index, float u[6]);
 /* Re-activation draw of tree node `index` in iteration `iter`. */
 float ko_reactivate_draw(uint64_t seed, uint32_t stream, uint32_t iter, uint32_t index);
+float ko_prune_draw(uint64_t seed, uint32_t stream, uint32_t iter, uint32_t index);
 
 /* Sizes derived from a configuration (same meaning as kpax_config_sizes). */
 int ko_sizes(const kpax_config* cfg, uint32_t* num_r1, uint32_t* r2_per_r1, uint32_t* sample_dim);

@@ -92,3 +92,17 @@ def test_cpp_wrapper_header_compiles():
         p.write_text(src)
         r = subprocess.run([gxx, "-std=c++17", "-fsyntax-only", f"-I{ROOT / 'include'}", str(p)], capture_output=True, text=True)
         assert r.returncode == 0, r.stderr
+
+
+def test_pruning_parameters_are_validated():
+    """PruneKPAX's goal-progress pruning needs a positive progress scale and finite biases."""
+    cfg = kpax.preset(kpax.PRESET_DI)
+    assert (cfg.prune, cfg.prune_goal_bias, cfg.prune_exploration_bias, cfg.prune_progress_scale) == (
+        0, np.float32(0.7), np.float32(0.3), 10.0)
+    lib = kpax.load()
+    cfg.prune = 1
+    assert lib.kpax_config_validate(ctypes.byref(cfg)) == kpax.OK
+    cfg.prune_progress_scale = 0.0
+    assert lib.kpax_config_validate(ctypes.byref(cfg)) == kpax.EINVAL
+    cfg.prune = 0
+    assert lib.kpax_config_validate(ctypes.byref(cfg)) == kpax.OK

@@ -98,6 +98,25 @@ def test_di_plan_bit_exact_goal_found(cuda, tmp_path):
     assert_plans_equal(g2, o2)
 
 
+@pytest.mark.parametrize("fast", [False, True])
+def test_di_plan_with_pruning_bit_exact(cuda, fast):
+    """PruneKPAX's goal-progress pruning (PruneKPAX.cu:466-498) as a frontier policy on the same
+    kernels: whole plans equal the oracle's bit for bit, and pruning removes children."""
+    import torch
+
+    cfg = small_di(fast=fast)
+    cfg.prune = 1
+    obs, s, goal = E.di_scene()
+    if fast:
+        goal = np.array([40, 40, 40, 0, 0, 0], np.float32)
+    g, _ = gpu_plan(torch, cfg, s, goal, obs)
+    o = O.plan(cfg, s, goal, obs, plan_idx=0)
+    assert_plans_equal(g, o)
+    cfg.prune = 0
+    plain = O.plan(cfg, s, goal, obs, plan_idx=0)
+    assert (g["tree_size"] < plain["tree_size"]) or (g["iters"] != plain["iters"])
+
+
 def test_plan_host_matches_device_obstacles(cuda):
     import torch
 

@@ -150,3 +150,22 @@ def test_reference_cell_overflow_is_listed_separately():
         counts = [ref.L.kref_cell_count(int(x + 21 * (y + 21 * z))) for z in range(a[2], b[2] + 1)
                   for y in range(a[1], b[1] + 1) for x in range(a[0], b[0] + 1)]
         assert max(counts) > 16
+
+
+def test_oracle_pruning_removes_children():
+    """With PruneKPAX's pruning on, accepted children are dropped with the goal-progress
+    probability; off, the plan is the plain one (PruneKPAX.cu:466-498)."""
+    import kpax
+    import kpax_envs as E
+
+    cfg = kpax.preset(kpax.PRESET_DI)
+    cfg.max_tree_size = 1 << 13
+    cfg.expansions_per_iter = 1 << 10
+    cfg.max_iter = 10
+    obs, s, g = E.di_scene()
+    plain = O.plan(cfg, s, g, obs, plan_idx=0, stop_at_goal=False)
+    cfg.prune = 1
+    pruned = O.plan(cfg, s, g, obs, plan_idx=0, stop_at_goal=False)
+    assert pruned["tree_size"] < plain["tree_size"]
+    # the first iteration's children (same draws) differ only by the pruning
+    assert pruned["expansions"] > 0 and pruned["valid_expansions"] > 0
