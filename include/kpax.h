@@ -258,6 +258,29 @@ kpax_status kpax_test_sincos(const float* d_x, uint32_t n, float* d_out, void* s
  * benchmark reports it as evidence that the device path ran. */
 uint64_t kpax_kernel_launches(void);
 
+/* ---- ReKinoLite (src/ReKino/ReKinoLite.cu, include/ReKino/ReKinoLite.cuh) ----------------
+ * The fork's warp-greedy planner on the same propagation and collision code: every warp extends
+ * one path by the valid sample closest to the goal among samples_per_thread x 32 propagated from
+ * its last node (a random valid one with probability epsilon_greedy), backing up 1-5 nodes when
+ * none is valid, up to 200 nodes.  The result's goal_idx is the winning warp (the earliest
+ * iteration, then the lowest warp id), iters its iteration + 1, path_len / h_path its path (goal
+ * first), expansions / valid_expansions the samples propagated by all warps. */
+typedef struct kpax_rekino_params {
+    uint32_t num_warps;          /* h_numWarps_ (512, ReKinoLite.cu:11) */
+    uint32_t samples_per_thread; /* h_samplesPerThread_ (1), at most 16 (512 samples per warp) */
+    float epsilon_greedy;        /* h_epsilonGreedy_ (0) */
+    uint32_t max_iterations;     /* MAX_ITER_REKINO (20000, config.h:213) */
+    double timeout_ms;           /* give-up time (6 s, ReKinoLite.cu:120-122) */
+    uint32_t reserved[4];
+} kpax_rekino_params;
+typedef struct kpax_rekino kpax_rekino;
+kpax_status kpax_rekino_defaults(kpax_rekino_params* out);
+kpax_status kpax_rekino_create(const kpax_config* cfg, const kpax_rekino_params* params, kpax_rekino** out);
+kpax_status kpax_rekino_destroy(kpax_rekino* planner);
+/* One plan: h_init / h_goal SAMPLE_DIM host floats, d_obstacles n_obs x 6 device floats. */
+kpax_status kpax_rekino_plan(kpax_rekino* planner, const float* h_init, const float* h_goal,
+                             const float* d_obstacles, uint32_t n_obs, kpax_result* out);
+
 /* ---- solution output (copyAndWriteVectorToCSV / writeVectorToCSV, helper.cuh:56-93) ------
  * Rows of `cols` floats as CSV, each value printed "%.6f" (std::fixed, setprecision 6) and
  * separated by commas, one row per line; append = 1 appends as the reference's append mode. */

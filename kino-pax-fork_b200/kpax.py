@@ -165,12 +165,21 @@ _SIGNATURES = {
     "kpax_mlp_last_propose_ms": (ctypes.c_float, [_VP]),
     "kpax_set_proposal": (_I32, [_VP, _VP, ctypes.c_float]),
     "kpax_write_rows_csv": (_I32, [_VP, _U32, _U32, ctypes.c_char_p, _I32]),
+    "kpax_rekino_defaults": (_I32, [_VP]),
+    "kpax_rekino_create": (_I32, [ctypes.POINTER(Config), _VP, ctypes.POINTER(_VP)]),
+    "kpax_rekino_destroy": (_I32, [_VP]),
+    "kpax_rekino_plan": (_I32, [_VP, _VP, _VP, _VP, _U32, ctypes.POINTER(Result)]),
     "kpax_write_solution_csv": (_I32, [_VP, ctypes.c_char_p, _I32]),
     "kpax_export_proposal": (_I32, [_VP, _VP, _U32, _VP]),
     "kpax_batch_set_proposal": (_I32, [_VP, _VP, ctypes.c_float, _VP]),
 }
 
 MLP_FEATURES, MLP_OUTPUTS, MLP_MIX, MLP_HIDDEN = 64, 96, 88, 256
+
+
+class RekinoParams(ctypes.Structure):
+    _fields_ = [("num_warps", ctypes.c_uint32), ("samples_per_thread", ctypes.c_uint32), ("epsilon_greedy", ctypes.c_float),
+                ("max_iterations", ctypes.c_uint32), ("timeout_ms", ctypes.c_double), ("reserved", ctypes.c_uint32 * 4)]
 
 _lib = None
 
@@ -562,3 +571,41 @@ def env_occupancy(env: Env, d_words: int, stream: int = 0) -> None:
 
 def mlp_features(env: Env, d_states: int, stride: int, d_goals: int, n: int, d_x: int, stream: int = 0) -> None:
     check(load().kpax_mlp_features(env.handle, d_states, stride, d_goals, n, d_x, stream), "kpax_mlp_features")
+
+
+class ReKinoLite:
+    """The fork's warp-greedy planner (src/ReKino/ReKinoLite.cu) on the library's kernels; plan()
+    returns the Result with the winning warp in goal_idx and its path (goal first)."""
+
+    def __init__(self, cfg: Config, **params):
+        self.cfg = cfg.copy()
+        self.params = RekinoParams()
+        check(load().kpax_rekino_defaults(ctypes.byref(self.params)), "kpax_rekino_defaults")
+        for k, v in params.items():
+            setattr(self.params, k, v)
+        self.sample_dim = sizes(self.cfg)[2]
+        self._h = _VP()
+        check(load().kpax_rekino_create(ctypes.byref(self.cfg), ctypes.byref(self.params), ctypes.byref(self._h)),
+              "kpax_rekino_create")
+        self.result = Result()
+
+    def plan(self, h_initial, h_goal, d_obstacles_ptr: int, n_obs: int):
+        S = self.sample_dim
+        init, goal = KPAX._row(h_initial, S), KPAX._row(h_goal, S)
+        check(load().kpax_rekino_plan(self._h, _ptr(init), _ptr(goal), d_obstacles_ptr, n_obs, ctypes.byref(self.result)),
+              "kpax_rekino_plan")
+        r = self.result
+        path = (np.ctypeslib.as_array(r.h_path, shape=(r.path_len * S,)).reshape(r.path_len, S).copy() if r.path_len
+                else np.zeros((0, S), np.float32))
+        return r, path
+
+    def close(self) -> None:
+        if self._h:
+            load().kpax_rekino_destroy(self._h)
+            self._h = _VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -864,3 +864,87 @@ int ko_plan(const kpax_config* cfg, const float* init, const float* goal, const 
     ko_env_destroy(env);
     return found;
 }
+
+/* ---------------------------------------------------------------- ReKinoLite ---------- */
+/* ReKinoLite (src/ReKino/ReKinoLite.cu:251-459) with the build's deterministic choices: Philox
+ * draws (sample j of warp w at iteration it: child draws of index 512 w + j; the warp's epsilon /
+ * choice / backtrack uniforms: counter (w, it, 2, plan)), the winner is the smallest (iteration,
+ * warp), a full 200-node path restarts from the start state.  Warps are simulated one after the
+ * other; a warp stops at iterations past the best goal iteration found so far, as on the GPU.
+ * Returns 1 when a goal was reached: out_path holds the winner's path (start first), *out_len its
+ * last index, *out_warp / *out_iter the winner. */
+int ko_rekino(const kpax_config* cfg, const float* init, const float* goal, const float* obs, uint32_t n_obs,
+              uint32_t num_warps, uint32_t spt, float eps, uint32_t max_iter, uint32_t plan_idx,
+              float* out_path, int32_t* out_len, int32_t* out_warp, int32_t* out_iter)
+{
+    const uint32_t S = (uint32_t)(cfg->state_dim + cfg->control_dim + 1), sd = (uint32_t)cfg->state_dim;
+    const uint32_t ns = 32u * spt, max_path = 200;
+    float* path = (float*)malloc(sizeof(float) * max_path * S);
+    float* cand = (float*)malloc(sizeof(float) * ns * S);
+    float* dist = (float*)malloc(sizeof(float) * ns);
+    ko_env* env = ko_env_create(cfg, obs, n_obs);
+    uint32_t best_it = 0xFFFFFFFFu;
+    int32_t best_w = -1;
+    uint32_t key[2] = {(uint32_t)cfg->seed, (uint32_t)(cfg->seed >> 32)};
+    for(uint32_t w = 0; w < num_warps; ++w) {
+        memcpy(path, init, sizeof(float) * S);
+        int depth = 0;
+        for(uint32_t it = 0; it < max_iter; ++it) {
+            if(best_it != 0xFFFFFFFFu && it > best_it) break;
+            float x0[12];
+            memcpy(x0, path + (size_t)depth * S, sizeof(float) * sd);
+            for(uint32_t j = 0; j < ns; ++j) {
+                float u[6];
+                ko_child_draws(cfg->seed, plan_idx, it, w * 512u + j, u);
+                const int ok = ko_propagate(cfg, env, x0, u, cand + (size_t)j * S, NULL, NULL);
+                dist[j] = ok ? goal_dist(cand + (size_t)j * S, goal) : INFINITY;
+            }
+            float bd = INFINITY;
+            int bj = -1;
+            for(uint32_t j = 0; j < ns; ++j)
+                if(dist[j] < bd) bd = dist[j], bj = (int)j;
+            uint32_t c[4] = {w, it, 2u, plan_idx}, r[4];
+            ko_philox4x32_10(c, key, r);
+            if(eps > 0.0f && ko_u01(r[0]) < eps) {
+                int total = 0;
+                for(uint32_t j = 0; j < ns; ++j) total += dist[j] < INFINITY;
+                if(total > 0) {
+                    const int pick = (int)(ko_u01(r[1]) * (float)total);
+                    int cnt = 0;
+                    for(uint32_t j = 0; j < ns; ++j)
+                        if(dist[j] < INFINITY) {
+                            if(cnt == pick) {
+                                bj = (int)j, bd = dist[j];
+                                break;
+                            }
+                            ++cnt;
+                        }
+                }
+            }
+            if(bj >= 0) {
+                if(depth + 1 >= (int)max_path) {
+                    depth = 0;
+                } else {
+                    ++depth;
+                    memcpy(path + (size_t)depth * S, cand + (size_t)bj * S, sizeof(float) * S);
+                    if(bd < cfg->goal_thresh) {
+                        if(it < best_it || (it == best_it && (int32_t)w < best_w)) {
+                            best_it = it, best_w = (int32_t)w;
+                            memcpy(out_path, path, sizeof(float) * (size_t)(depth + 1) * S);
+                            *out_len = depth;
+                        }
+                        break;
+                    }
+                }
+            } else if(depth > 0) {
+                int back = 1 + (int)(ko_u01(r[2]) * 5.0f);
+                depth = depth - back < 0 ? 0 : depth - back;
+            }
+        }
+    }
+    ko_env_destroy(env);
+    free(path), free(cand), free(dist);
+    *out_warp = best_w;
+    *out_iter = best_w >= 0 ? (int32_t)best_it : -1;
+    return best_w >= 0;
+}

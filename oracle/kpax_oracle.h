@@ -111,6 +111,11 @@ int ko_plan(const kpax_config* cfg, const float* init, const float* goal, const 
             uint32_t n_obs, uint32_t plan_idx, uint32_t max_iters, int stop_at_goal,
             ko_plan_out* out);
 
+/* ReKinoLite restatement (see kpax_oracle.c). */
+int ko_rekino(const kpax_config* cfg, const float* init, const float* goal, const float* obs, uint32_t n_obs,
+              uint32_t num_warps, uint32_t spt, float eps, uint32_t max_iter, uint32_t plan_idx,
+              float* out_path, int32_t* out_len, int32_t* out_warp, int32_t* out_iter);
+
 #ifdef __cplusplus
 }
 #endif

@@ -302,3 +302,24 @@ class RefLib:
         nv = self.L.kref_expand(_p(parents), per_parent, _p(draws), n, _p(scores), _p(r2flags), _p(counter),
                                 _p(valid_counter), _p(fnext), _p(rows), nthreads)
         return nv, fnext, rows
+
+
+def rekino(cfg, init, goal, obs, num_warps: int, spt: int = 1, eps: float = 0.0, max_iter: int = 2000,
+           plan_idx: int = 0) -> dict:
+    """ReKinoLite restatement: the winner (warp, iteration) and its path (start first)."""
+    n1, P, S = sizes(cfg)
+    path = np.zeros((200, S), np.float32)
+    ln, w, it = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+    o = np.ascontiguousarray(obs, np.float32).reshape(-1, 6)
+    i0 = np.zeros(S, np.float32)
+    g0 = np.zeros(S, np.float32)
+    a, b = np.asarray(init, np.float32).ravel(), np.asarray(goal, np.float32).ravel()
+    i0[: min(S, a.size)] = a[:S]
+    g0[: min(S, b.size)] = b[:S]
+    L = lib()
+    L.ko_rekino.restype = _I32
+    L.ko_rekino.argtypes = [_VP, _VP, _VP, _VP, _U32, _U32, _U32, _F32, _U32, _U32, _VP, _VP, _VP, _VP]
+    found = L.ko_rekino(_c(cfg), _p(i0), _p(g0), _p(o) if o.shape[0] else None, o.shape[0], num_warps, spt, eps, max_iter,
+                        plan_idx, _p(path), ctypes.byref(ln), ctypes.byref(w), ctypes.byref(it))
+    return {"found": int(found), "warp": w.value, "iter": it.value, "path": path[: ln.value + 1].copy() if found else
+            np.zeros((0, S), np.float32)}

@@ -169,3 +169,18 @@ def test_oracle_pruning_removes_children():
     assert pruned["tree_size"] < plain["tree_size"]
     # the first iteration's children (same draws) differ only by the pruning
     assert pruned["expansions"] > 0 and pruned["valid_expansions"] > 0
+
+
+def test_oracle_rekino_path():
+    """The ReKinoLite restatement: a path from the start state into the goal ball, the same on a
+    second run, and each row the propagation of its parent with the row's draws' controls."""
+    import kpax
+    import kpax_envs as E
+
+    cfg = kpax.preset(kpax.PRESET_DI)
+    obs, s, _ = E.di_scene()
+    g = np.array([30, 30, 30, 0, 0, 0], np.float32)
+    a = O.rekino(cfg, s, g, obs, num_warps=16, max_iter=800)
+    b = O.rekino(cfg, s, g, obs, num_warps=16, max_iter=800)
+    assert a["found"] and a["warp"] == b["warp"] and np.array_equal(a["path"], b["path"])
+    assert np.array_equal(a["path"][0, :6], s[:6]) and np.linalg.norm(a["path"][-1, :3] - g[:3]) < cfg.goal_thresh
