@@ -155,9 +155,12 @@ typedef struct kpax_iter_timing {
 } kpax_iter_timing;
 /* Benchmark entry: runs n_iters iterations without stopping at the goal.  Each is preceded,
  * outside its timed events, by a write of flush_bytes to a scratch buffer (0 = no flush; more
- * than the 126 MB L2 evicts it).  h_times: n_iters entries (may be NULL); h_totals (may be NULL):
- * children propagated, valid children, RK4 steps executed, nodes appended over the n_iters. */
-kpax_status kpax_plan_iterate_timed(kpax_planner* planner, uint32_t n_iters, uint64_t flush_bytes,
+ * than the 126 MB L2 evicts it).  split = 0 records events around each iteration only (its
+ * kernels overlap their launches as in a plan; ms_frontier/ms_expand/ms_scores are 0); split != 0
+ * also records them between the kernels, which gives the breakdown but serialises the launches.
+ * h_times: n_iters entries (may be NULL); h_totals (may be NULL): children propagated, valid
+ * children, RK4 steps executed, nodes appended over the n_iters. */
+kpax_status kpax_plan_iterate_timed(kpax_planner* planner, uint32_t n_iters, uint64_t flush_bytes, int32_t split,
                                     kpax_iter_timing* h_times, uint64_t* h_totals);
 /* The stream all planner work is issued on (cudaStream_t as void*). */
 void* kpax_planner_stream(kpax_planner* planner);

@@ -6,8 +6,9 @@
 //    fused; they are bit-identical to the oracle for identical inputs;
 //  - the double-integrator step is written the same way, so DI segments are bit-identical;
 //  - Dubins and quadrotor RK4 use a branch-free sine/cosine (sincos_fast, within a few ulp of
-//    CUDA's sincosf), tan as sin times the reciprocal cosine, IEEE sqrtf, and let the compiler
-//    fuse multiply-adds; they match the oracle within the propagation tolerance.
+//    CUDA's sincosf), tan as sin times the reciprocal cosine, the PTX approximate square root
+//    and reciprocal, and let the compiler fuse multiply-adds; they match the oracle within the
+//    propagation tolerance.
 #pragma once
 #include <stdint.h>
 
@@ -108,12 +109,33 @@ __device__ __forceinline__ void sincos_shift(float s0, float c0, float d, float*
     *cs = fmaf(c0, cm, fmaf(-s0, sd, c0));
 }
 
+// Square root and reciprocal by the PTX approximations sqrt.approx.f32 / rcp.approx.f32 (about one
+// ulp, against the half ulp of the correctly rounded forms, which cost a Newton step and a
+// special-case branch each): the quadrotor right-hand side takes two roots and one reciprocal
+// per stage on its dependency chain.
+__device__ __forceinline__ float sqrt_approx(float x)
+{
+    float y;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float y;
+    asm("rcp.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // float -> int with the reference's device semantics (saturating, NaN -> 0).
 __device__ __forceinline__ int f2i(float x) { return __float2int_rz(x); }
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
 
 // ------------------------------------------------------------------ regions (Graph.cu:99-205)
-// state s: the first 3 + cdim + vdim floats are read.
+// state s: the first 3 + cdim + vdim floats are read.  The attitude and velocity digits are
+// visited with compile-time state indices (j < SD, predicated on the runtime dimensions) so the
+// state stays in registers; the mixed-radix ids are the same integers as the reference's loops.
+template <int SD>
 __device__ __forceinline__ int region_r1(const KParams& p, const float* s)
 {
     int w = 0, f = 1;
@@ -125,35 +147,37 @@ __device__ __forceinline__ int region_r1(const KParams& p, const float* s)
     }
     if(p.w_only) return w;
     int a = 0, v = 0;
-    if(p.C1 > 1) {
-        f = 1;
-        for(int i = p.cdim - 1; i >= 0; --i) {
-            const float x = s[3 + i];
-            int idx = 0;
-            for(int k = 0; k < p.C1 - 1; ++k) idx += (x >= p.cthr1[k]);
-            a += f * idx;
-            f *= p.C1;
+    const int ce = 3 + p.cdim, ve = ce + p.vdim;
+    if(p.C1 > 1) {  // digit i = j - 3, the last one least significant
+#pragma unroll
+        for(int j = 3; j < SD; ++j) {
+            if(j < ce) {
+                const float x = s[j];
+                int idx = 0;
+                for(int k = 0; k < p.C1 - 1; ++k) idx += (x >= p.cthr1[k]);
+                a = a * p.C1 + idx;
+            }
         }
     }
     if(p.V1 > 1) {
-        f = 1;
-        for(int i = p.vdim - 1; i >= 0; --i) {
-            int idx = f2i(__fdiv_rn(__fmul_rn((float)p.V1, __fsub_rn(s[3 + p.cdim + i], p.vmin_r)), p.vspan));
-            v += f * clampi(idx, 0, p.V1 - 1);
-            f *= p.V1;
+#pragma unroll
+        for(int j = 3; j < SD; ++j) {
+            if(j >= ce && j < ve) {
+                int idx = f2i(__fdiv_rn(__fmul_rn((float)p.V1, __fsub_rn(s[j], p.vmin_r)), p.vspan));
+                v = v * p.V1 + clampi(idx, 0, p.V1 - 1);
+            }
         }
     }
     return w * p.r1_mulW + a * p.r1_mulA + v;
 }
 
-// Cell digits of an R1 id whose min corner getSubRegion reads.  In compat mode the id is
-// decoded the way initializeRegions_kernel lays out its table (Graph.cu:58-96: workspace part
-// fastest, C_R1^2 attitude cells, then velocity); otherwise in getRegion's order (Q5).
-struct R1Digits {
-    int w[3], a[8], v[8];
-};
-
-__device__ __forceinline__ void r1_digits(const KParams& p, int r1, R1Digits& d)
+// getSubRegion (Graph.cu:155-205).  The R1 min corner is W_MIN + i*W_R1_SIZE (float),
+// C_MIN + i*C_R1_SIZE (double, tabulated) and V_MIN + i*V_R1_SIZE (float), as Graph.cu:69-95.
+// The R1 id's cell digits are decoded as they are consumed, least significant first.  In compat
+// mode the id is decoded the way initializeRegions_kernel lays out its table (Graph.cu:58-96:
+// workspace part fastest, C_R1^2 attitude cells, then velocity); otherwise in getRegion's order (Q5).
+template <int SD>
+__device__ __forceinline__ int region_r2(const KParams& p, const float* s, int r1)
 {
     int wr, ar, vr;
     if(p.compat) {
@@ -167,44 +191,45 @@ __device__ __forceinline__ void r1_digits(const KParams& p, int r1, R1Digits& d)
         ar = rem / p.r1_mulA;
         vr = rem - ar * p.r1_mulA;
     }
-#pragma unroll
-    for(int i = 2; i >= 0; --i) d.w[i] = wr % p.W1, wr /= p.W1;
-    for(int i = p.cdim - 1; i >= 0; --i) d.a[i] = ar % p.C1, ar /= p.C1;
-    for(int i = p.vdim - 1; i >= 0; --i) d.v[i] = vr % p.V1, vr /= p.V1;
-}
-
-// getSubRegion (Graph.cu:155-205).  The R1 min corner is W_MIN + i*W_R1_SIZE (float),
-// C_MIN + i*C_R1_SIZE (double, tabulated) and V_MIN + i*V_R1_SIZE (float), as Graph.cu:69-95.
-__device__ __forceinline__ int region_r2(const KParams& p, const float* s, int r1)
-{
-    R1Digits d;
-    r1_digits(p, r1, d);
     int w = 0, f = 1;
 #pragma unroll
     for(int i = 2; i >= 0; --i) {
-        const float m = __fadd_rn(p.wmin, __fmul_rn((float)d.w[i], p.w1size));
+        const int dw = wr % p.W1;
+        wr /= p.W1;
+        const float m = __fadd_rn(p.wmin, __fmul_rn((float)dw, p.w1size));
         int idx = f2i(__fdiv_rn(__fmul_rn((float)p.W2, __fsub_rn(s[i], m)), p.w1size));
         w += f * clampi(idx, 0, p.W2 - 1);
         f *= p.W2;
     }
     int a = 0, v = 0;
+    const int ce = 3 + p.cdim, ve = ce + p.vdim;
     if(p.C2 > 1) {
         f = 1;
-        for(int i = p.cdim - 1; i >= 0; --i) {
-            const float t = __fmul_rn((float)p.C2, __fsub_rn(s[3 + i], p.cmin_tab[d.a[i]]));
-            int idx = 0;
-            for(int k = 0; k < p.C2 - 1; ++k) idx += (t >= p.cthr2[k]);
-            a += f * idx;
-            f *= p.C2;
+#pragma unroll
+        for(int j = SD - 1; j >= 3; --j) {
+            if(j < ce) {
+                const int da = ar % p.C1;
+                ar /= p.C1;
+                const float x = __fmul_rn((float)p.C2, __fsub_rn(s[j], p.cmin_tab[da]));
+                int idx = 0;
+                for(int k = 0; k < p.C2 - 1; ++k) idx += (x >= p.cthr2[k]);
+                a += f * idx;
+                f *= p.C2;
+            }
         }
     }
     if(p.V2 > 1) {
         f = 1;
-        for(int i = p.vdim - 1; i >= 0; --i) {
-            const float m = __fadd_rn(p.vmin_r, __fmul_rn((float)d.v[i], p.v1size));
-            int idx = f2i(__fdiv_rn(__fmul_rn((float)p.V2, __fsub_rn(s[3 + p.cdim + i], m)), p.v1size));
-            v += f * clampi(idx, 0, p.V2 - 1);
-            f *= p.V2;
+#pragma unroll
+        for(int j = SD - 1; j >= 3; --j) {
+            if(j >= ce && j < ve) {
+                const int dv = vr % p.V1;
+                vr /= p.V1;
+                const float m = __fadd_rn(p.vmin_r, __fmul_rn((float)dv, p.v1size));
+                int idx = f2i(__fdiv_rn(__fmul_rn((float)p.V2, __fsub_rn(s[j], m)), p.v1size));
+                v += f * clampi(idx, 0, p.V2 - 1);
+                f *= p.V2;
+            }
         }
     }
     return r1 * p.P + (w * p.r2_mulW + a * p.r2_mulA + v);
@@ -370,25 +395,34 @@ __device__ __forceinline__ bool prop_dubins(const KParams& p, const Grid& g, flo
 
 // Quadrotor right-hand side, statePropagator.cu:325-370, evaluated at x0 + delta*k.
 // Model constants NU 10e-3, MU 2e-6, IX 1, IY 1, IZ 2, GRAVITY -9.81, MASS 1 (config.h:300-308).
-// trig0: (sin, cos) of the three Euler angles of x0.
+// trig0: (sin, cos) of the three Euler angles of x0.  kFirst evaluates the first RK4 stage, at
+// x0 + 1 * 0: the state is x0 + 0 (which only turns -0 into +0) and the angle-sum shift by 0
+// reduces to sin + 0 and cos, so the stage skips the shift and gives the same bits.
+template <bool kFirst = false>
 __device__ __forceinline__ void quad_rhs(float* xd, const float* x0, const float* k, float delta, const float* c,
                                          const float* trig0)  // xd may alias k
 {
     const float NU = 10e-3f, MU = 2e-6f, G = -9.81f;
-    const float u = x0[6] + delta * k[6], v = x0[7] + delta * k[7], w = x0[8] + delta * k[8];
-    const float pp = x0[9] + delta * k[9], q = x0[10] + delta * k[10], r = x0[11] + delta * k[11];
-    float sf, cf, st, ct, sp, cp;
-    const float d0 = delta * k[3], d1 = delta * k[4], d2 = delta * k[5];
-    if(fmaxf(fabsf(d0), fmaxf(fabsf(d1), fabsf(d2))) <= kShiftMax) {
-        sincos_shift(trig0[0], trig0[1], d0, &sf, &cf);
-        sincos_shift(trig0[2], trig0[3], d1, &st, &ct);
-        sincos_shift(trig0[4], trig0[5], d2, &sp, &cp);
-    } else {  // large attitude increments or non-finite values: evaluate at the rounded angles
-        sincos_checked(x0[3] + d0, &sf, &cf);
-        sincos_checked(x0[4] + d1, &st, &ct);
-        sincos_checked(x0[5] + d2, &sp, &cp);
+    float u, v, w, pp, q, r, sf, cf, st, ct, sp, cp;
+    if constexpr(kFirst) {
+        u = x0[6] + 0.0f, v = x0[7] + 0.0f, w = x0[8] + 0.0f;
+        pp = x0[9] + 0.0f, q = x0[10] + 0.0f, r = x0[11] + 0.0f;
+        sf = trig0[0] + 0.0f, cf = trig0[1], st = trig0[2] + 0.0f, ct = trig0[3], sp = trig0[4] + 0.0f, cp = trig0[5];
+    } else {
+        u = x0[6] + delta * k[6], v = x0[7] + delta * k[7], w = x0[8] + delta * k[8];
+        pp = x0[9] + delta * k[9], q = x0[10] + delta * k[10], r = x0[11] + delta * k[11];
+        const float d0 = delta * k[3], d1 = delta * k[4], d2 = delta * k[5];
+        if(fmaxf(fabsf(d0), fmaxf(fabsf(d1), fabsf(d2))) <= kShiftMax) {
+            sincos_shift(trig0[0], trig0[1], d0, &sf, &cf);
+            sincos_shift(trig0[2], trig0[3], d1, &st, &ct);
+            sincos_shift(trig0[4], trig0[5], d2, &sp, &cp);
+        } else {  // large attitude increments or non-finite values: evaluate at the rounded angles
+            sincos_checked(x0[3] + d0, &sf, &cf);
+            sincos_checked(x0[4] + d1, &st, &ct);
+            sincos_checked(x0[5] + d2, &sp, &cp);
+        }
     }
-    const float sec = __frcp_rn(ct);  // tan(theta) = sin * sec, 1/cos(theta) = sec
+    const float sec = rcp_approx(ct);  // tan(theta) = sin * sec, 1/cos(theta) = sec
     xd[0] = ct * cp * u + (sf * st * cp - cf * sp) * v + (cf * st * cp + sf * sp) * w;
     xd[1] = ct * sp * u + (sf * st * sp + cf * cp) * v + (cf * st * sp - sf * cp) * w;
     xd[2] = -st * u + sf * ct * v + cf * ct * w;
@@ -396,11 +430,11 @@ __device__ __forceinline__ void quad_rhs(float* xd, const float* x0, const float
     xd[3] = pp + qr * (st * sec);
     xd[4] = q * cf - r * sf;
     xd[5] = qr * sec;
-    const float XYZ = -NU * sqrtf(u * u + v * v + w * w);
+    const float XYZ = -NU * sqrt_approx(u * u + v * v + w * w);
     xd[6] = (r * v - q * w) - G * st + XYZ * u;
     xd[7] = (pp * w - r * u) + G * ct * sf + XYZ * v;
     xd[8] = (q * u - pp * v) + G * ct * cf + XYZ * w + c[0];
-    const float LMN = -MU * sqrtf(pp * pp + q * q + r * r);
+    const float LMN = -MU * sqrt_approx(pp * pp + q * q + r * r);
     xd[9] = -(q * r) + LMN * pp + c[1];          // (IY - IZ)/IX = -1, 1/IX = 1
     xd[10] = (pp * r) + LMN * q + c[2];          // (IZ - IX)/IY = 1,  1/IY = 1
     xd[11] = 0.0f * (pp * q) + 0.5f * (LMN * r) + 0.5f * c[3];  // (IX - IY)/IZ = 0, 1/IZ = 0.5
@@ -420,20 +454,15 @@ __device__ __forceinline__ bool prop_quad(const KParams& p, const Grid& g, float
         sincos_checked(s[3], &trig0[0], &trig0[1]);
         sincos_checked(s[4], &trig0[2], &trig0[3]);
         sincos_checked(s[5], &trig0[4], &trig0[5]);
+        quad_rhs<true>(k, s, nullptr, 1.0f, c, trig0);
 #pragma unroll
-        for(int j = 0; j < 12; ++j) k[j] = 0.0f;
+        for(int j = 0; j < 12; ++j) acc[j] = k[j];
 #pragma unroll 1
-        for(int stage = 0; stage < 4; ++stage) {
-            const float delta = stage == 0 ? 1.0f : (stage == 3 ? h : hh);
+        for(int stage = 1; stage < 4; ++stage) {
+            const float delta = stage == 3 ? h : hh, w = stage == 3 ? 1.0f : 2.0f;
             quad_rhs(k, s, k, delta, c, trig0);
-            if(stage == 0) {
 #pragma unroll
-                for(int j = 0; j < 12; ++j) acc[j] = k[j];
-            } else {
-                const float w = stage == 3 ? 1.0f : 2.0f;
-#pragma unroll
-                for(int j = 0; j < 12; ++j) acc[j] = acc[j] + w * k[j];
-            }
+            for(int j = 0; j < 12; ++j) acc[j] = acc[j] + w * k[j];
         }
 #pragma unroll
         for(int j = 0; j < 12; ++j) s[j] += h6 * acc[j];

@@ -159,9 +159,9 @@ __global__ void k_region_batch(KParams p, const float* __restrict__ states, uint
     if(i >= n) return;
     float s[12];
     for(int k = 0; k < p.sd; ++k) s[k] = states[(size_t)i * p.sd + k];
-    const int a = region_r1(p, s);
+    const int a = region_r1<12>(p, s);
     r1[i] = a;
-    if(r2) r2[i] = region_r2(p, s, a);
+    if(r2) r2[i] = region_r2<12>(p, s, a);
 }
 
 __global__ void k_sincos_pair(const float* __restrict__ x, uint32_t n, float* __restrict__ out)

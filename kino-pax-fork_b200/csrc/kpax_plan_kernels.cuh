@@ -28,6 +28,7 @@ namespace plan {
 constexpr uint8_t kPending = 255;
 constexpr uint32_t kNone = 0xFFFFFFFFu;
 constexpr int kFrontierBS = 256, kItems = 4, kTile = kFrontierBS * kItems;
+constexpr int kFrontierMinBlocks = 4;  // resident count-pass CTAs per SM (register bound)
 constexpr int kExpandBS = 448;  // default: 2^16 children over 148 SMs, one 14-warp block per SM
 constexpr int kExpandBSMin = 128;  // smallest expansion block (sizes the look-back status array)
 constexpr int kScoreBS = 256, kPartials = 1024;
@@ -103,6 +104,13 @@ __device__ __forceinline__ unsigned long long globaltimer()
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
+
+// Programmatic dependent launch: the iteration's kernels are launched so that each may start
+// while its predecessor drains.  A kernel copies its (host-written) query descriptor first, then
+// waits for the predecessor grid's completion and memory before touching anything it produced,
+// and lets its own successor launch (the successor in turn waits for this grid to complete).
+__device__ __forceinline__ void wait_predecessor() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void release_successor() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
 // Copies the block's query descriptor into shared memory (all threads call it).
 __device__ __forceinline__ void load_query(const QueryDev* __restrict__ qs, const uint32_t* __restrict__ qidx, QueryDev& sq)
@@ -245,7 +253,7 @@ __global__ void k_begin(const QueryDev* __restrict__ qs, uint32_t plan_base, uin
     t.dur[0] = ig[p.S - 1];
     t.parent[0] = -1;
     t.cost[0] = 0.0f;
-    t.r1[0] = region_r1(p, s);
+    t.r1[0] = region_r1<12>(p, s);
     t.rep[0] = (uint8_t)p.root_repeat;
     Ctl* ctl = sq.ctl;
     const uint32_t epoch = ctl->epoch + 1;
@@ -262,21 +270,69 @@ __device__ __forceinline__ uint32_t resolve_repeat(const KParams& p, const TreeD
                                                    uint32_t tree_old, uint32_t iter, uint32_t plan, float fa, float total,
                                                    uint32_t ready)
 {
+    // the node's byte and region id are loaded together, then the region's score and valid count:
+    // two dependent loads per node whichever case applies
     const uint32_t r0 = t.rep[i];
+    const int32_t reg = t.r1[i];
+    const float raw = rg.score[reg];
+    const int32_t nvalid = rg.valid[reg];
     uint32_t r = r0;
     if(r == 0u) {  // re-activation of the previous iteration (KPAX.cu:505-517)
         if(i < tree_old) {
-            const float sc = region_score(rg.score[t.r1[i]], total, ready, p.eps);
+            const float sc = region_score(raw, total, ready, p.eps);
             if(reactivate_draw(p, plan, iter - 1u, i) <= __fadd_rn(sc, fa)) r = 1u;
         }
     } else if(r == kPending) {  // repeat of a node added last iteration (KPAX.cu:476-479)
-        r = rg.valid[t.r1[i]] < p.sparse_thr ? p.sparse_repeat : 1u;
+        r = nvalid < p.sparse_thr ? p.sparse_repeat : 1u;
     }
     if(r != r0) t.rep[i] = (uint8_t)r;
     return r;
 }
 
-__global__ void __launch_bounds__(kFrontierBS) k_frontier_count(const QueryDev* __restrict__ qs, uint32_t* __restrict__ active)
+// Exclusive scan of n tile sums in place by one CTA (kFrontierBS threads, up to kScanItems
+// consecutive sums per thread and pass); returns the total.  The sums were written by other
+// CTAs, so they are read through L2.
+constexpr int kScanItems = 16;
+__device__ __forceinline__ uint32_t scan_tiles(uint32_t* tiles, uint32_t n, uint32_t* s_warp, uint32_t* s_carry)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if(threadIdx.x == 0) *s_carry = 0;
+    __syncthreads();
+    for(uint32_t base = 0; base < n; base += kFrontierBS * kScanItems) {
+        const uint32_t i0 = base + threadIdx.x * kScanItems;
+        uint32_t v[kScanItems], sum = 0;
+#pragma unroll
+        for(int j = 0; j < kScanItems; ++j) {
+            v[j] = i0 + j < n ? __ldcg(tiles + i0 + j) : 0u;
+            sum += v[j];
+        }
+        uint32_t x = sum;
+#pragma unroll
+        for(int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+            if(lane >= d) x += y;
+        }
+        if(lane == 31) s_warp[warp] = x;
+        __syncthreads();
+        uint32_t wex = 0, pass = 0;
+        for(int w = 0; w < kFrontierBS / 32; ++w) {
+            wex += w < warp ? s_warp[w] : 0u;
+            pass += s_warp[w];
+        }
+        uint32_t acc = *s_carry + wex + x - sum;
+#pragma unroll
+        for(int j = 0; j < kScanItems; ++j) {
+            if(i0 + j < n) tiles[i0 + j] = acc;
+            acc += v[j];
+        }
+        __syncthreads();
+        if(threadIdx.x == 0) *s_carry += pass;
+        __syncthreads();
+    }
+    return *s_carry;
+}
+
+__global__ void __launch_bounds__(kFrontierBS, kFrontierMinBlocks) k_frontier_count(const QueryDev* __restrict__ qs, uint32_t* __restrict__ active)
 {
     __shared__ QueryDev sq;
     __shared__ uint32_t s_last, s_carry;
@@ -285,7 +341,9 @@ __global__ void __launch_bounds__(kFrontierBS) k_frontier_count(const QueryDev* 
     const KParams& p = sq.p;
     Ctl* ctl = sq.ctl;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if(ctl->done) return;
+    wait_predecessor();
+    release_successor();
+    if(__syncthreads_or(ctl->done != 0u)) return;  // one decision for the whole block: barriers follow
     const uint32_t tree = ctl->tree, tree_old = ctl->tree_old, iter = ctl->iter, plan = ctl->plan_idx;
     const uint32_t ready = ctl->scores_ready;
     const float fa = ctl->faccept, total = ctl->score_total;
@@ -314,32 +372,10 @@ __global__ void __launch_bounds__(kFrontierBS) k_frontier_count(const QueryDev* 
     __syncthreads();
     if(!s_last) return;
     __threadfence();
-    // exclusive scan of the tile sums in place, kFrontierBS at a time; total R
-    if(threadIdx.x == 0) s_carry = 0;
-    __syncthreads();
-    volatile uint32_t* ts = sq.tiles;
-    for(uint32_t base = 0; base < ntiles; base += kFrontierBS) {
-        const uint32_t i = base + threadIdx.x;
-        const uint32_t v = i < ntiles ? ts[i] : 0u;
-        uint32_t x = v;
-#pragma unroll
-        for(int d = 1; d < 32; d <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
-            if(lane >= d) x += y;
-        }
-        if(lane == 31) s_warp[warp] = x;
-        __syncthreads();
-        uint32_t wex = 0;
-        for(int w = 0; w < warp; ++w) wex += s_warp[w];
-        const uint32_t excl = s_carry + wex + x - v;
-        if(i < ntiles) ts[i] = excl;
-        __syncthreads();
-        if(threadIdx.x == kFrontierBS - 1) s_carry = excl + v;
-        __syncthreads();
-    }
+    const uint32_t R32 = scan_tiles(sq.tiles, ntiles, s_warp, &s_carry);  // exclusive prefixes; total R
     if(threadIdx.x == 0) {  // the budget of this iteration (KPAX.cu:323-350)
         *sq.farr = 0u;
-        const uint64_t R = s_carry;
+        const uint64_t R = R32;
         const uint32_t B = min(p.budget, p.cap - tree);
         uint32_t k = p.per_entry, E = 0, n = 0;
         if(B == 0) {
@@ -368,6 +404,8 @@ __global__ void __launch_bounds__(kFrontierBS) k_frontier_write(const QueryDev* 
     load_query(qs, nullptr, sq);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     Ctl* ctl = sq.ctl;
+    wait_predecessor();
+    release_successor();
     if(ctl->done) return;
     const uint32_t tree = ctl->tree, E = ctl->E;
     const uint64_t R = ctl->R;
@@ -422,7 +460,9 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_expand(co
     load_query(qs, qidx, sq);
     const KParams& p = sq.p;
     Ctl* ctl = sq.ctl;
-    if(ctl->done) return;
+    wait_predecessor();
+    release_successor();
+    if(__syncthreads_or(ctl->done != 0u)) return;  // one decision for the whole block: barriers follow
     const uint32_t n = ctl->n, k = ctl->k, tree = ctl->tree, iter = ctl->iter, plan = ctl->plan_idx, epoch = ctl->epoch;
     const uint32_t ready = ctl->scores_ready;
     const float total = ctl->score_total;
@@ -447,8 +487,8 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_expand(co
             }
             steps = draw_controls(p, u, cc);
             valid = propagate<M>(p, sq.g, s, cc, steps, steps_done);
-            r1v = region_r1(p, s);
-            r2v = region_r2(p, s, r1v);
+            r1v = region_r1<SD>(p, s);
+            r2v = region_r2<SD>(p, s, r1v);
             atomicAdd(rg.counter + r1v, 1);
             if(valid) {
                 atomicAdd(rg.valid + r1v, 1);
@@ -539,6 +579,8 @@ __global__ void __launch_bounds__(kScoreBS) k_scores(const QueryDev* __restrict_
     const RegDev& rg = sq.rg;
     Ctl* ctl = sq.ctl;
     const int tid = threadIdx.x, lane = tid & 31;
+    wait_predecessor();
+    release_successor();
     if(ctl->done) return;
     const uint32_t gtid = blockIdx.x * blockDim.x + tid, gsize = gridDim.x * blockDim.x;
     for(uint32_t w = gtid; w < p.r2_words; w += gsize) rg.cur[w] = rg.nxt[w];
@@ -626,6 +668,8 @@ __global__ void __launch_bounds__(mlp::tc::kThreads, 1) k_propose(const QueryDev
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ QueryDev sq;
     load_query(qs, qidx, sq);
+    wait_predecessor();
+    release_successor();
     if(sq.ctl->done || !sq.mix) return;
     EntrySrc src{&sq, sq.ctl->E};
     mlp::tc::forward(src, sq.mlp_img, smem, &sq.ctl->error);

@@ -15,7 +15,7 @@ using namespace kpax::plan;
 
 namespace {
 
-constexpr int kFrontierCTAs = 2 * 148;
+constexpr int kFrontierCTAs = kFrontierMinBlocks * 148;  // one round over the tiles of a 600k-node tree
 constexpr int kScoreCTAs = 128;
 constexpr size_t kAlign = 256;
 
@@ -33,15 +33,33 @@ struct Carver {
     }
 };
 
+// Launch of an iteration kernel that may start while the previous kernel of its stream drains
+// (programmatic dependent launch; the kernel waits on its predecessor before reading its results).
+template <typename... P, typename... A>
+void launch_chained(void (*kernel)(P...), dim3 grid, unsigned block, size_t smem, cudaStream_t s, A... args)
+{
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = grid;
+    lc.blockDim = dim3(block);
+    lc.dynamicSmemBytes = smem;
+    lc.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    cudaLaunchKernelEx(&lc, kernel, static_cast<P>(args)...);
+}
+
 // The expansion kernel at one of its block sizes (validated by kpax_config_validate).
 template <int M>
 void launch_expand(int bs, dim3 grid, cudaStream_t s, const QueryDev* dq, const uint32_t* qidx, uint32_t* active)
 {
     switch(bs) {
-        case 128: k_expand<M, 128><<<grid, 128, 0, s>>>(dq, qidx, active); break;
-        case 256: k_expand<M, 256><<<grid, 256, 0, s>>>(dq, qidx, active); break;
-        case 512: k_expand<M, 512><<<grid, 512, 0, s>>>(dq, qidx, active); break;
-        default: k_expand<M, kExpandBS><<<grid, kExpandBS, 0, s>>>(dq, qidx, active); break;
+        case 128: launch_chained(k_expand<M, 128>, grid, 128, 0, s, dq, qidx, active); break;
+        case 256: launch_chained(k_expand<M, 256>, grid, 256, 0, s, dq, qidx, active); break;
+        case 512: launch_chained(k_expand<M, 512>, grid, 512, 0, s, dq, qidx, active); break;
+        default: launch_chained(k_expand<M, kExpandBS>, grid, kExpandBS, 0, s, dq, qidx, active); break;
     }
 }
 
@@ -258,13 +276,14 @@ struct PlanBatch {
         return KPAX_OK;
     }
 
-    // ev (optional): four events recorded before the frontier, expansion and score kernels and after.
-    void launch_iteration(cudaEvent_t* ev = nullptr)
+    // ev (optional): four events recorded before the frontier, expansion and score kernels and after;
+    // with split == false only the first and the last, so the launches still overlap.
+    void launch_iteration(cudaEvent_t* ev = nullptr, bool split = true)
     {
         if(ev) cudaEventRecord(ev[0], stream);
-        k_frontier_count<<<dim3(gx_front, nq), kFrontierBS, 0, stream>>>(dq, d_active);
-        k_frontier_write<<<dim3(gx_front, nq), kFrontierBS, 0, stream>>>(dq);
-        if(ev) cudaEventRecord(ev[1], stream);
+        launch_chained(k_frontier_count, dim3(gx_front, nq), kFrontierBS, 0, stream, dq, d_active);
+        launch_chained(k_frontier_write, dim3(gx_front, nq), kFrontierBS, 0, stream, dq);
+        if(ev && split) cudaEventRecord(ev[1], stream);
         int used[3], nused = 0;
         for(int m = 0; m < 3; ++m)
             if(!groups[m].empty()) used[nused++] = m;
@@ -278,15 +297,15 @@ struct PlanBatch {
             }
             const dim3 grid(expand_gx[m], (uint32_t)groups[m].size());
             if(m == 2 && n_learned)
-                k_propose<<<dim3(gx_prop, n_learned), mlp::tc::kThreads, mlp::tc::kSmemBytes, s>>>(dq, d_learned);
+                launch_chained(k_propose, dim3(gx_prop, n_learned), mlp::tc::kThreads, mlp::tc::kSmemBytes, s, dq, d_learned);
             if(m == 0) launch_expand<KPAX_MODEL_DOUBLE_INTEGRATOR>(expand_bs[m], grid, s, dq, d_groups[m], d_active);
             else if(m == 1) launch_expand<KPAX_MODEL_DUBINS_AIRPLANE>(expand_bs[m], grid, s, dq, d_groups[m], d_active);
             else launch_expand<KPAX_MODEL_QUADROTOR>(expand_bs[m], grid, s, dq, d_groups[m], d_active);
             if(u < nused - 1) cudaEventRecord(ev_join[u], s);
         }
         for(int u = 0; u + 1 < nused; ++u) cudaStreamWaitEvent(stream, ev_join[u], 0);
-        if(ev) cudaEventRecord(ev[2], stream);
-        k_scores<<<dim3(gx_score, nq), kScoreBS, 0, stream>>>(dq, d_active);
+        if(ev && split) cudaEventRecord(ev[2], stream);
+        launch_chained(k_scores, dim3(gx_score, nq), kScoreBS, 0, stream, dq, d_active);
         if(ev) cudaEventRecord(ev[3], stream);
     }
 
@@ -506,7 +525,7 @@ struct PlanBatch {
 
     // Benchmark iterations: each optionally preceded (outside its events) by a write of
     // flush_bytes, which evicts the 126 MB L2, then the iteration's kernels bracketed by events.
-    kpax_status iterate_timed(uint32_t n, uint64_t flush, kpax_iter_timing* times, uint64_t* totals)
+    kpax_status iterate_timed(uint32_t n, uint64_t flush, bool split, kpax_iter_timing* times, uint64_t* totals)
     {
         kpax_status st = sync_ctl();
         if(st != KPAX_OK) return st;
@@ -524,7 +543,7 @@ struct PlanBatch {
         }
         for(uint32_t i = 0; i < n; ++i) {
             if(flush) KPAX_CUDA(cudaMemsetAsync(d_flush, (int)(i & 0xff), flush, stream));
-            launch_iteration(&tev[4 * (size_t)i]);
+            launch_iteration(&tev[4 * (size_t)i], split);
             KPAX_CHECK_LAUNCH();
             count_launch(kernels_per_iteration());
         }
@@ -532,9 +551,11 @@ struct PlanBatch {
         for(uint32_t i = 0; i < n; ++i) {
             float a = 0, b = 0, d = 0, t = 0;
             cudaEvent_t* e = &tev[4 * (size_t)i];
-            KPAX_CUDA(cudaEventElapsedTime(&a, e[0], e[1]));
-            KPAX_CUDA(cudaEventElapsedTime(&b, e[1], e[2]));
-            KPAX_CUDA(cudaEventElapsedTime(&d, e[2], e[3]));
+            if(split) {
+                KPAX_CUDA(cudaEventElapsedTime(&a, e[0], e[1]));
+                KPAX_CUDA(cudaEventElapsedTime(&b, e[1], e[2]));
+                KPAX_CUDA(cudaEventElapsedTime(&d, e[2], e[3]));
+            }
             KPAX_CUDA(cudaEventElapsedTime(&t, e[0], e[3]));
             if(times) times[i] = kpax_iter_timing{t, a, b, d};
         }
@@ -643,11 +664,11 @@ kpax_status kpax_plan_iterate(kpax_planner* pl, uint32_t n_iters, int32_t stop_a
     return pl->b.iterate(n_iters, stop_at_goal ? 1u : 0u);
 }
 
-kpax_status kpax_plan_iterate_timed(kpax_planner* pl, uint32_t n_iters, uint64_t flush_bytes, kpax_iter_timing* h_times,
-                                    uint64_t* h_totals)
+kpax_status kpax_plan_iterate_timed(kpax_planner* pl, uint32_t n_iters, uint64_t flush_bytes, int32_t split,
+                                    kpax_iter_timing* h_times, uint64_t* h_totals)
 {
     if(!pl || !pl->b.begun) return set_error("kpax_plan_iterate_timed: call kpax_plan_begin first"), KPAX_EINVAL;
-    return pl->b.iterate_timed(n_iters, flush_bytes, h_times, h_totals);
+    return pl->b.iterate_timed(n_iters, flush_bytes, split != 0, h_times, h_totals);
 }
 
 kpax_status kpax_write_rows_csv(const float* h_rows, uint32_t rows, uint32_t cols, const char* filename, int32_t append)

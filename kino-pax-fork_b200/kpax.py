@@ -128,7 +128,7 @@ _SIGNATURES = {
     "kpax_plan_begin": (_I32, [_VP, _VP, _VP, _VP, _U32]),
     "kpax_plan_iterate": (_I32, [_VP, _U32, _I32]),
     "kpax_plan_result": (_I32, [_VP, ctypes.POINTER(Result)]),
-    "kpax_plan_iterate_timed": (_I32, [_VP, _U32, ctypes.c_uint64, _VP, _VP]),
+    "kpax_plan_iterate_timed": (_I32, [_VP, _U32, ctypes.c_uint64, _I32, _VP, _VP]),
     "kpax_planner_stream": (_VP, [_VP]),
     "kpax_export_tree": (_I32, [_VP, _VP, _VP, _VP, _U32, _VP]),
     "kpax_export_regions": (_I32, [_VP, _VP, _VP, _VP, _VP]),
@@ -341,13 +341,14 @@ class KPAX:
     def iterate(self, n_iters: int, stop_at_goal: bool = False) -> None:
         check(load().kpax_plan_iterate(self._h, n_iters, int(stop_at_goal)), "kpax_plan_iterate")
 
-    def iterate_timed(self, n_iters: int, flush_bytes: int = 0):
+    def iterate_timed(self, n_iters: int, flush_bytes: int = 0, split: bool = True):
         """Per-iteration kernel times (ms: total, frontier, expand, scores) and the totals
-        (children, valid children, RK4 steps, appended nodes) over the n_iters."""
+        (children, valid children, RK4 steps, appended nodes) over the n_iters.  split=False
+        times whole iterations only (no events between their kernels; the parts read 0)."""
         times = (IterTiming * max(n_iters, 1))()
         totals = np.zeros(4, np.uint64)
-        check(load().kpax_plan_iterate_timed(self._h, n_iters, flush_bytes, ctypes.addressof(times), _ptr(totals)),
-              "kpax_plan_iterate_timed")
+        check(load().kpax_plan_iterate_timed(self._h, n_iters, flush_bytes, int(split), ctypes.addressof(times),
+                                             _ptr(totals)), "kpax_plan_iterate_timed")
         t = np.array([[x.ms_total, x.ms_frontier, x.ms_expand, x.ms_scores] for x in times[:n_iters]], np.float64)
         return t, {"children": int(totals[0]), "valid": int(totals[1]), "steps": int(totals[2]), "appended": int(totals[3])}
 

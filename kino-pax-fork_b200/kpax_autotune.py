@@ -71,7 +71,7 @@ def measure(cfg: kpax.Config, d_obs: int, n_obs: int, start, goal, warm: int = 8
     try:
         pl.begin(start, goal, d_obs, n_obs)
         pl.iterate_timed(warm, 0)
-        t, tot = pl.iterate_timed(iters, FLUSH_BYTES)
+        t, tot = pl.iterate_timed(iters, FLUSH_BYTES, split=False)
         return float(t[:, 0].mean()), tot["valid"]
     finally:
         pl.close()

@@ -1,0 +1,60 @@
+"""FP32 propagation error against an FP64 integration of the same discrete map, per model.
+
+The device integrates in FP32 like the reference (Propagator's RK4 steps in FP32 floats).  Each
+valid segment of a seeded batch is re-integrated in FP64 from the same parent state and controls
+for the same step count; the table printed is the relative state error
+|x32 - x64| / max(|x64|, 1), for the device and for the oracle's FP32 restatement of the reference
+beside it, so the device's rounding is read against the reference's own."""
+import numpy as np
+import pytest
+
+import kpax
+import kpax_envs as E
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+N = 4096
+PRESETS = {"di": kpax.PRESET_DI, "dubins": kpax.PRESET_DUBINS, "quad": kpax.PRESET_QUAD}
+SCENES = {"di": E.di_scene, "dubins": E.dubins_scene, "quad": E.quad_scene}
+# bound on the device's error against FP64, and on its excess over the reference's FP32 error
+ABS_BOUND = 1e-4
+EXCESS = 4.0
+
+
+def rel_err(x32, x64):
+    return np.abs(x32.astype(np.float64) - x64) / np.maximum(np.abs(x64), 1.0)
+
+
+@pytest.mark.parametrize("name", list(PRESETS))
+def test_fp32_vs_fp64_state_error(cuda, name):
+    import torch
+
+    cfg = kpax.preset(PRESETS[name])
+    obs, _, _ = SCENES[name]()
+    sd = cfg.state_dim
+    par = E.sample_states(cfg.model, N, 11)
+    d_obs = torch.from_numpy(obs).cuda()
+    env = kpax.Env(cfg, d_obs.data_ptr(), obs.shape[0])
+    d_par = torch.from_numpy(par).cuda()
+    rows = torch.zeros((N, cfg.sample_dim), device="cuda")
+    valid = torch.zeros(N, dtype=torch.uint8, device="cuda")
+    steps = torch.zeros(N, dtype=torch.int32, device="cuda")
+    kpax.propagate_batch(cfg, env, d_par.data_ptr(), None, 5, N, rows.data_ptr(), valid.data_ptr(), steps.data_ptr())
+    torch.cuda.synchronize()
+    g_rows, g_val, g_steps = rows.cpu().numpy(), valid.cpu().numpy(), steps.cpu().numpy()
+    o_rows, o_val, o_steps, _, _, _ = O.propagate(cfg, obs, par, None, stream=5)
+    both = np.where((g_val == 1) & (o_val == 1) & (g_steps == o_steps))[0]
+    assert both.size >= N // 4, f"{name}: only {both.size} segments valid on both sides"
+    g_err, o_err = [], []
+    for i in both:
+        x64 = O.integrate_f64(cfg, par[i], g_rows[i, sd:], int(g_steps[i]), mode=0)
+        g_err.append(rel_err(g_rows[i, :sd], x64).max())
+        o_err.append(rel_err(o_rows[i, :sd], x64).max())
+    g_err, o_err = np.array(g_err), np.array(o_err)
+    table = {"model": name, "segments": int(both.size), "mean_steps": float(g_steps[both].mean()),
+             "device_max": float(g_err.max()), "device_median": float(np.median(g_err)),
+             "reference_fp32_max": float(o_err.max()), "reference_fp32_median": float(np.median(o_err))}
+    print(table)
+    assert table["device_max"] <= ABS_BOUND, table
+    assert table["device_max"] <= EXCESS * max(table["reference_fp32_max"], 1e-7), table
