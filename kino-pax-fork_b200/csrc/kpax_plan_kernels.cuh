@@ -565,8 +565,9 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_expand(co
     }
 }
 
-// Region scores (Graph.cu:233-358): one warp per partial sum j, lane m scoring region j + 1024*m,
-// summed in ascending region order; the last CTA adds the 1024 partials with a fixed halving
+// Region scores (Graph.cu:233-358): one warp per partial sum j; the warp scores groups of 32
+// consecutive regions (g = j, j + 1024, ...: coalesced loads), adds each group by a xor butterfly
+// and the groups in ascending order; the last CTA adds the 1024 partials with a fixed halving
 // tree, so the total (and every normalised score) is bit-identical to the oracle's.  Raw scores
 // are stored (negative = no valid sample) and normalised where they are read (region_score).
 __global__ void __launch_bounds__(kScoreBS) k_scores(const QueryDev* __restrict__ qs, uint32_t* __restrict__ active)
@@ -585,10 +586,11 @@ __global__ void __launch_bounds__(kScoreBS) k_scores(const QueryDev* __restrict_
     const uint32_t gtid = blockIdx.x * blockDim.x + tid, gsize = gridDim.x * blockDim.x;
     for(uint32_t w = gtid; w < p.r2_words; w += gsize) rg.cur[w] = rg.nxt[w];
     const int nwarps = gridDim.x * (kScoreBS / 32);
+    const uint32_t ngroups = (p.num_r1 + 31) / 32;  // 32 consecutive regions per group
     for(int j = blockIdx.x * (kScoreBS / 32) + (tid >> 5); j < kPartials; j += nwarps) {
         float part = 0.0f;
-        for(int m0 = 0; j + kPartials * m0 < p.num_r1; m0 += 32) {
-            const int r = j + kPartials * (m0 + lane);
+        for(uint32_t grp = j; grp < ngroups; grp += kPartials) {
+            const int r = 32 * grp + lane;
             float contrib = 0.0f;
             if(r < p.num_r1) {
                 const int nv = rg.valid[r];
@@ -604,10 +606,9 @@ __global__ void __launch_bounds__(kScoreBS) k_scores(const QueryDev* __restrict_
                 }
                 rg.score[r] = stored;
             }
-            for(int q = 0; q < 32; ++q) {
-                const float v = __shfl_sync(0xffffffffu, contrib, q);
-                if(j + kPartials * (m0 + q) < p.num_r1) part = __fadd_rn(part, v);
-            }
+#pragma unroll
+            for(int d = 16; d > 0; d >>= 1) contrib = __fadd_rn(contrib, __shfl_xor_sync(0xffffffffu, contrib, d));
+            part = __fadd_rn(part, contrib);
         }
         if(lane == 0) sq.partials[j] = part;
     }

@@ -654,7 +654,9 @@ static uint32_t range_popcount(const uint32_t* bits, uint64_t lo, uint64_t hi)
 }
 
 /* Syclop-style region score (Graph.cu:241-256, 319-335) and normalisation (:297-304, :349-357)
- * with the total summed in a fixed order: 1024 strided partial sums, then a halving tree. */
+ * with the total summed in a fixed order (the reference adds with atomics): regions in groups of
+ * 32 consecutive ids, each group summed by a xor butterfly (v[i] += v[i ^ d] for d = 16 .. 1),
+ * group g added to partial g mod 1024 in ascending g, then a halving tree over the partials. */
 void ko_scores(const kpax_config* cfg, const int32_t* counter, const int32_t* valid, const uint32_t* r2_bits, float* scores)
 {
     uint32_t n1, P;
@@ -675,7 +677,15 @@ void ko_scores(const kpax_config* cfg, const int32_t* counter, const int32_t* va
             sc = fv4 / ((1.0f + cov) * (1.0f + cf * cf));
         }
         raw[r] = sc;
-        part[r & 1023] += sc;
+    }
+    for(uint32_t g = 0; 32u * g < n1; ++g) {
+        float v[32], w[32];
+        for(int i = 0; i < 32; ++i) v[i] = 32u * g + i < n1 ? raw[32u * g + i] : 0.0f;
+        for(int d = 16; d > 0; d >>= 1) {
+            for(int i = 0; i < 32; ++i) w[i] = v[i] + v[i ^ d];
+            memcpy(v, w, sizeof(v));
+        }
+        part[g & 1023] += v[0];
     }
     for(int s = 512; s > 0; s >>= 1)
         for(int j = 0; j < s; ++j) part[j] += part[j + s];

@@ -55,6 +55,14 @@ def test_fp32_vs_fp64_state_error(cuda, name):
     table = {"model": name, "segments": int(both.size), "mean_steps": float(g_steps[both].mean()),
              "device_max": float(g_err.max()), "device_median": float(np.median(g_err)),
              "reference_fp32_max": float(o_err.max()), "reference_fp32_median": float(np.median(o_err))}
+    if name == "di":
+        # the reference's double-integrator position update x += h(5v + 2ah)/6 is not the exact
+        # x += hv + ah^2/2 (statePropagatorSpatialHash.cu:92-94): the model discrepancy, reported
+        # apart from the rounding error
+        disc = [rel_err(O.integrate_f64(cfg, par[i], g_rows[i, sd:], int(g_steps[i]), mode=0),
+                        O.integrate_f64(cfg, par[i], g_rows[i, sd:], int(g_steps[i]), mode=1)).max() for i in both]
+        table["model_discrepancy_max"] = float(np.max(disc))
+        table["model_discrepancy_median"] = float(np.median(disc))
     print(table)
     assert table["device_max"] <= ABS_BOUND, table
     assert table["device_max"] <= EXCESS * max(table["reference_fp32_max"], 1e-7), table
