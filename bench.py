@@ -47,6 +47,8 @@ WORKLOADS = {
     "di": (kpax.PRESET_DI, E.di_scene, "6D double integrator, 20 AABBs, 2^14 expansions/iteration, U{1..10} steps of 0.1 s"),
 }
 FLUSH_BYTES = 256 << 20  # > 126 MB L2
+SEGMENTS_DESC = ("Dubins airplane propagation/collision microbench: 2^22 independent segments, parents uniform within "
+                 "the bounds, forest of 200 columns, 20 RK4 steps of 0.05 s")
 
 
 def load_peaks() -> dict:
@@ -179,9 +181,54 @@ def dist_setup(n_gpus: int):
     return ws, rank, local
 
 
+def segment_inputs(n: int, seed: int):
+    """The microbench's parents (uniform within the Dubins bounds) and its forest scene."""
+    cfg = kpax.preset(kpax.PRESET_DUBINS)
+    obs, _, _ = E.dubins_scene()
+    parents = E.sample_states(kpax.MODEL_DUBINS_AIRPLANE, n, seed, vmin=cfg.v_min, vmax=cfg.v_max)
+    return cfg, obs, parents
+
+
+def cpu_segments_rate(budget_s: float, n: int = 1 << 16, steps: int = 3):
+    """The reference's own propagate + collide routine (oracle/_ref, OpenMP, all host threads) on
+    microbench segments: valid segments per second, threads, sample description."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    cfg, obs, parents = segment_inputs(n, 3)
+    ref = O.RefLib(cfg.model)
+    ref.set_obstacles(obs)
+    threads = ref.L.kref_max_threads()
+    draws = E.uniform_draws(n, 97)
+    draws[:, 4] = np.float32((cfg.max_propagation_duration - 0.5) / cfg.max_propagation_duration)  # 20 steps
+    tot_v, tot_t, runs = 0, 0.0, 0
+    while runs < steps or tot_t < budget_s:
+        t0 = time.perf_counter()
+        _, valid = ref.propagate(parents, draws, use_hash=True, nthreads=threads)
+        tot_t += time.perf_counter() - t0
+        tot_v += int(valid.sum())
+        runs += 1
+        if tot_t > 4 * budget_s:
+            break
+    return (tot_v / tot_t, threads,
+            f"{runs} runs of {n} segments (20 steps each), {tot_v / (runs * n):.2f} valid, {tot_t:.1f} s", 1000 * tot_t / runs)
+
+
 def run_reference(args) -> None:
     ws, rank, _ = dist_setup(args.gpus)
     if rank != 0:
+        return
+    if args.workload == "segments":
+        rate, threads, sample, ms = cpu_segments_rate(min(20.0, 2.0 * max(args.steps, 1)), steps=max(args.steps, 1))
+        line = {
+            "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": SEGMENTS_DESC, "segments_per_step": 1 << 16, "parallelism": "host OpenMP"},
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
         return
     pre, scene, desc = WORKLOADS[args.workload]
     cfg = kpax.preset(pre)
@@ -274,6 +321,20 @@ def run_ours(args) -> None:
     t_s = float(times[:, 0].sum()) / 1000.0
     t_s, valid_all = combine_over_ranks(dist, "cuda", t_s, tot["valid"])
     value = valid_all / t_s
+    # single-launch floor on the planner stream: a one-element fill between two events, queued
+    # behind a sleep so that the host's launch time does not show
+    one = torch.zeros(1, device="cuda")
+    fl = []
+    with torch.cuda.stream(stream):
+        for _ in range(20):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda._sleep(200000)
+            a.record(stream)
+            one.fill_(1.0)
+            b.record(stream)
+            torch.cuda.synchronize()
+            fl.append(a.elapsed_time(b))
+    launch_floor_ms = float(np.median(fl[5:]))
     # the per-kernel breakdown from as many iterations with events between the kernels, on a new
     # plan grown the same way (the tree stays below its capacity)
     pl.begin(start, goal, d_obs.data_ptr(), obs.shape[0])
@@ -338,7 +399,8 @@ def run_ours(args) -> None:
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
             "breakdown_ms_per_step": {"frontier": float(times_split[:, 1].mean()), "expand": float(times_split[:, 2].mean()),
                                       "scores": float(times_split[:, 3].mean()),
-                                      "total_with_split_events": float(times_split[:, 0].mean())},
+                                      "total_with_split_events": float(times_split[:, 0].mean()),
+                                      "single_launch_floor": launch_floor_ms},
         }
         print(json.dumps(line), flush=True)
     pl.close()
@@ -359,6 +421,116 @@ def batch_configs(queries):
         c.seed = c.seed + 7919 * q
         cfgs.append(c)
     return cfgs
+
+
+def run_segments(args) -> None:
+    """2^22 independent Dubins segments per step through kpax_propagate_batch (device Philox draws)."""
+    import torch
+
+    ws, rank, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    n = 1 << 22
+    cfg, obs, parents = segment_inputs(n, 5 + rank)
+    S = cfg.sample_dim
+    d_obs = torch.from_numpy(obs).cuda()
+    env = kpax.Env(cfg, d_obs.data_ptr(), obs.shape[0])
+    d_par = torch.from_numpy(parents).cuda()
+    rows = torch.empty((n, S), dtype=torch.float32, device="cuda")
+    valid = torch.empty(n, dtype=torch.uint8, device="cuda")
+    steps = torch.empty(n, dtype=torch.int32, device="cuda")
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def launch(i):
+        kpax.propagate_batch(cfg, env, d_par.data_ptr(), None, i, n, rows.data_ptr(), valid.data_ptr(), steps.data_ptr(),
+                             stream=stream.cuda_stream)
+
+    for i in range(max(args.warmup, 3)):
+        launch(1000 + i)
+    launches0 = kpax.kernel_launches()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    n_valid, n_steps = 0, 0
+    with Clocks(local) as clk:
+        for i in range(args.steps):
+            flush.fill_(i & 0xFF)  # evict the 126 MB L2 between steps, outside the events
+            ev[i][0].record(stream)
+            launch(i)
+            ev[i][1].record(stream)
+            n_valid += valid.sum(dtype=torch.int64)  # device-side tallies, outside the events
+            n_steps += steps.sum(dtype=torch.int64)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches = kpax.kernel_launches() - launches0
+    t_s = sum(a.elapsed_time(b) for a, b in ev) / 1000.0
+    n_valid, n_steps = int(n_valid.item()), int(n_steps.item())
+    t_job, valid_all = combine_over_ranks(dist, "cuda", t_s, n_valid)
+    value = valid_all / t_job
+
+    peaks = load_peaks()
+    sm_mhz = peaks.get("sm_max_mhz", 1965.0)
+    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    achieved = n_steps * FLOP_PER_STEP[cfg.model] / t_s / 1e12
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                "traffic": None, "kernel": "k_propagate_batch<Dubins>",
+                "peak_note": "nominal FP32: 148 SM x 128 lanes x 2 FLOP x clocks.max.sm (no measured FP32 peak in "
+                             "MEASURED_PEAKS.json); plus 12 transcendental per step on the MUFU pipe",
+                "work": f"{n_steps} RK4 steps x {FLOP_PER_STEP[cfg.model]} FLOP over {args.steps} launches",
+                "ms_per_launch": 1000 * t_s / args.steps, "rk4_steps_per_s": n_steps / t_s}
+
+    # end to end through the C ABI from pinned host buffers: parents in, rows and verdicts out
+    h_par = torch.from_numpy(parents).pin_memory()
+    h_rows = torch.empty((n, S), dtype=torch.float32).pin_memory()
+    h_valid = torch.empty(n, dtype=torch.uint8).pin_memory()
+    e2e_steps = max(2, min(args.steps, 5))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_valid = torch.zeros((), dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for i in range(e2e_steps):
+        d_par.copy_(h_par, non_blocking=True)
+        launch(500 + i)
+        h_rows.copy_(rows, non_blocking=True)
+        h_valid.copy_(valid, non_blocking=True)
+        e2e_valid += valid.sum(dtype=torch.int64)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_t = e0.elapsed_time(e1) / 1000.0
+    e2e_valid = int(e2e_valid.item())
+    e2e = {"value": e2e_valid / e2e_t, "unit": UNIT, "h2d_bytes_per_step": int(h_par.numel() * 4),
+           "d2h_bytes_per_step": int(h_rows.numel() * 4 + h_valid.numel())}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        try:
+            rate, cores, sample, _ = cpu_segments_rate(args.cpu_seconds)
+            cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample}
+        except (FileNotFoundError, OSError) as exc:
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"unavailable: {exc}"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000 * t_job / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": SEGMENTS_DESC, "segments_per_step": n, "valid_fraction": n_valid / (n * args.steps),
+                       "l2": "flushed before each timed step (256 MiB write, outside the events)",
+                       "parallelism": f"replicas x{ws}"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def run_batch(args) -> None:
@@ -536,7 +708,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "learned"], default="quad")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "learned", "segments"], default="quad")
     ap.add_argument("--seeds", type=int, default=256, help="held-out scenes of the learned workload")
     ap.add_argument("--eps", type=float, default=0.2, help="uniform fraction of the learned proposal")
     ap.add_argument("--proposal", choices=["on", "off"], default="on", help="learned proposal for batched quadrotor queries")
@@ -552,6 +724,8 @@ def main() -> None:
         run_batch(args)
     elif args.workload == "learned":
         run_learned(args)
+    elif args.workload == "segments":
+        run_segments(args)
     else:
         run_ours(args)
 
