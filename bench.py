@@ -436,7 +436,7 @@ def run_segments(args) -> None:
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
-    n = 1 << 22
+    n = 1 << args.segments_log2
     cfg, obs, parents = segment_inputs(n, 5 + rank)
     S = cfg.sample_dim
     d_obs = torch.from_numpy(obs).cuda()
@@ -522,7 +522,8 @@ def run_segments(args) -> None:
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000 * t_job / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "fp32", "data": "synthetic",
-            "config": {"workload": SEGMENTS_DESC, "segments_per_step": n, "valid_fraction": n_valid / (n * args.steps),
+            "config": {"workload": SEGMENTS_DESC if n == 1 << 22 else SEGMENTS_DESC.replace("2^22", f"2^{args.segments_log2}"),
+                       "segments_per_step": n, "valid_fraction": n_valid / (n * args.steps),
                        "l2": "flushed before each timed step (256 MiB write, outside the events)",
                        "parallelism": f"replicas x{ws}"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
@@ -717,6 +718,7 @@ def main() -> None:
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="ignore the autotuner's cached launch parameters")
+    ap.add_argument("--segments-log2", type=int, default=22, help="segments per step of the segments workload (log2)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -304,93 +304,66 @@ __device__ __forceinline__ int draw_controls(const KParams& p, const float u[6],
 }
 
 // ------------------------------------------------------------------ models
-// Each propagates `steps` steps from s (in place), checking every step like the reference,
-// and returns validity; `done` receives the number of steps executed.
+// One integration step per model with the reference's per-step checks, in the reference's order
+// (bounds, then the swept box's collision query); the output row holds the state after the
+// failing step, as the reference's break does.
 
-// Double integrator, statePropagatorSpatialHash.cu:72-134 (Q1: x += h(5v + 2ah)/6).
-__device__ __forceinline__ bool prop_di(const KParams& p, const Grid& g, float* s, const float* c, int steps, int& done)
+// Double integrator, statePropagatorSpatialHash.cu:72-134 (Q1: x += h(5v + 2ah)/6).  One step
+// from s in place; false when the step fails a check (velocity box, workspace, finite, collision).
+__device__ __forceinline__ bool step_di(const KParams& p, const Grid& g, float* s, const float* c)
 {
     const float h = p.h;
-    bool valid = true;
-    int i = 0;
-    for(; i < steps; ++i) {
-        const float p0[3] = {s[0], s[1], s[2]};
+    const float p0[3] = {s[0], s[1], s[2]};
 #pragma unroll
-        for(int d = 0; d < 3; ++d) {
-            const float v = s[3 + d], a = c[d];
-            // (v + (v + 2*(v + a*h/2) + (v + a*h))) * h / 6
-            const float t1 = __fadd_rn(v, __fdiv_rn(__fmul_rn(a, h), 2.0f));
-            const float t2 = __fadd_rn(v, __fmul_rn(a, h));
-            const float sum = __fadd_rn(v, __fadd_rn(__fadd_rn(v, __fmul_rn(2.0f, t1)), t2));
-            s[d] = __fadd_rn(s[d], __fdiv_rn(__fmul_rn(sum, h), 6.0f));
-            // (a + 2a + 2a + a) * h / 6
-            const float asum = __fadd_rn(__fadd_rn(__fadd_rn(a, __fmul_rn(2.0f, a)), __fmul_rn(2.0f, a)), a);
-            s[3 + d] = __fadd_rn(v, __fdiv_rn(__fmul_rn(asum, h), 6.0f));
-        }
-        if(s[3] < p.vmin || s[3] > p.vmax || s[4] < p.vmin || s[4] > p.vmax || s[5] < p.vmin || s[5] > p.vmax) {
-            valid = false;
-            break;
-        }
-        if(s[0] < p.ws_lo || s[0] > p.ws_hi || s[1] < p.ws_lo || s[1] > p.ws_hi || s[2] < p.ws_lo || s[2] > p.ws_hi) {
-            valid = false;
-            break;
-        }
-        if(!finite_all(s, 6) || !step_free(g, p0, s)) {
-            valid = false;
-            break;
-        }
+    for(int d = 0; d < 3; ++d) {
+        const float v = s[3 + d], a = c[d];
+        // (v + (v + 2*(v + a*h/2) + (v + a*h))) * h / 6
+        const float t1 = __fadd_rn(v, __fdiv_rn(__fmul_rn(a, h), 2.0f));
+        const float t2 = __fadd_rn(v, __fmul_rn(a, h));
+        const float sum = __fadd_rn(v, __fadd_rn(__fadd_rn(v, __fmul_rn(2.0f, t1)), t2));
+        s[d] = __fadd_rn(s[d], __fdiv_rn(__fmul_rn(sum, h), 6.0f));
+        // (a + 2a + 2a + a) * h / 6
+        const float asum = __fadd_rn(__fadd_rn(__fadd_rn(a, __fmul_rn(2.0f, a)), __fmul_rn(2.0f, a)), a);
+        s[3 + d] = __fadd_rn(v, __fdiv_rn(__fmul_rn(asum, h), 6.0f));
     }
-    done = i < steps ? i + 1 : steps;
-    return valid;
+    if(s[3] < p.vmin || s[3] > p.vmax || s[4] < p.vmin || s[4] > p.vmax || s[5] < p.vmin || s[5] > p.vmax) return false;
+    if(s[0] < p.ws_lo || s[0] > p.ws_hi || s[1] < p.ws_lo || s[1] > p.ws_hi || s[2] < p.ws_lo || s[2] > p.ws_hi) return false;
+    return finite_all(s, 6) && step_free(g, p0, s);
 }
 
-// Dubins airplane, statePropagatorSpatialHash.cu:139-229; c = (a, yawRate, pitchRate).
-__device__ __forceinline__ bool prop_dubins(const KParams& p, const Grid& g, float* s, const float* c, int steps, int& done)
+// Dubins airplane, statePropagatorSpatialHash.cu:139-229; c = (a, yawRate, pitchRate).  One step
+// from s in place; false when the step fails a check (speed, pitch range, workspace, finite, collision).
+__device__ __forceinline__ bool step_dubins(const KParams& p, const Grid& g, float* s, const float* c)
 {
     const float h = p.h, hh = p.hh, h6 = p.h6;
     const float a = c[0], yr = c[1], pr = c[2];
-    bool valid = true;
-    int i = 0;
-    for(; i < steps; ++i) {
-        const float p0[3] = {s[0], s[1], s[2]};
-        const float yaw = s[3], pitch = s[4], v = s[5];
-        float sp0, cp0, sy0, cy0, sp1, cp1, sy1, cy1, sp2, cp2, sy2, cy2;
-        sincos_checked(pitch, &sp0, &cp0);
-        sincos_checked(yaw, &sy0, &cy0);
-        if(fmaxf(fabsf(h * pr), fabsf(h * yr)) <= kShiftMax) {
-            sincos_shift(sp0, cp0, hh * pr, &sp1, &cp1);
-            sincos_shift(sy0, cy0, hh * yr, &sy1, &cy1);
-            sincos_shift(sp0, cp0, h * pr, &sp2, &cp2);
-            sincos_shift(sy0, cy0, h * yr, &sy2, &cy2);
-        } else {
-            sincos_checked(pitch + hh * pr, &sp1, &cp1);
-            sincos_checked(yaw + hh * yr, &sy1, &cy1);
-            sincos_checked(pitch + h * pr, &sp2, &cp2);
-            sincos_checked(yaw + h * yr, &sy2, &cy2);
-        }
-        const float vm = v + hh * a, ve = v + h * a;
-        const float mx = vm * cp1 * cy1, my = vm * cp1 * sy1, mz = vm * sp1;
-        s[0] += h6 * (v * cp0 * cy0 + 2.0f * (mx + mx) + ve * cp2 * cy2);
-        s[1] += h6 * (v * cp0 * sy0 + 2.0f * (my + my) + ve * cp2 * sy2);
-        s[2] += h6 * (v * sp0 + 2.0f * (mz + mz) + ve * sp2);
-        s[3] = yaw + h * yr;
-        s[4] = pitch + h * pr;
-        s[5] = v + h6 * (a + 2.0f * (a + a) + a);
-        if(s[5] < p.vmin || s[5] > p.vmax || s[4] < p.pitch_lo || s[4] > p.pitch_hi) {
-            valid = false;
-            break;
-        }
-        if(s[0] < p.ws_lo || s[0] > p.ws_hi || s[1] < p.ws_lo || s[1] > p.ws_hi || s[2] < p.ws_lo || s[2] > p.ws_hi) {
-            valid = false;
-            break;
-        }
-        if(!finite_all(s, 6) || !step_free(g, p0, s)) {
-            valid = false;
-            break;
-        }
+    const float p0[3] = {s[0], s[1], s[2]};
+    const float yaw = s[3], pitch = s[4], v = s[5];
+    float sp0, cp0, sy0, cy0, sp1, cp1, sy1, cy1, sp2, cp2, sy2, cy2;
+    sincos_checked(pitch, &sp0, &cp0);
+    sincos_checked(yaw, &sy0, &cy0);
+    if(fmaxf(fabsf(h * pr), fabsf(h * yr)) <= kShiftMax) {
+        sincos_shift(sp0, cp0, hh * pr, &sp1, &cp1);
+        sincos_shift(sy0, cy0, hh * yr, &sy1, &cy1);
+        sincos_shift(sp0, cp0, h * pr, &sp2, &cp2);
+        sincos_shift(sy0, cy0, h * yr, &sy2, &cy2);
+    } else {
+        sincos_checked(pitch + hh * pr, &sp1, &cp1);
+        sincos_checked(yaw + hh * yr, &sy1, &cy1);
+        sincos_checked(pitch + h * pr, &sp2, &cp2);
+        sincos_checked(yaw + h * yr, &sy2, &cy2);
     }
-    done = i < steps ? i + 1 : steps;
-    return valid;
+    const float vm = v + hh * a, ve = v + h * a;
+    const float mx = vm * cp1 * cy1, my = vm * cp1 * sy1, mz = vm * sp1;
+    s[0] += h6 * (v * cp0 * cy0 + 2.0f * (mx + mx) + ve * cp2 * cy2);
+    s[1] += h6 * (v * cp0 * sy0 + 2.0f * (my + my) + ve * cp2 * sy2);
+    s[2] += h6 * (v * sp0 + 2.0f * (mz + mz) + ve * sp2);
+    s[3] = yaw + h * yr;
+    s[4] = pitch + h * pr;
+    s[5] = v + h6 * (a + 2.0f * (a + a) + a);
+    if(s[5] < p.vmin || s[5] > p.vmax || s[4] < p.pitch_lo || s[4] > p.pitch_hi) return false;
+    if(s[0] < p.ws_lo || s[0] > p.ws_hi || s[1] < p.ws_lo || s[1] > p.ws_hi || s[2] < p.ws_lo || s[2] > p.ws_hi) return false;
+    return finite_all(s, 6) && step_free(g, p0, s);
 }
 
 // Quadrotor right-hand side, statePropagator.cu:325-370, evaluated at x0 + delta*k.
@@ -443,52 +416,54 @@ __device__ __forceinline__ void quad_rhs(float* xd, const float* x0, const float
 // Quadrotor RK4, statePropagatorSpatialHash.cu:234-308.  The four stages run as a loop over one
 // copy of the right-hand side (k is updated in place: each stage reads the previous stage's k
 // before writing its own); the stage sum keeps the reference's order ((k1 + 2k2) + 2k3) + k4.
-__device__ __forceinline__ bool prop_quad(const KParams& p, const Grid& g, float* s, const float* c, int steps, int& done)
+// One step from s in place; false when the step fails a check (velocity box, workspace, finite,
+// collision).
+__device__ __forceinline__ bool step_quad(const KParams& p, const Grid& g, float* s, const float* c)
 {
     const float h = p.h, hh = p.hh, h6 = p.h6;
-    bool valid = true;
-    int i = 0;
-    for(; i < steps; ++i) {
-        const float p0[3] = {s[0], s[1], s[2]};
-        float k[12], acc[12], trig0[6];
-        sincos_checked(s[3], &trig0[0], &trig0[1]);
-        sincos_checked(s[4], &trig0[2], &trig0[3]);
-        sincos_checked(s[5], &trig0[4], &trig0[5]);
-        quad_rhs<true>(k, s, nullptr, 1.0f, c, trig0);
+    const float p0[3] = {s[0], s[1], s[2]};
+    float k[12], acc[12], trig0[6];
+    sincos_checked(s[3], &trig0[0], &trig0[1]);
+    sincos_checked(s[4], &trig0[2], &trig0[3]);
+    sincos_checked(s[5], &trig0[4], &trig0[5]);
+    quad_rhs<true>(k, s, nullptr, 1.0f, c, trig0);
 #pragma unroll
-        for(int j = 0; j < 12; ++j) acc[j] = k[j];
+    for(int j = 0; j < 12; ++j) acc[j] = k[j];
 #pragma unroll 1
-        for(int stage = 1; stage < 4; ++stage) {
-            const float delta = stage == 3 ? h : hh, w = stage == 3 ? 1.0f : 2.0f;
-            quad_rhs(k, s, k, delta, c, trig0);
+    for(int stage = 1; stage < 4; ++stage) {
+        const float delta = stage == 3 ? h : hh, w = stage == 3 ? 1.0f : 2.0f;
+        quad_rhs(k, s, k, delta, c, trig0);
 #pragma unroll
-            for(int j = 0; j < 12; ++j) acc[j] = acc[j] + w * k[j];
-        }
-#pragma unroll
-        for(int j = 0; j < 12; ++j) s[j] += h6 * acc[j];
-        if(s[6] < p.vmin || s[6] > p.vmax || s[7] < p.vmin || s[7] > p.vmax || s[8] < p.vmin || s[8] > p.vmax) {
-            valid = false;
-            break;
-        }
-        if(s[0] < p.ws_lo || s[0] > p.ws_hi || s[1] < p.ws_lo || s[1] > p.ws_hi || s[2] < p.ws_lo || s[2] > p.ws_hi) {
-            valid = false;
-            break;
-        }
-        if(!finite_all(s, 12) || !step_free(g, p0, s)) {
-            valid = false;
-            break;
-        }
+        for(int j = 0; j < 12; ++j) acc[j] = acc[j] + w * k[j];
     }
-    done = i < steps ? i + 1 : steps;
-    return valid;
+#pragma unroll
+    for(int j = 0; j < 12; ++j) s[j] += h6 * acc[j];
+    if(s[6] < p.vmin || s[6] > p.vmax || s[7] < p.vmin || s[7] > p.vmax || s[8] < p.vmin || s[8] > p.vmax) return false;
+    if(s[0] < p.ws_lo || s[0] > p.ws_hi || s[1] < p.ws_lo || s[1] > p.ws_hi || s[2] < p.ws_lo || s[2] > p.ws_hi) return false;
+    return finite_all(s, 12) && step_free(g, p0, s);
 }
 
 template <int M>
+__device__ __forceinline__ bool model_step(const KParams& p, const Grid& g, float* s, const float* c)
+{
+    if constexpr(M == KPAX_MODEL_DOUBLE_INTEGRATOR) return step_di(p, g, s, c);
+    else if constexpr(M == KPAX_MODEL_DUBINS_AIRPLANE) return step_dubins(p, g, s, c);
+    else return step_quad(p, g, s, c);
+}
+
+// Propagates `steps` steps from s (in place), checking every step like the reference, and
+// returns validity; `done` receives the number of steps executed (the failing one included).
+template <int M>
 __device__ __forceinline__ bool propagate(const KParams& p, const Grid& g, float* s, const float* c, int steps, int& done)
 {
-    if constexpr(M == KPAX_MODEL_DOUBLE_INTEGRATOR) return prop_di(p, g, s, c, steps, done);
-    else if constexpr(M == KPAX_MODEL_DUBINS_AIRPLANE) return prop_dubins(p, g, s, c, steps, done);
-    else return prop_quad(p, g, s, c, steps, done);
+    for(int i = 0; i < steps; ++i) {
+        if(!model_step<M>(p, g, s, c)) {
+            done = i + 1;
+            return false;
+        }
+    }
+    done = steps;
+    return true;
 }
 
 template <int M>

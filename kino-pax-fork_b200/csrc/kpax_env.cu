@@ -110,7 +110,7 @@ inline uint32_t warp_blocks(uint32_t n) { return (uint32_t)(((uint64_t)n * 32 + 
 // ---------------------------------------------------------------- batch kernels
 
 template <int M>
-__global__ void __launch_bounds__(256) k_propagate_batch(KParams p, Grid g, const float* __restrict__ parents,
+__global__ void __launch_bounds__(256, 4) k_propagate_batch(KParams p, Grid g, const float* __restrict__ parents,
                                                          const float* __restrict__ draws, uint32_t stream_id, uint32_t n,
                                                          float* __restrict__ rows, uint8_t* __restrict__ valid,
                                                          int32_t* __restrict__ steps_out)
