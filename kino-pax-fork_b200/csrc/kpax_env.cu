@@ -54,22 +54,36 @@ __global__ void k_env_count(Grid g, const float* __restrict__ obs, uint32_t n, f
     for(int k = lane; k < total; k += 32) atomicAdd(counts + box_cell(g, c0, c1, k), 1u);
 }
 
-// Exclusive scan of counts[0, n) in place (single CTA of 1024 threads); counts[n] = total;
-// cursor gets a copy of the offsets.
+// Exclusive scan of counts[0, n) in place (single CTA of 1024 threads; each thread scans 8
+// consecutive counts per pass, read and written as two 16-byte vectors where the pass is full and
+// both arrays start 16-byte aligned, one count at a time otherwise); counts[n] = total; cursor
+// gets a copy of the offsets.
+constexpr int kEnvScanItems = 8;
 __global__ void __launch_bounds__(1024) k_env_scan(uint32_t* __restrict__ counts, uint32_t n, uint32_t* __restrict__ cursor)
 {
     __shared__ uint32_t s_warp[32];
     __shared__ uint32_t s_carry;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool vec = ((reinterpret_cast<uintptr_t>(counts) | reinterpret_cast<uintptr_t>(cursor)) & 15u) == 0;
     if(threadIdx.x == 0) s_carry = 0;
     __syncthreads();
-    for(uint32_t base = 0; base < n; base += 1024) {
-        const uint32_t i = base + threadIdx.x;
-        const uint32_t v = i < n ? counts[i] : 0u;
-        uint32_t x = v;
+    for(uint32_t base = 0; base < n; base += 1024 * kEnvScanItems) {
+        const uint32_t i0 = base + threadIdx.x * kEnvScanItems;
+        const bool full = vec && i0 + kEnvScanItems <= n;
+        uint32_t v[kEnvScanItems], sum = 0;
+        if(full) {
+            const uint4 a = *reinterpret_cast<const uint4*>(counts + i0), b = *reinterpret_cast<const uint4*>(counts + i0 + 4);
+            v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w, v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+        } else {
+#pragma unroll
+            for(int j = 0; j < kEnvScanItems; ++j) v[j] = i0 + j < n ? counts[i0 + j] : 0u;
+        }
+#pragma unroll
+        for(int j = 0; j < kEnvScanItems; ++j) sum += v[j];
+        uint32_t x = sum;
 #pragma unroll
         for(int d = 1; d < 32; d <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
             if(lane >= d) x += y;
         }
         if(lane == 31) s_warp[warp] = x;
@@ -78,16 +92,26 @@ __global__ void __launch_bounds__(1024) k_env_scan(uint32_t* __restrict__ counts
             uint32_t w = s_warp[lane];
 #pragma unroll
             for(int d = 1; d < 32; d <<= 1) {
-                uint32_t y = __shfl_up_sync(0xffffffffu, w, d);
+                const uint32_t y = __shfl_up_sync(0xffffffffu, w, d);
                 if(lane >= d) w += y;
             }
             s_warp[lane] = w;
         }
         __syncthreads();
-        const uint32_t excl = s_carry + (warp ? s_warp[warp - 1] : 0u) + x - v;
-        if(i < n) counts[i] = excl, cursor[i] = excl;
+        uint32_t e[kEnvScanItems], acc = s_carry + (warp ? s_warp[warp - 1] : 0u) + x - sum;
+#pragma unroll
+        for(int j = 0; j < kEnvScanItems; ++j) e[j] = acc, acc += v[j];
+        if(full) {
+            const uint4 a = make_uint4(e[0], e[1], e[2], e[3]), b = make_uint4(e[4], e[5], e[6], e[7]);
+            *reinterpret_cast<uint4*>(counts + i0) = a, *reinterpret_cast<uint4*>(counts + i0 + 4) = b;
+            *reinterpret_cast<uint4*>(cursor + i0) = a, *reinterpret_cast<uint4*>(cursor + i0 + 4) = b;
+        } else {
+#pragma unroll
+            for(int j = 0; j < kEnvScanItems; ++j)
+                if(i0 + j < n) counts[i0 + j] = e[j], cursor[i0 + j] = e[j];
+        }
         __syncthreads();
-        if(threadIdx.x == 1023) s_carry = excl + v;
+        if(threadIdx.x == 0) s_carry += s_warp[31];
         __syncthreads();
     }
     if(threadIdx.x == 0) counts[n] = s_carry;
@@ -372,7 +396,7 @@ constexpr uint32_t kNoAllocMaxEntries = 1u << 18;  // (cell, obstacle) pairs
 
 struct NoAllocScratch {
     float4 obs[2 * kNoAllocMaxObstacles];
-    uint32_t off[kNoAllocMaxCells + 1];
+    uint32_t off[kNoAllocMaxCells + 4];  // cells + 1, padded so that cursor starts 16-byte aligned
     uint32_t cursor[kNoAllocMaxCells];
     uint32_t ent[kNoAllocMaxEntries];
 };
