@@ -335,6 +335,28 @@ def run_ours(args) -> None:
             torch.cuda.synchronize()
             fl.append(a.elapsed_time(b))
     launch_floor_ms = float(np.median(fl[5:]))
+    # latency floor of the expansion: the propagation kernel on 4096 independent segments (one warp
+    # per SM), whose time is the dependency chain of its longest full-length segment
+    seg_n = 4096
+    seg_par = torch.from_numpy(E.sample_states(cfg.model, seg_n, 17)).cuda()
+    seg_rows = torch.empty((seg_n, cfg.sample_dim), device="cuda")
+    seg_valid = torch.empty(seg_n, dtype=torch.uint8, device="cuda")
+    seg_env = kpax.Env(cfg, d_obs.data_ptr(), obs.shape[0])
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    fl_seg = []
+    with torch.cuda.stream(stream):
+        for i in range(8):
+            flush.fill_(i & 0xFF)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            kpax.propagate_batch(cfg, seg_env, seg_par.data_ptr(), None, 900 + i, seg_n, seg_rows.data_ptr(),
+                                 seg_valid.data_ptr(), stream=stream.cuda_stream)
+            b.record(stream)
+            torch.cuda.synchronize()
+            fl_seg.append(a.elapsed_time(b))
+    seg_env.close()
+    del flush
+    chain_floor_ms = float(np.median(fl_seg[3:]))
     # the per-kernel breakdown from as many iterations with events between the kernels, on a new
     # plan grown the same way (the tree stays below its capacity)
     pl.begin(start, goal, d_obs.data_ptr(), obs.shape[0])
@@ -354,7 +376,12 @@ def run_ours(args) -> None:
                 "peak_note": "nominal FP32: 148 SM x 128 lanes x 2 FLOP x clocks.max.sm (no measured FP32 peak in "
                              "MEASURED_PEAKS.json)",
                 "work": f"{tot_split['steps']} RK4 steps x {FLOP_PER_STEP[cfg.model]} FLOP over {args.steps} launches",
-                "expand_ms_per_launch": 1000 * t_exp / args.steps}
+                "expand_ms_per_launch": 1000 * t_exp / args.steps,
+                "latency_floor_ms": chain_floor_ms,
+                "floor_note": "the propagation kernel on 4096 independent segments of the same model and scene (one warp "
+                              "per SM): the dependency chain of one full-length segment, which bounds the expansion "
+                              "kernel from below whatever its FP32 rate",
+                "floor_frac": chain_floor_ms / (1000 * t_exp / args.steps)}
 
     # end to end: whole plans from host buffers through the C ABI
     e2e_v, e2e_t, tts, found = 0, 0.0, [], 0
