@@ -55,3 +55,30 @@ def test_tuned_double_integrator_matches_oracle(cuda):
     assert r.tree_size == o["tree_size"] and r.valid_expansions == o["valid_expansions"]
     assert np.array_equal(rows.view(np.uint32), np.ascontiguousarray(o["rows"], np.float32).view(np.uint32))
     assert np.array_equal(par, o["parents"])
+
+
+@pytest.mark.parametrize("split", [False, True])
+def test_timed_iterations_expand_the_same_tree(cuda, split):
+    """The benchmark's timed path (direct launches, with or without events between the chained
+    kernels, an L2-evicting write before each iteration) expands the tree the captured plan loop
+    expands for the same iterations."""
+    import torch
+
+    cfg = kpax.preset(kpax.PRESET_QUAD)
+    cfg.max_iter = 10
+    obs, s, g = E.quad_scene()
+    d = torch.from_numpy(np.ascontiguousarray(obs, np.float32)).cuda()
+    ref = kpax.KPAX(cfg)
+    ref.begin(s, g, d.data_ptr(), obs.shape[0])
+    ref.iterate(cfg.max_iter)
+    rows0, par0, _ = ref.export_tree()
+    pl = kpax.KPAX(cfg)
+    pl.begin(s, g, d.data_ptr(), obs.shape[0])
+    times, tot = pl.iterate_timed(cfg.max_iter, 1 << 20, split=split)
+    rows, par, _ = pl.export_tree()
+    assert times.shape == (cfg.max_iter, 4) and np.all(times[:, 0] > 0)
+    assert np.all(times[:, 1:] > 0) if split else np.all(times[:, 1:] == 0)
+    assert tot["appended"] == rows.shape[0] - 1
+    assert np.array_equal(rows.view(np.uint32), rows0.view(np.uint32)) and np.array_equal(par, par0)
+    ref.close()
+    pl.close()
