@@ -293,6 +293,19 @@ kpax_status kpax_write_rows_csv(const float* h_rows, uint32_t rows, uint32_t col
  * node first and the root last (every row; the reference writes h_itr_ rows, Q12).  No file
  * content is written when no path was found (an empty file unless appending). */
 kpax_status kpax_write_solution_csv(kpax_planner* planner, const char* filename, int32_t append);
+/* planBench (KPAX.cu:243-300) with the reference's per-iteration dumps (writeDeviceVectorsToCSV,
+ * KPAX.cu:545-633, and writeExecutionTimeToCSV, 635-643): plans like kpax_plan, one iteration at a
+ * time, and after each iteration writes under out_dir/Data/<Name>/<Name><bench_itr>/ the tree rows
+ * (samples<itr>.csv: MAX_TREE_SIZE rows of SAMPLE_DIM, unused rows 0), parents (parents<itr>.csv,
+ * unused -1), one row per iteration of the region counters, valid counters, frontier flags,
+ * frontier repeat counts and region scores, one value per iteration of the frontier size, tree
+ * size and children expanded, the solution rows when found (controlPathToGoal.csv), and the
+ * run's seconds to Data/ExecutionTime/executionTime.csv.  A run's files start fresh at its first
+ * iteration (the reference appends to whatever a previous run left).  Debug output: every
+ * iteration copies the whole tree to the host. */
+kpax_status kpax_plan_bench(kpax_planner* planner, const float* h_init, const float* h_goal,
+                            const float* d_obstacles, uint32_t n_obs, int32_t bench_itr,
+                            const char* out_dir, kpax_result* out);
 
 /* ---- learned proposal (no counterpart in the reference) ----------------------------------
  * The reference draws every control and duration uniformly (statePropagatorSpatialHash.cu,

@@ -32,12 +32,16 @@ public:
     void plan(float* h_initial, float* h_goal, float* d_obstacles_ptr, unsigned h_obstaclesCount, bool saveTree = false)
     {
         check(kpax_plan(handle_, h_initial, h_goal, d_obstacles_ptr, h_obstaclesCount, saveTree ? 1 : 0, &result_));
-        h_treeSize_ = result_.tree_size;
-        h_itr_ = result_.iters;
-        h_pathToGoal_ = (int)result_.goal_idx;
-        h_costToGoal_ = (float)result_.path_cost;
-        path_.assign(result_.h_path, result_.h_path + (size_t)result_.path_len * sample_dim_);
-        h_controlPathToGoal_ = path_.data();
+        publish();
+    }
+
+    /* KPAX::planBench (src/planners/KPAX.cu:243-300): the plan with the per-iteration CSV dumps of
+     * writeDeviceVectorsToCSV under out_dir/Data (the reference writes under the working directory). */
+    void planBench(float* h_initial, float* h_goal, float* d_obstacles_ptr, unsigned h_obstaclesCount, int benchItr,
+                   const char* out_dir = ".")
+    {
+        check(kpax_plan_bench(handle_, h_initial, h_goal, d_obstacles_ptr, h_obstaclesCount, benchItr, out_dir, &result_));
+        publish();
     }
 
     const kpax_result& result() const { return result_; }
@@ -51,6 +55,15 @@ public:
     float* h_controlPathToGoal_ = nullptr; /* path rows, goal first, result().path_len of them */
 
 private:
+    void publish()
+    {
+        h_treeSize_ = result_.tree_size;
+        h_itr_ = result_.iters;
+        h_pathToGoal_ = (int)result_.goal_idx;
+        h_costToGoal_ = (float)result_.path_cost;
+        path_.assign(result_.h_path, result_.h_path + (size_t)result_.path_len * sample_dim_);
+        h_controlPathToGoal_ = path_.data();
+    }
     static kpax_config make_preset(int preset)
     {
         kpax_config c;

@@ -5,6 +5,9 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
+#include <filesystem>
+#include <string>
 #include <vector>
 
 #include "kpax_internal.h"
@@ -698,6 +701,120 @@ kpax_status kpax_write_solution_csv(kpax_planner* pl, const char* filename, int3
     kpax_status st = pl->b.finish(&r);
     if(st != KPAX_OK) return st;
     return kpax_write_rows_csv(r.h_path, r.path_len, (uint32_t)pl->b.prm[0].S, filename, append);
+}
+
+}  // extern "C"
+
+namespace {
+
+// Text output in the formats of the reference's helpers: rows of comma-separated values, floats
+// with std::fixed and 6 digits (writeVectorToCSV, helper.cuh:56-80); one value per line, floats
+// with 10 digits (writeValueToCSV, helper.cuh:93-106).
+bool write_rows_f(const std::string& path, const float* v, size_t rows, size_t cols, bool append)
+{
+    FILE* f = fopen(path.c_str(), append ? "a" : "w");
+    if(!f) return false;
+    for(size_t i = 0; i < rows; ++i)
+        for(size_t j = 0; j < cols; ++j) fprintf(f, j + 1 < cols ? "%.6f," : "%.6f\n", (double)v[i * cols + j]);
+    return fclose(f) == 0;
+}
+
+template <class T>
+bool write_rows_i(const std::string& path, const T* v, size_t rows, size_t cols, bool append)
+{
+    FILE* f = fopen(path.c_str(), append ? "a" : "w");
+    if(!f) return false;
+    for(size_t i = 0; i < rows; ++i)
+        for(size_t j = 0; j < cols; ++j) fprintf(f, j + 1 < cols ? "%lld," : "%lld\n", (long long)v[i * cols + j]);
+    return fclose(f) == 0;
+}
+
+bool write_value(const std::string& path, long long v, bool append)
+{
+    FILE* f = fopen(path.c_str(), append ? "a" : "w");
+    if(!f) return false;
+    fprintf(f, "%lld\n", v);
+    return fclose(f) == 0;
+}
+
+bool write_value(const std::string& path, double v, bool append)
+{
+    FILE* f = fopen(path.c_str(), append ? "a" : "w");
+    if(!f) return false;
+    fprintf(f, "%.10f\n", v);
+    return fclose(f) == 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+kpax_status kpax_plan_bench(kpax_planner* pl, const float* h_init, const float* h_goal, const float* d_obstacles,
+                            uint32_t n_obs, int32_t bench_itr, const char* out_dir, kpax_result* out)
+{
+    if(!pl || !out_dir) return set_error("kpax_plan_bench: null argument"), KPAX_EINVAL;
+    const auto t0 = std::chrono::steady_clock::now();
+    PlanBatch& b = pl->b;
+    kpax_status st = b.begin(h_init, h_goal, 0, &d_obstacles, &n_obs, b.cfg[0].max_iter, 1u);
+    if(st != KPAX_OK) return st;
+    const KParams& p = b.prm[0];
+    const uint32_t cap = p.cap, S = (uint32_t)p.S, n1 = (uint32_t)p.num_r1;
+    const std::string base = std::string(out_dir) + "/Data/", bi = std::to_string(bench_itr);
+    static const char* kDirs[] = {"Samples", "Parents", "TotalCountPerVertex", "ValidCountPerVertex", "Frontier",
+                                  "FrontierRepeatCount", "VertexScores", "FrontierSize", "TreeSize", "ExpandedNodes",
+                                  "ControlPathToGoal"};
+    std::error_code ec;
+    for(const char* d : kDirs) std::filesystem::create_directories(base + d + "/" + d + bi, ec);
+    std::filesystem::create_directories(base + "ExecutionTime", ec);
+    if(ec) return set_error("kpax_plan_bench: cannot create %s: %s", base.c_str(), ec.message().c_str()), KPAX_EINVAL;
+    auto file = [&](const char* d, const std::string& name) { return base + d + "/" + d + bi + "/" + name; };
+    std::vector<float> rows((size_t)cap * S), scores(n1);
+    std::vector<int32_t> parents(cap), counter(n1), valid(n1), r1(cap);
+    std::vector<uint8_t> rep(cap), flag(cap);
+    uint64_t frontier_size = 1;  // the root, the frontier of the first iteration
+    bool ok = true;
+    for(uint32_t itr = 1; itr <= b.cfg[0].max_iter; ++itr) {
+        if((st = b.iterate(1, 1u)) != KPAX_OK || (st = b.sync_ctl()) != KPAX_OK) return st;
+        const Ctl c = b.h_ctl[0];
+        if(c.iters_done < itr) break;  // the plan stopped before this iteration (tree full or error)
+        uint32_t n = 0;
+        std::fill(rows.begin(), rows.end(), 0.0f);
+        std::fill(parents.begin(), parents.end(), -1);
+        if((st = kpax_export_tree(pl, rows.data(), parents.data(), nullptr, cap, &n)) != KPAX_OK) return st;
+        if((st = kpax_export_regions(pl, counter.data(), valid.data(), scores.data(), nullptr)) != KPAX_OK) return st;
+        std::fill(rep.begin(), rep.end(), 0);
+        if((st = kpax_export_frontier(pl, rep.data(), r1.data(), n)) != KPAX_OK) return st;
+        uint64_t next_size = 0;
+        for(uint32_t i = 0; i < n; ++i) {  // last iteration's nodes: their repeat as the next count pass sets it
+            if(rep[i] == kPending) rep[i] = (uint8_t)(valid[r1[i]] < p.sparse_thr ? p.sparse_repeat : 1u);
+            flag[i] = rep[i] != 0;
+            next_size += flag[i];
+        }
+        std::fill(flag.begin() + n, flag.end(), 0);
+        // a run's files start fresh with its first iteration (the reference appends to any left over)
+        const bool app = itr > 1;
+        const std::string k = std::to_string(itr);
+        ok = ok && write_rows_f(file("Samples", "samples" + k + ".csv"), rows.data(), cap, S, false);
+        ok = ok && write_rows_i(file("Parents", "parents" + k + ".csv"), parents.data(), cap, 1, false);
+        ok = ok && write_rows_i(file("TotalCountPerVertex", "totalCountPerVertex.csv"), counter.data(), 1, n1, app);
+        ok = ok && write_rows_i(file("ValidCountPerVertex", "validCountPerVertex.csv"), valid.data(), 1, n1, app);
+        ok = ok && write_rows_i(file("Frontier", "frontier.csv"), flag.data(), 1, cap, app);
+        ok = ok && write_rows_i(file("FrontierRepeatCount", "frontierRepeatCount.csv"), rep.data(), 1, cap, app);
+        ok = ok && write_rows_f(file("VertexScores", "vertexScores.csv"), scores.data(), 1, n1, app);
+        ok = ok && write_value(file("FrontierSize", "frontierSize.csv"), (long long)frontier_size, app);
+        ok = ok && write_value(file("TreeSize", "treeSize.csv"), (long long)c.tree, app);
+        ok = ok && write_value(file("ExpandedNodes", "expandedNodes.csv"), (long long)c.n, app);
+        if(!ok) return set_error("kpax_plan_bench: cannot write under %s", base.c_str()), KPAX_EINVAL;
+        frontier_size = next_size;
+        if(c.goal_idx != kNone || c.full || c.error) break;
+    }
+    if((st = b.finish(out)) != KPAX_OK) return st;
+    if(out->found && !write_rows_f(file("ControlPathToGoal", "controlPathToGoal.csv"), out->h_path, out->path_len, S, false))
+        return set_error("kpax_plan_bench: cannot write the path under %s", base.c_str()), KPAX_EINVAL;
+    const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if(!write_value(base + "ExecutionTime/executionTime.csv", secs, true))
+        return set_error("kpax_plan_bench: cannot write the execution time under %s", base.c_str()), KPAX_EINVAL;
+    return KPAX_OK;
 }
 
 kpax_status kpax_plan_result(kpax_planner* pl, kpax_result* out)

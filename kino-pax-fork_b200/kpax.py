@@ -124,6 +124,7 @@ _SIGNATURES = {
     "kpax_create": (_I32, [ctypes.POINTER(Config), ctypes.POINTER(_VP)]),
     "kpax_destroy": (_I32, [_VP]),
     "kpax_plan": (_I32, [_VP, _VP, _VP, _VP, _U32, _I32, ctypes.POINTER(Result)]),
+    "kpax_plan_bench": (_I32, [_VP, _VP, _VP, _VP, _U32, _I32, ctypes.c_char_p, ctypes.POINTER(Result)]),
     "kpax_plan_host": (_I32, [_VP, _VP, _VP, _VP, _U32, ctypes.POINTER(Result)]),
     "kpax_plan_begin": (_I32, [_VP, _VP, _VP, _VP, _U32]),
     "kpax_plan_iterate": (_I32, [_VP, _U32, _I32]),
@@ -323,6 +324,15 @@ class KPAX:
         init, goal = self._row(h_initial, S), self._row(h_goal, S)
         check(load().kpax_plan(self._h, _ptr(init), _ptr(goal), d_obstacles_ptr, h_obstaclesCount, int(saveTree),
                                ctypes.byref(self.result)), "kpax_plan")
+        return self._publish()
+
+    def planBench(self, h_initial, h_goal, d_obstacles_ptr: int, h_obstaclesCount: int, benchItr: int,
+                  out_dir: str | os.PathLike = ".") -> Result:
+        """KPAX::planBench: the plan with the reference's per-iteration CSV dumps under out_dir/Data."""
+        S = self.sample_dim
+        init, goal = self._row(h_initial, S), self._row(h_goal, S)
+        check(load().kpax_plan_bench(self._h, _ptr(init), _ptr(goal), d_obstacles_ptr, h_obstaclesCount, int(benchItr),
+                                     os.fsencode(os.fspath(out_dir)), ctypes.byref(self.result)), "kpax_plan_bench")
         return self._publish()
 
     def plan_host(self, h_initial, h_goal, obstacles: np.ndarray) -> Result:

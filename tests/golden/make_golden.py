@@ -10,6 +10,8 @@ CUDA path with the reference's outputs on a machine where the reference tree is 
 Each <config>.npz holds: obstacles, parents, draws (n x 6 uniforms: controls in draw order,
 duration, frontier draw), rows and valid from propagateAndCheck*SpatialHash, valid_brute from
 the brute-force propagateAndCheck*, and r1/r2 from getRegion/getSubRegion of the rows.
+quad_<scene>.npz do the same for the quadrotor in the reference's own obstacle files
+(include/config/obstacles/<scene>/obstacles.csv, read with the reference's CSV format).
 """
 import sys
 from pathlib import Path
@@ -24,6 +26,8 @@ import kpax_envs as E  # noqa: E402
 import oracle as O  # noqa: E402
 
 N = 512
+REF_SCENES = Path("/root/reference/include/config/obstacles")
+QUAD_SCENES = ("quadTrees", "quadHouse", "quadPillars")
 
 
 def edge_draws(cfg, n: int, seed: int) -> np.ndarray:
@@ -55,6 +59,19 @@ def main() -> None:
                             valid_brute=valid_b, r1=r1, r2=r2, overflow_cells=np.int32(overflow),
                             start=start, goal=goal)
         print(name, "valid", valid.mean(), "overflow cells", overflow)
+    cfg = kpax.preset(kpax.PRESET_QUAD)
+    for k, scene in enumerate(QUAD_SCENES):
+        obs = E.read_obstacles_csv(REF_SCENES / scene / "obstacles.csv")
+        ref = O.RefLib(cfg.model)
+        overflow = ref.set_obstacles(obs)
+        parents = E.sample_states(cfg.model, N, 300 + k, cfg.v_min, cfg.v_max)
+        draws = edge_draws(cfg, N, 400 + k)
+        rows, valid = ref.propagate(parents, draws, use_hash=True)
+        _, valid_b = ref.propagate(parents, draws, use_hash=False)
+        r1, r2 = ref.regions(rows)
+        np.savez_compressed(out_dir / f"quad_{scene}.npz", obstacles=obs, parents=parents, draws=draws, rows=rows,
+                            valid=valid, valid_brute=valid_b, r1=r1, r2=r2, overflow_cells=np.int32(overflow))
+        print(f"quad_{scene}", obs.shape[0], "obstacles, valid", valid.mean(), "overflow cells", overflow)
 
 
 if __name__ == "__main__":

@@ -67,12 +67,17 @@ def compare_segments(cfg, rows, valid, ref_rows, ref_valid, margin, label):
     return near, float(row_err.max()) if row_err.size else 0.0
 
 
-@pytest.mark.parametrize("name", list(PRESETS))
+# the benchmark scenes per model, and the quadrotor in the reference's own obstacle files
+GOLDEN_SETS = {**PRESETS, "quad_quadTrees": kpax.PRESET_QUAD, "quad_quadHouse": kpax.PRESET_QUAD,
+               "quad_quadPillars": kpax.PRESET_QUAD}
+
+
+@pytest.mark.parametrize("name", list(GOLDEN_SETS))
 def test_propagate_matches_reference_golden(cuda, name):
     import torch
 
     g = np.load(GOLDEN / f"{name}.npz")
-    cfg = kpax.preset(PRESETS[name])
+    cfg = kpax.preset(GOLDEN_SETS[name])
     rows, valid, steps, env = gpu_propagate(torch, cfg, g["obstacles"], g["parents"], g["draws"])
     orow, oval, ostep, margin, nonfinite, kind = O.propagate(cfg, g["obstacles"], g["parents"], g["draws"])
     assert np.array_equal(bits(orow), bits(g["rows"]))  # oracle pinned to the reference

@@ -47,11 +47,16 @@ def test_uniforms_in_half_open_unit_interval():
     assert abs(float(u.mean()) - 0.5) < 0.01
 
 
-@pytest.mark.parametrize("name", list(PRESETS))
+# the benchmark scenes per model, and the quadrotor in the reference's own obstacle files
+GOLDEN_SETS = {**PRESETS, "quad_quadTrees": kpax.PRESET_QUAD, "quad_quadHouse": kpax.PRESET_QUAD,
+               "quad_quadPillars": kpax.PRESET_QUAD}
+
+
+@pytest.mark.parametrize("name", list(GOLDEN_SETS))
 def test_golden_vectors_reproduced(name):
     """The oracle reproduces the reference's outputs stored in tests/golden (bit-exact)."""
     g = np.load(GOLDEN / f"{name}.npz")
-    cfg = kpax.preset(PRESETS[name])
+    cfg = kpax.preset(GOLDEN_SETS[name])
     rows, valid, steps, margin, nonfinite, kind = O.propagate(cfg, g["obstacles"], g["parents"], g["draws"])
     assert np.array_equal(bits(rows), bits(g["rows"]))
     assert np.array_equal(valid, g["valid"])
@@ -184,3 +189,19 @@ def test_oracle_rekino_path():
     b = O.rekino(cfg, s, g, obs, num_warps=16, max_iter=800)
     assert a["found"] and a["warp"] == b["warp"] and np.array_equal(a["path"], b["path"])
     assert np.array_equal(a["path"][0, :6], s[:6]) and np.linalg.norm(a["path"][-1, :3] - g[:3]) < cfg.goal_thresh
+
+
+def test_obstacle_csv_reader(tmp_path):
+    """readObstaclesFromCSV (helper.cu:13-39): comma-separated floats, any number per line, six per
+    obstacle; the written form reads back exactly at float32."""
+    import kpax_envs as E
+
+    text = "50.7722,37.8436,0.0,53.37019999999999,39.3436,20.0\n1,2,3,\n4,5,6\n"
+    (tmp_path / "a.csv").write_text(text)
+    obs = E.read_obstacles_csv(tmp_path / "a.csv")
+    want = np.array([[50.7722, 37.8436, 0.0, 53.37019999999999, 39.3436, 20.0], [1, 2, 3, 4, 5, 6]], np.float32)
+    assert obs.dtype == np.float32 and np.array_equal(obs, want)
+    g = np.load(GOLDEN / "quad_quadTrees.npz")
+    E.write_obstacles_csv(tmp_path / "b.csv", g["obstacles"])
+    back = E.read_obstacles_csv(tmp_path / "b.csv")
+    assert back.shape == (158, 6) and np.allclose(back, g["obstacles"], atol=5e-7 * 100, rtol=0)
