@@ -326,6 +326,8 @@ def main(argv=None):
     e.add_argument("--seeds", type=int, default=256)
     e.add_argument("--eps", type=float, default=0.2)
     e.add_argument("--max-iter", type=int, default=0)
+    e.add_argument("--expansions-log2", type=int, default=0, help="expansions per iteration (log2; 0 = preset)")
+    e.add_argument("--tree-log2", type=int, default=0, help="tree capacity (log2; 0 = preset)")
     pp = sub.add_parser("propose", help="time the tensor-core proposal pass on random states")
     pp.add_argument("--weights", type=Path, default=DEFAULT_WEIGHTS)
     pp.add_argument("--rows", type=int, default=1 << 16)
@@ -378,6 +380,10 @@ def main(argv=None):
     else:
         net = load_network(a.weights)
         seeds = [EVAL_SEED0 + i for i in range(a.seeds)]
+        if a.expansions_log2:
+            cfg.expansions_per_iter = 1 << a.expansions_log2
+        if a.tree_log2:
+            cfg.max_tree_size = 1 << a.tree_log2
         plain = summarize(evaluate(seeds, cfg))
         learned = summarize(evaluate(seeds, cfg, net, a.eps))
         print(json.dumps({"plain": plain, "learned": learned}))
