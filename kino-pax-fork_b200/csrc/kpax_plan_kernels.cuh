@@ -587,7 +587,8 @@ __global__ void __launch_bounds__(kScoreBS) k_scores(const QueryDev* __restrict_
     for(uint32_t w = gtid; w < p.r2_words; w += gsize) rg.cur[w] = rg.nxt[w];
     const int nwarps = gridDim.x * (kScoreBS / 32);
     const uint32_t ngroups = (p.num_r1 + 31) / 32;  // 32 consecutive regions per group
-    for(int j = blockIdx.x * (kScoreBS / 32) + (tid >> 5); j < kPartials; j += nwarps) {
+    const int used = (int)min(ngroups, (uint32_t)kPartials);  // partials at and above `used` stay 0
+    for(int j = blockIdx.x * (kScoreBS / 32) + (tid >> 5); j < used; j += nwarps) {
         float part = 0.0f;
         for(uint32_t grp = j; grp < ngroups; grp += kPartials) {
             const int r = 32 * grp + lane;
@@ -614,18 +615,25 @@ __global__ void __launch_bounds__(kScoreBS) k_scores(const QueryDev* __restrict_
     }
     __threadfence();
     __syncthreads();
-    if(tid == 0) s_last = atomicAdd(sq.sarr, 1u) == gridDim.x - 1u;
+    if(gridDim.x > 1) {  // the last CTA to arrive adds the partials
+        if(tid == 0) s_last = atomicAdd(sq.sarr, 1u) == gridDim.x - 1u;
+        __syncthreads();
+        if(!s_last) return;
+        __threadfence();
+    }
+    // halving tree over the 1024 partials; the levels whose upper halves hold only the zero
+    // partials at and above `used` leave the lower entries unchanged (x + 0 = x), so the tree
+    // starts at the first power of two not below `used` and gives the same total
+    int half = 1;
+    while(half < used) half <<= 1;
+    for(int j = tid; j < half; j += kScoreBS) s_part[j] = j < used ? ((volatile float*)sq.partials)[j] : 0.0f;
     __syncthreads();
-    if(!s_last) return;
-    __threadfence();
-    for(int j = tid; j < kPartials; j += kScoreBS) s_part[j] = ((volatile float*)sq.partials)[j];
-    __syncthreads();
-    for(int s = kPartials / 2; s > 0; s >>= 1) {
+    for(int s = half / 2; s > 0; s >>= 1) {
         for(int j = tid; j < s; j += kScoreBS) s_part[j] = __fadd_rn(s_part[j], s_part[j + s]);
         __syncthreads();
     }
     if(tid == 0) {
-        *sq.sarr = 0u;
+        if(gridDim.x > 1) *sq.sarr = 0u;
         ctl->score_total = s_part[0];
         ctl->scores_ready = 1u;
         const uint32_t iter = ctl->iter, tree_old = ctl->tree, tree_new = tree_old + ctl->appended;

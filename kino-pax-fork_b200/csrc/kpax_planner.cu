@@ -212,7 +212,10 @@ struct PlanBatch {
         }
         gx_front = n == 1 ? std::min<uint32_t>(max_tiles, kFrontierCTAs)
                           : std::max<uint32_t>(1, std::min<uint32_t>(max_tiles, 8 * 148 * 2 / n));
-        gx_score = n == 1 ? kScoreCTAs : std::max<uint32_t>(1, 1024 / n);
+        // a single query: enough CTAs for its 32-region groups (eight warps each), at most kScoreCTAs
+        const uint32_t groups0 = ((uint32_t)prm[0].num_r1 + 31) / 32;
+        gx_score = n == 1 ? std::min<uint32_t>(kScoreCTAs, std::max<uint32_t>(1, (groups0 + 7) / 8))
+                          : std::max<uint32_t>(1, 1024 / n);
         // control blocks, counters and arrival flags start at zero; no node is in a frontier
         KPAX_CUDA(cudaMemsetAsync(pool, 0, region_lo, stream));
         KPAX_CUDA(cudaMemsetAsync(d_ctl, 0, sizeof(Ctl) * n, stream));
