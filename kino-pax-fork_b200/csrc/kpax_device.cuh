@@ -100,13 +100,26 @@ __device__ __forceinline__ void sincos_checked(float x, float* sn, float* cs)
 // stages evaluate the attitude at a0 + (h/2) k and a0 + h k; this replaces three of every four
 // full evaluations per angle and step.
 constexpr float kShiftMax = 0.25f;
-__device__ __forceinline__ void sincos_shift(float s0, float c0, float d, float* sn, float* cs)
+struct ShiftCoef {
+    float sd, cm;  // sin(d) and cos(d) - 1
+};
+
+__device__ __forceinline__ ShiftCoef shift_coef(float d)
 {
     const float d2 = d * d;
-    const float sd = fmaf(d * d2, fmaf(d2, fmaf(d2, -1.0f / 5040.0f, 1.0f / 120.0f), -1.0f / 6.0f), d);
-    const float cm = d2 * fmaf(d2, fmaf(d2, fmaf(d2, 1.0f / 40320.0f, -1.0f / 720.0f), 1.0f / 24.0f), -0.5f);
-    *sn = fmaf(s0, cm, fmaf(c0, sd, s0));
-    *cs = fmaf(c0, cm, fmaf(-s0, sd, c0));
+    return {fmaf(d * d2, fmaf(d2, fmaf(d2, -1.0f / 5040.0f, 1.0f / 120.0f), -1.0f / 6.0f), d),
+            d2 * fmaf(d2, fmaf(d2, fmaf(d2, 1.0f / 40320.0f, -1.0f / 720.0f), 1.0f / 24.0f), -0.5f)};
+}
+
+__device__ __forceinline__ void sincos_apply(float s0, float c0, ShiftCoef k, float* sn, float* cs)
+{
+    *sn = fmaf(s0, k.cm, fmaf(c0, k.sd, s0));
+    *cs = fmaf(c0, k.cm, fmaf(-s0, k.sd, c0));
+}
+
+__device__ __forceinline__ void sincos_shift(float s0, float c0, float d, float* sn, float* cs)
+{
+    sincos_apply(s0, c0, shift_coef(d), sn, cs);
 }
 
 // Square root and reciprocal by the PTX approximations sqrt.approx.f32 / rcp.approx.f32 (about one
@@ -308,23 +321,42 @@ __device__ __forceinline__ int draw_controls(const KParams& p, const float u[6],
 // (bounds, then the swept box's collision query); the output row holds the state after the
 // failing step, as the reference's break does.
 
-// Double integrator, statePropagatorSpatialHash.cu:72-134 (Q1: x += h(5v + 2ah)/6).  One step
-// from s in place; false when the step fails a check (velocity box, workspace, finite, collision).
-__device__ __forceinline__ bool step_di(const KParams& p, const Grid& g, float* s, const float* c)
+// Double integrator, statePropagatorSpatialHash.cu:72-134 (Q1: x += h(5v + 2ah)/6).  The terms
+// that depend on the segment's acceleration only (a*h/2, a*h and the velocity increment
+// (a + 2a + 2a + a)*h/6) are computed once per segment, with the same rounded operations.
+struct DIConsts {
+    float ah2[3], ah[3], dv[3];
+};
+
+__device__ __forceinline__ DIConsts di_consts(const KParams& p, const float* c)
+{
+    DIConsts k;
+#pragma unroll
+    for(int d = 0; d < 3; ++d) {
+        const float a = c[d];
+        k.ah[d] = __fmul_rn(a, p.h);
+        k.ah2[d] = __fdiv_rn(k.ah[d], 2.0f);
+        const float asum = __fadd_rn(__fadd_rn(__fadd_rn(a, __fmul_rn(2.0f, a)), __fmul_rn(2.0f, a)), a);
+        k.dv[d] = __fdiv_rn(__fmul_rn(asum, p.h), 6.0f);
+    }
+    return k;
+}
+
+// One step from s in place; false when the step fails a check (velocity box, workspace, finite,
+// collision).
+__device__ __forceinline__ bool step_di(const KParams& p, const Grid& g, float* s, const DIConsts& k)
 {
     const float h = p.h;
     const float p0[3] = {s[0], s[1], s[2]};
 #pragma unroll
     for(int d = 0; d < 3; ++d) {
-        const float v = s[3 + d], a = c[d];
+        const float v = s[3 + d];
         // (v + (v + 2*(v + a*h/2) + (v + a*h))) * h / 6
-        const float t1 = __fadd_rn(v, __fdiv_rn(__fmul_rn(a, h), 2.0f));
-        const float t2 = __fadd_rn(v, __fmul_rn(a, h));
+        const float t1 = __fadd_rn(v, k.ah2[d]);
+        const float t2 = __fadd_rn(v, k.ah[d]);
         const float sum = __fadd_rn(v, __fadd_rn(__fadd_rn(v, __fmul_rn(2.0f, t1)), t2));
         s[d] = __fadd_rn(s[d], __fdiv_rn(__fmul_rn(sum, h), 6.0f));
-        // (a + 2a + 2a + a) * h / 6
-        const float asum = __fadd_rn(__fadd_rn(__fadd_rn(a, __fmul_rn(2.0f, a)), __fmul_rn(2.0f, a)), a);
-        s[3 + d] = __fadd_rn(v, __fdiv_rn(__fmul_rn(asum, h), 6.0f));
+        s[3 + d] = __fadd_rn(v, k.dv[d]);  // v + (a + 2a + 2a + a) * h / 6
     }
     if(s[3] < p.vmin || s[3] > p.vmax || s[4] < p.vmin || s[4] > p.vmax || s[5] < p.vmin || s[5] > p.vmax) return false;
     if(s[0] < p.ws_lo || s[0] > p.ws_hi || s[1] < p.ws_lo || s[1] > p.ws_hi || s[2] < p.ws_lo || s[2] > p.ws_hi) return false;
@@ -333,7 +365,21 @@ __device__ __forceinline__ bool step_di(const KParams& p, const Grid& g, float* 
 
 // Dubins airplane, statePropagatorSpatialHash.cu:139-229; c = (a, yawRate, pitchRate).  One step
 // from s in place; false when the step fails a check (speed, pitch range, workspace, finite, collision).
-__device__ __forceinline__ bool step_dubins(const KParams& p, const Grid& g, float* s, const float* c)
+// The stage angle increments of a Dubins segment are its fixed rates times h/2 and h, so their
+// sine / cosine series are evaluated once per segment.
+struct DubinsShifts {
+    bool shift;  // all four increments within kShiftMax
+    ShiftCoef p1, y1, p2, y2;
+};
+
+__device__ __forceinline__ DubinsShifts dubins_shifts(const KParams& p, const float* c)
+{
+    const float h = p.h, hh = p.hh, yr = c[1], pr = c[2];
+    return {fmaxf(fabsf(h * pr), fabsf(h * yr)) <= kShiftMax, shift_coef(hh * pr), shift_coef(hh * yr), shift_coef(h * pr),
+            shift_coef(h * yr)};
+}
+
+__device__ __forceinline__ bool step_dubins(const KParams& p, const Grid& g, float* s, const float* c, const DubinsShifts& k)
 {
     const float h = p.h, hh = p.hh, h6 = p.h6;
     const float a = c[0], yr = c[1], pr = c[2];
@@ -342,11 +388,11 @@ __device__ __forceinline__ bool step_dubins(const KParams& p, const Grid& g, flo
     float sp0, cp0, sy0, cy0, sp1, cp1, sy1, cy1, sp2, cp2, sy2, cy2;
     sincos_checked(pitch, &sp0, &cp0);
     sincos_checked(yaw, &sy0, &cy0);
-    if(fmaxf(fabsf(h * pr), fabsf(h * yr)) <= kShiftMax) {
-        sincos_shift(sp0, cp0, hh * pr, &sp1, &cp1);
-        sincos_shift(sy0, cy0, hh * yr, &sy1, &cy1);
-        sincos_shift(sp0, cp0, h * pr, &sp2, &cp2);
-        sincos_shift(sy0, cy0, h * yr, &sy2, &cy2);
+    if(k.shift) {
+        sincos_apply(sp0, cp0, k.p1, &sp1, &cp1);
+        sincos_apply(sy0, cy0, k.y1, &sy1, &cy1);
+        sincos_apply(sp0, cp0, k.p2, &sp2, &cp2);
+        sincos_apply(sy0, cy0, k.y2, &sy2, &cy2);
     } else {
         sincos_checked(pitch + hh * pr, &sp1, &cp1);
         sincos_checked(yaw + hh * yr, &sy1, &cy1);
@@ -443,11 +489,22 @@ __device__ __forceinline__ bool step_quad(const KParams& p, const Grid& g, float
     return finite_all(s, 12) && step_free(g, p0, s);
 }
 
+// Per-segment constants of a model's step (the double integrator's acceleration terms, the Dubins
+// stage shifts; nothing for the quadrotor).
+struct NoSegmentConsts {};
 template <int M>
-__device__ __forceinline__ bool model_step(const KParams& p, const Grid& g, float* s, const float* c)
+__device__ __forceinline__ auto segment_consts(const KParams& p, const float* c)
 {
-    if constexpr(M == KPAX_MODEL_DOUBLE_INTEGRATOR) return step_di(p, g, s, c);
-    else if constexpr(M == KPAX_MODEL_DUBINS_AIRPLANE) return step_dubins(p, g, s, c);
+    if constexpr(M == KPAX_MODEL_DUBINS_AIRPLANE) return dubins_shifts(p, c);
+    else if constexpr(M == KPAX_MODEL_DOUBLE_INTEGRATOR) return di_consts(p, c);
+    else return NoSegmentConsts{};
+}
+
+template <int M, class K>
+__device__ __forceinline__ bool model_step(const KParams& p, const Grid& g, float* s, const float* c, const K& k)
+{
+    if constexpr(M == KPAX_MODEL_DOUBLE_INTEGRATOR) return step_di(p, g, s, k);
+    else if constexpr(M == KPAX_MODEL_DUBINS_AIRPLANE) return step_dubins(p, g, s, c, k);
     else return step_quad(p, g, s, c);
 }
 
@@ -456,8 +513,9 @@ __device__ __forceinline__ bool model_step(const KParams& p, const Grid& g, floa
 template <int M>
 __device__ __forceinline__ bool propagate(const KParams& p, const Grid& g, float* s, const float* c, int steps, int& done)
 {
+    const auto k = segment_consts<M>(p, c);
     for(int i = 0; i < steps; ++i) {
-        if(!model_step<M>(p, g, s, c)) {
+        if(!model_step<M>(p, g, s, c, k)) {
             done = i + 1;
             return false;
         }
