@@ -321,6 +321,17 @@ __device__ __forceinline__ int draw_controls(const KParams& p, const float u[6],
 // (bounds, then the swept box's collision query); the output row holds the state after the
 // failing step, as the reference's break does.
 
+// The configuration values a step reads, copied to registers once per segment (the planner keeps
+// its KParams in shared memory).
+struct StepParams {
+    float h, hh, h6, vmin, vmax, ws_lo, ws_hi, pitch_lo, pitch_hi;
+};
+
+__device__ __forceinline__ StepParams step_params(const KParams& p)
+{
+    return {p.h, p.hh, p.h6, p.vmin, p.vmax, p.ws_lo, p.ws_hi, p.pitch_lo, p.pitch_hi};
+}
+
 // Double integrator, statePropagatorSpatialHash.cu:72-134 (Q1: x += h(5v + 2ah)/6).  The terms
 // that depend on the segment's acceleration only (a*h/2, a*h and the velocity increment
 // (a + 2a + 2a + a)*h/6) are computed once per segment, with the same rounded operations.
@@ -344,7 +355,7 @@ __device__ __forceinline__ DIConsts di_consts(const KParams& p, const float* c)
 
 // One step from s in place; false when the step fails a check (velocity box, workspace, finite,
 // collision).
-__device__ __forceinline__ bool step_di(const KParams& p, const Grid& g, float* s, const DIConsts& k)
+__device__ __forceinline__ bool step_di(const StepParams& p, const Grid& g, float* s, const DIConsts& k)
 {
     const float h = p.h;
     const float p0[3] = {s[0], s[1], s[2]};
@@ -379,7 +390,7 @@ __device__ __forceinline__ DubinsShifts dubins_shifts(const KParams& p, const fl
             shift_coef(h * yr)};
 }
 
-__device__ __forceinline__ bool step_dubins(const KParams& p, const Grid& g, float* s, const float* c, const DubinsShifts& k)
+__device__ __forceinline__ bool step_dubins(const StepParams& p, const Grid& g, float* s, const float* c, const DubinsShifts& k)
 {
     const float h = p.h, hh = p.hh, h6 = p.h6;
     const float a = c[0], yr = c[1], pr = c[2];
@@ -464,7 +475,7 @@ __device__ __forceinline__ void quad_rhs(float* xd, const float* x0, const float
 // before writing its own); the stage sum keeps the reference's order ((k1 + 2k2) + 2k3) + k4.
 // One step from s in place; false when the step fails a check (velocity box, workspace, finite,
 // collision).
-__device__ __forceinline__ bool step_quad(const KParams& p, const Grid& g, float* s, const float* c)
+__device__ __forceinline__ bool step_quad(const StepParams& p, const Grid& g, float* s, const float* c)
 {
     const float h = p.h, hh = p.hh, h6 = p.h6;
     const float p0[3] = {s[0], s[1], s[2]};
@@ -501,7 +512,7 @@ __device__ __forceinline__ auto segment_consts(const KParams& p, const float* c)
 }
 
 template <int M, class K>
-__device__ __forceinline__ bool model_step(const KParams& p, const Grid& g, float* s, const float* c, const K& k)
+__device__ __forceinline__ bool model_step(const StepParams& p, const Grid& g, float* s, const float* c, const K& k)
 {
     if constexpr(M == KPAX_MODEL_DOUBLE_INTEGRATOR) return step_di(p, g, s, k);
     else if constexpr(M == KPAX_MODEL_DUBINS_AIRPLANE) return step_dubins(p, g, s, c, k);
@@ -514,8 +525,10 @@ template <int M>
 __device__ __forceinline__ bool propagate(const KParams& p, const Grid& g, float* s, const float* c, int steps, int& done)
 {
     const auto k = segment_consts<M>(p, c);
+    const StepParams sp = step_params(p);
+    const Grid gl = g;  // register copy of the grid's pointers and cell map
     for(int i = 0; i < steps; ++i) {
-        if(!model_step<M>(p, g, s, c, k)) {
+        if(!model_step<M>(sp, gl, s, c, k)) {
             done = i + 1;
             return false;
         }
