@@ -14,6 +14,12 @@ the reference's own counter (sum of d_validCounterArray_, src/planners/KPAX.cu:3
          host (oracle/_ref, OpenMP over all cores) on a bounded sample of the same children.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload quad|dubins|di|segments|learned|batch]
+
+Other workloads: dubins / di (the same iteration on the other models), segments (2^22 independent
+Dubins segments through kpax_propagate_batch), learned (learned-vs-plain A/B on 256 held-out
+scenes, tensor-core pass and training rates), batch (1024 mixed queries in one batched plan).
+The reference arm has no counterpart for learned and batch and says so.
 """
 from __future__ import annotations
 
@@ -217,6 +223,12 @@ def cpu_segments_rate(budget_s: float, n: int = 1 << 16, steps: int = 3):
 def run_reference(args) -> None:
     ws, rank, _ = dist_setup(args.gpus)
     if rank != 0:
+        return
+    if args.workload in ("learned", "batch"):
+        why = ("the reference has no learned proposal" if args.workload == "learned" else
+               "the reference plans one query per plan() call with a compile-time model; its per-child routines are "
+               "timed by the single-query workloads")
+        print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
         return
     if args.workload == "segments":
         rate, threads, sample, ms = cpu_segments_rate(min(20.0, 2.0 * max(args.steps, 1)), steps=max(args.steps, 1))
