@@ -10,6 +10,7 @@
 #include <string.h>
 
 #include <mutex>
+#include <new>
 
 #include "kpax_internal.h"
 
@@ -305,9 +306,10 @@ kpax_status kpax_test_sincos(const float* d_x, uint32_t n, float* d_out, void* s
 
 kpax_status kpax_env_create(const kpax_config* cfg, const float* d_obstacles, uint32_t n_obs, void* stream, kpax_env** out)
 {
-    if(!out || (n_obs && !d_obstacles)) return set_error("kpax_env_create: null argument"), KPAX_EINVAL;
+    if(!cfg || !out || (n_obs && !d_obstacles)) return set_error("kpax_env_create: null argument"), KPAX_EINVAL;
     *out = nullptr;
-    kpax_env* e = new kpax_env();
+    kpax_env* e = new(std::nothrow) kpax_env();
+    if(!e) return set_error("kpax_env_create: host allocation failed"), KPAX_ENOMEM;
     kpax_status st = derive_params(*cfg, &e->params);
     if(st == KPAX_OK) st = e->env.build(e->params, d_obstacles, n_obs, (cudaStream_t)stream);
     if(st == KPAX_OK) {

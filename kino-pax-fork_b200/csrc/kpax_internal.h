@@ -4,6 +4,8 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <exception>
+#include <new>
 
 #include "kpax_device.cuh"
 #include "kpax_params.h"
@@ -19,6 +21,24 @@
     } while(0)
 
 #define KPAX_CHECK_LAUNCH() KPAX_CUDA(cudaGetLastError())
+
+namespace kpax {
+// Runs f() and turns a C++ exception (a failed host allocation above all) into a status, so
+// nothing thrown crosses the C ABI.
+template <class F>
+kpax_status no_throw(const char* what, F&& f)
+{
+    try {
+        return f();
+    } catch(const std::bad_alloc&) {
+        set_error("%s: host allocation failed", what);
+        return KPAX_ENOMEM;
+    } catch(const std::exception& e) {
+        set_error("%s: %s", what, e.what());
+        return KPAX_EINVAL;
+    }
+}
+}  // namespace kpax
 
 namespace kpax {
 

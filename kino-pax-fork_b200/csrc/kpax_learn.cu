@@ -13,6 +13,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <new>
 #include <vector>
 
 #include "kpax.h"
@@ -415,7 +416,8 @@ kpax_status kpax_mlp_create(uint32_t max_batch, kpax_mlp** out)
 {
     if(!out || max_batch == 0 || max_batch > (1u << 22)) return set_error("kpax_mlp_create: bad arguments"), KPAX_EINVAL;
     *out = nullptr;
-    kpax_mlp* n = new kpax_mlp();
+    kpax_mlp* n = new(std::nothrow) kpax_mlp();
+    if(!n) return set_error("kpax_mlp_create: host allocation failed"), KPAX_ENOMEM;
     n->max_batch = max_batch;
     const size_t P = kNumParams, B = max_batch;
     auto fail = [&](kpax_status st) {

@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <chrono>
 #include <filesystem>
+#include <new>
 #include <string>
 #include <vector>
 
@@ -599,8 +600,9 @@ kpax_status kpax_create(const kpax_config* cfg, kpax_planner** out)
 {
     if(!cfg || !out) return set_error("kpax_create: null argument"), KPAX_EINVAL;
     *out = nullptr;
-    kpax_planner* pl = new kpax_planner();
-    kpax_status st = pl->b.init(cfg, 1);
+    kpax_planner* pl = new(std::nothrow) kpax_planner();
+    if(!pl) return set_error("kpax_create: host allocation failed"), KPAX_ENOMEM;
+    kpax_status st = no_throw("kpax_create", [&] { return pl->b.init(cfg, 1); });
     if(st != KPAX_OK) {
         pl->b.release();
         delete pl;
@@ -752,8 +754,8 @@ bool write_value(const std::string& path, double v, bool append)
 
 extern "C" {
 
-kpax_status kpax_plan_bench(kpax_planner* pl, const float* h_init, const float* h_goal, const float* d_obstacles,
-                            uint32_t n_obs, int32_t bench_itr, const char* out_dir, kpax_result* out)
+static kpax_status plan_bench_body(kpax_planner* pl, const float* h_init, const float* h_goal, const float* d_obstacles,
+                                   uint32_t n_obs, int32_t bench_itr, const char* out_dir, kpax_result* out)
 {
     if(!pl || !out_dir) return set_error("kpax_plan_bench: null argument"), KPAX_EINVAL;
     const auto t0 = std::chrono::steady_clock::now();
@@ -820,14 +822,30 @@ kpax_status kpax_plan_bench(kpax_planner* pl, const float* h_init, const float* 
     return KPAX_OK;
 }
 
+kpax_status kpax_plan_bench(kpax_planner* pl, const float* h_init, const float* h_goal, const float* d_obstacles,
+                            uint32_t n_obs, int32_t bench_itr, const char* out_dir, kpax_result* out)
+{
+    return no_throw("kpax_plan_bench",
+                    [&] { return plan_bench_body(pl, h_init, h_goal, d_obstacles, n_obs, bench_itr, out_dir, out); });
+}
+
 kpax_status kpax_plan_result(kpax_planner* pl, kpax_result* out)
 {
     if(!pl || !pl->b.begun) return set_error("kpax_plan_result: no plan"), KPAX_EINVAL;
     return pl->b.finish(out);
 }
 
+static kpax_status export_tree_body(kpax_planner* pl, float* h_rows, int32_t* h_parents, float* h_costs, uint32_t max_rows,
+                                    uint32_t* n_rows);
+
 kpax_status kpax_export_tree(kpax_planner* pl, float* h_rows, int32_t* h_parents, float* h_costs, uint32_t max_rows,
                              uint32_t* n_rows)
+{
+    return no_throw("kpax_export_tree", [&] { return export_tree_body(pl, h_rows, h_parents, h_costs, max_rows, n_rows); });
+}
+
+static kpax_status export_tree_body(kpax_planner* pl, float* h_rows, int32_t* h_parents, float* h_costs, uint32_t max_rows,
+                                    uint32_t* n_rows)
 {
     if(!pl) return set_error("kpax_export_tree: null planner"), KPAX_EINVAL;
     PlanBatch& b = pl->b;
@@ -949,8 +967,9 @@ kpax_status kpax_batch_create(const kpax_config* cfgs, uint32_t n, kpax_batch** 
 {
     if(!cfgs || !n || !out) return set_error("kpax_batch_create: null argument or empty batch"), KPAX_EINVAL;
     *out = nullptr;
-    kpax_batch* b = new kpax_batch();
-    kpax_status st = b->b.init(cfgs, n);
+    kpax_batch* b = new(std::nothrow) kpax_batch();
+    if(!b) return set_error("kpax_batch_create: host allocation failed"), KPAX_ENOMEM;
+    kpax_status st = no_throw("kpax_batch_create", [&] { return b->b.init(cfgs, n); });
     if(st != KPAX_OK) {
         b->b.release();
         delete b;

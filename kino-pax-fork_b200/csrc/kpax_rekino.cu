@@ -23,6 +23,8 @@
 #include <vector>
 
 #include "kpax.h"
+#include <new>
+
 #include "kpax_internal.h"
 
 using namespace kpax;
@@ -232,7 +234,8 @@ kpax_status kpax_rekino_create(const kpax_config* cfg, const kpax_rekino_params*
         return set_error("kpax_rekino_create: samples_per_thread in [1, 16]"), KPAX_EINVAL;
     if(!(rp->epsilon_greedy >= 0.0f && rp->epsilon_greedy <= 1.0f) || !(rp->timeout_ms > 0.0))
         return set_error("kpax_rekino_create: epsilon_greedy in [0,1] and a positive timeout"), KPAX_EINVAL;
-    kpax_rekino* r = new kpax_rekino();
+    kpax_rekino* r = new(std::nothrow) kpax_rekino();
+    if(!r) return set_error("kpax_rekino_create: host allocation failed"), KPAX_ENOMEM;
     r->cfg = *cfg;
     r->rp = *rp;
     kpax_status st = derive_params(*cfg, &r->p);
@@ -271,8 +274,17 @@ kpax_status kpax_rekino_destroy(kpax_rekino* r)
     return KPAX_OK;
 }
 
+static kpax_status rekino_plan_body(kpax_rekino* r, const float* h_init, const float* h_goal, const float* d_obstacles,
+                                    uint32_t n_obs, kpax_result* out);
+
 kpax_status kpax_rekino_plan(kpax_rekino* r, const float* h_init, const float* h_goal, const float* d_obstacles, uint32_t n_obs,
                              kpax_result* out)
+{
+    return no_throw("kpax_rekino_plan", [&] { return rekino_plan_body(r, h_init, h_goal, d_obstacles, n_obs, out); });
+}
+
+static kpax_status rekino_plan_body(kpax_rekino* r, const float* h_init, const float* h_goal, const float* d_obstacles,
+                                    uint32_t n_obs, kpax_result* out)
 {
     if(!r || !h_init || !h_goal || !out || (n_obs && !d_obstacles)) return set_error("kpax_rekino_plan: null argument"), KPAX_EINVAL;
     const KParams& p = r->p;

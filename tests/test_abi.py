@@ -106,3 +106,18 @@ def test_pruning_parameters_are_validated():
     assert lib.kpax_config_validate(ctypes.byref(cfg)) == kpax.EINVAL
     cfg.prune = 0
     assert lib.kpax_config_validate(ctypes.byref(cfg)) == kpax.OK
+
+
+def test_null_arguments_are_rejected_without_a_gpu():
+    """Every creation and plan call checks its pointers before touching the device."""
+    lib = kpax.load()
+    out = ctypes.c_void_p()
+    cfg = kpax.preset(kpax.PRESET_DI)
+    assert lib.kpax_create(None, ctypes.byref(out)) == kpax.EINVAL
+    assert lib.kpax_create(ctypes.byref(cfg), None) == kpax.EINVAL
+    assert lib.kpax_env_create(None, None, 0, None, ctypes.byref(out)) == kpax.EINVAL
+    assert lib.kpax_batch_create(ctypes.byref(cfg), 0, ctypes.byref(out)) == kpax.EINVAL
+    assert lib.kpax_plan(None, None, None, None, 0, 0, None) == kpax.EINVAL
+    assert lib.kpax_plan_bench(None, None, None, None, 0, 0, None, None) == kpax.EINVAL
+    assert lib.kpax_export_tree(None, None, None, None, 0, None) == kpax.EINVAL
+    assert lib.kpax_last_error()
