@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define KPAX_ABI_VERSION 1
+#define KPAX_ABI_VERSION 2
 
 typedef enum kpax_status {
     KPAX_OK = 0,

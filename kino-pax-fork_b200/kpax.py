@@ -17,6 +17,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libkpax.so"
+ABI_VERSION = 2  # KPAX_ABI_VERSION of include/kpax.h this binding was written for
 
 OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, ECAPACITY, ENOTFOUND = range(7)
 MODEL_DOUBLE_INTEGRATOR, MODEL_DUBINS_AIRPLANE, MODEL_QUADROTOR = 1, 2, 3
@@ -197,6 +198,8 @@ def load(path: os.PathLike | None = None) -> ctypes.CDLL:
     for name, (res, args) in _SIGNATURES.items():
         fn = getattr(lib, name)
         fn.restype, fn.argtypes = res, args
+    if lib.kpax_abi_version() != ABI_VERSION:
+        raise ImportError(f"{p} has ABI version {lib.kpax_abi_version()}, this binding expects {ABI_VERSION}: rebuild it")
     if path is None:
         _lib = lib
     return lib
