@@ -167,6 +167,122 @@ __global__ void __launch_bounds__(256, 4) k_propagate_batch(KParams p, Grid g, c
     if(steps_out) steps_out[i] = done;
 }
 
+// Large batches run in two phases so that lanes do not idle behind their warp's longest segment:
+// the head runs every segment for its first kHeadSteps steps and finishes the segments that end
+// there (a fifth of them fail in their first steps); the others are appended, state and controls,
+// to a compact list that the tail carries to the end with full warps.  Both phases run the same
+// per-step code in the same order, so rows, verdicts and step counts equal the one-pass kernel's.
+constexpr int kHeadSteps = 2;
+constexpr uint32_t kTwoPhaseMin = 1u << 18;  // segments; below this the one-pass kernel is used
+
+struct LiveList {
+    uint32_t* count;
+    uint32_t* idx;
+    int32_t* steps;
+    float* ctl;    // 4 per entry
+    float* state;  // SD per entry
+};
+
+template <int M>
+__device__ __forceinline__ void write_segment(const KParams& p, uint32_t i, const float* s, const float* c, int steps, bool ok,
+                                              int done, float* __restrict__ rows, uint8_t* __restrict__ valid,
+                                              int32_t* __restrict__ steps_out)
+{
+    constexpr int SD = ModelDims<M>::SD, CD = ModelDims<M>::CD, S = SD + CD + 1;
+    float rc[4];
+    row_controls<M>(c, rc);
+    float* dst = rows + (size_t)i * S;
+#pragma unroll
+    for(int k = 0; k < SD; ++k) dst[k] = s[k];
+#pragma unroll
+    for(int k = 0; k < CD; ++k) dst[SD + k] = rc[k];
+    dst[SD + CD] = __fmul_rn(p.h, (float)steps);
+    valid[i] = ok ? 1 : 0;
+    if(steps_out) steps_out[i] = done;
+}
+
+template <int M>
+__global__ void __launch_bounds__(256, 4) k_propagate_head(KParams p, Grid g, const float* __restrict__ parents,
+                                                        const float* __restrict__ draws, uint32_t stream_id, uint32_t n,
+                                                        float* __restrict__ rows, uint8_t* __restrict__ valid,
+                                                        int32_t* __restrict__ steps_out, LiveList live)
+{
+    constexpr int SD = ModelDims<M>::SD;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    bool alive = false;
+    float s[SD], c[4];
+    int steps = 0;
+    if(i < n) {
+        float u[6];
+#pragma unroll
+        for(int k = 0; k < SD; ++k) s[k] = __ldg(parents + (size_t)i * SD + k);
+        if(draws) {
+#pragma unroll
+            for(int k = 0; k < 5; ++k) u[k] = __ldg(draws + (size_t)i * 5 + k);
+            u[5] = 0.0f;
+        } else {
+            child_draws(p, stream_id, 0u, i, u);
+        }
+        steps = draw_controls(p, u, c);
+        const auto k = segment_consts<M>(p, c);
+        const StepParams sp = step_params(p);
+        bool ok = true;
+        int done = 0;
+        while(done < steps && done < kHeadSteps) {
+            ok = model_step<M>(sp, g, s, c, k);
+            ++done;
+            if(!ok) break;
+        }
+        alive = ok && done < steps;
+        if(!alive) write_segment<M>(p, i, s, c, steps, ok, done, rows, valid, steps_out);
+    }
+    // append the live segments, one atomic per warp
+    const uint32_t m = __ballot_sync(0xffffffffu, alive);
+    if(m) {
+        const int leader = __ffs(m) - 1;
+        uint32_t base = 0;
+        if(lane == leader) base = atomicAdd(live.count, (uint32_t)__popc(m));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if(alive) {
+            const uint32_t j = base + __popc(m & ((1u << lane) - 1u));
+            live.idx[j] = i;
+            live.steps[j] = steps;
+#pragma unroll
+            for(int k = 0; k < 4; ++k) live.ctl[(size_t)j * 4 + k] = c[k];
+#pragma unroll
+            for(int k = 0; k < SD; ++k) live.state[(size_t)j * SD + k] = s[k];
+        }
+    }
+}
+
+template <int M>
+__global__ void __launch_bounds__(256, 4) k_propagate_tail(KParams p, Grid g, float* __restrict__ rows,
+                                                        uint8_t* __restrict__ valid, int32_t* __restrict__ steps_out,
+                                                        LiveList live)
+{
+    constexpr int SD = ModelDims<M>::SD;
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if(j >= *live.count) return;
+    const uint32_t i = live.idx[j];
+    const int steps = live.steps[j];
+    float s[SD], c[4];
+#pragma unroll
+    for(int k = 0; k < 4; ++k) c[k] = live.ctl[(size_t)j * 4 + k];
+#pragma unroll
+    for(int k = 0; k < SD; ++k) s[k] = live.state[(size_t)j * SD + k];
+    const auto kc = segment_consts<M>(p, c);
+    const StepParams sp = step_params(p);
+    bool ok = true;
+    int done = kHeadSteps;
+    while(done < steps) {
+        ok = model_step<M>(sp, g, s, c, kc);
+        ++done;
+        if(!ok) break;
+    }
+    write_segment<M>(p, i, s, c, steps, ok, done, rows, valid, steps_out);
+}
+
 __global__ void k_collide_batch(Grid g, const float* __restrict__ bbmin, const float* __restrict__ bbmax, uint32_t n,
                                 uint8_t* __restrict__ free_out)
 {
@@ -261,6 +377,7 @@ void Env::release()
     if(d_off) cudaFree(d_off);
     if(d_cursor) cudaFree(d_cursor);
     if(d_ent) cudaFree(d_ent);
+    if(d_live) cudaFree(d_live), d_live = nullptr, live_cap = 0;
     if(h_total) cudaFreeHost(h_total);
     d_obs = nullptr, d_off = d_cursor = d_ent = h_total = nullptr;
     obs_cap = ent_cap = n_cells = n_ent = n_obs = 0;
@@ -353,8 +470,44 @@ kpax_status kpax_propagate_batch(const kpax_config* cfg, kpax_env* env, const fl
     if(st != KPAX_OK) return st;
     if(p.gdim != env->env.dim || p.cell != env->env.cell || p.wmin != env->env.wmin)
         return set_error("kpax_propagate_batch: env was built for another workspace grid"), KPAX_EINVAL;
-    return launch_propagate(p, env->env.view(), d_parents, d_draws, draw_stream, n, d_rows, d_valid, d_steps,
-                            (cudaStream_t)stream);
+    if(n < kTwoPhaseMin)
+        return launch_propagate(p, env->env.view(), d_parents, d_draws, draw_stream, n, d_rows, d_valid, d_steps,
+                                (cudaStream_t)stream);
+    // two phases: the live list lives in the env's scratch, grown on demand
+    Env& e = env->env;
+    auto align = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t o_idx = 256, o_steps = o_idx + align(4ull * n), o_ctl = o_steps + align(4ull * n),
+                 o_state = o_ctl + align(16ull * n), bytes = o_state + align(4ull * p.sd * n);
+    if(bytes > e.live_cap) {
+        if(e.d_live) cudaFree(e.d_live), e.d_live = nullptr, e.live_cap = 0;
+        KPAX_CUDA(cudaMalloc(&e.d_live, bytes));
+        e.live_cap = bytes;
+    }
+    char* base = static_cast<char*>(e.d_live);
+    const LiveList live{reinterpret_cast<uint32_t*>(base), reinterpret_cast<uint32_t*>(base + o_idx),
+                        reinterpret_cast<int32_t*>(base + o_steps), reinterpret_cast<float*>(base + o_ctl),
+                        reinterpret_cast<float*>(base + o_state)};
+    cudaStream_t s = (cudaStream_t)stream;
+    KPAX_CUDA(cudaMemsetAsync(live.count, 0, sizeof(uint32_t), s));
+    const Grid g = e.view();
+    const uint32_t blocks = (n + 255) / 256;
+    switch(p.model) {
+        case KPAX_MODEL_DOUBLE_INTEGRATOR:
+            k_propagate_head<KPAX_MODEL_DOUBLE_INTEGRATOR><<<blocks, 256, 0, s>>>(p, g, d_parents, d_draws, draw_stream, n, d_rows, d_valid, d_steps, live);
+            k_propagate_tail<KPAX_MODEL_DOUBLE_INTEGRATOR><<<blocks, 256, 0, s>>>(p, g, d_rows, d_valid, d_steps, live);
+            break;
+        case KPAX_MODEL_DUBINS_AIRPLANE:
+            k_propagate_head<KPAX_MODEL_DUBINS_AIRPLANE><<<blocks, 256, 0, s>>>(p, g, d_parents, d_draws, draw_stream, n, d_rows, d_valid, d_steps, live);
+            k_propagate_tail<KPAX_MODEL_DUBINS_AIRPLANE><<<blocks, 256, 0, s>>>(p, g, d_rows, d_valid, d_steps, live);
+            break;
+        default:
+            k_propagate_head<KPAX_MODEL_QUADROTOR><<<blocks, 256, 0, s>>>(p, g, d_parents, d_draws, draw_stream, n, d_rows, d_valid, d_steps, live);
+            k_propagate_tail<KPAX_MODEL_QUADROTOR><<<blocks, 256, 0, s>>>(p, g, d_rows, d_valid, d_steps, live);
+            break;
+    }
+    KPAX_CHECK_LAUNCH();
+    count_launch(2);
+    return KPAX_OK;
 }
 
 kpax_status kpax_collide_batch(kpax_env* env, const float* d_bbmin, const float* d_bbmax, uint32_t n, uint8_t* d_free,

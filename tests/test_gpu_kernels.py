@@ -213,3 +213,37 @@ def test_sincos_within_a_few_ulp_of_cuda(cuda):
         err = np.abs(a - b)
         assert np.all(err <= np.maximum(4 * ulp, 2e-7)), float((err / np.maximum(ulp, 1e-45)).max())
     assert np.all(np.isnan(o[~fin, :2]))
+
+
+@pytest.mark.parametrize("name", list(PRESETS))
+def test_two_phase_large_batch_equals_one_pass(cuda, name):
+    """Batches of 2^18 segments or more run in two phases (the first steps of every segment, then
+    the live ones compacted); rows, verdicts and step counts equal the one-pass kernel's, which
+    smaller batches use: here the same draws propagated in slices of 2^17."""
+    import torch
+
+    cfg = kpax.preset(PRESETS[name])
+    obs, _, _ = SCENES[name]()
+    n = (1 << 18) + 123  # ragged: the last warp of the head is partly empty
+    S = cfg.sample_dim
+    par = E.sample_states(cfg.model, n, 91, cfg.v_min, cfg.v_max)
+    draws = np.ascontiguousarray(E.uniform_draws(n, 92)[:, :5])
+    d_obs = dev(torch, obs.astype(np.float32))
+    env = kpax.Env(cfg, d_obs.data_ptr(), obs.shape[0])
+    d_par, d_draw = dev(torch, par), dev(torch, draws)
+
+    def run(lo, hi, rows, valid, steps):
+        m = hi - lo
+        kpax.propagate_batch(cfg, env, d_par[lo:hi].data_ptr(), d_draw[lo:hi].data_ptr(), 0, m, rows[lo:hi].data_ptr(),
+                             valid[lo:hi].data_ptr(), steps[lo:hi].data_ptr())
+
+    out = [(torch.zeros((n, S), device="cuda"), torch.zeros(n, dtype=torch.uint8, device="cuda"),
+            torch.zeros(n, dtype=torch.int32, device="cuda")) for _ in range(2)]
+    run(0, n, *out[0])
+    for lo in range(0, n, 1 << 17):
+        run(lo, min(n, lo + (1 << 17)), *out[1])
+    torch.cuda.synchronize()
+    a, b = [[x.cpu().numpy() for x in o] for o in out]
+    assert np.array_equal(bits(a[0]), bits(b[0])), f"{name}: rows differ"
+    assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2]), f"{name}: verdicts or step counts differ"
+    assert 0 < a[1].mean() < 1
