@@ -45,6 +45,9 @@ METRIC = "valid expansions/s"
 UNIT = "expansions/s"
 # Algorithmic FP32 work per RK4 step (FMA = 2), counted from a CSE'd restatement of the models.
 FLOP_PER_STEP = {kpax.MODEL_DOUBLE_INTEGRATOR: 18, kpax.MODEL_DUBINS_AIRPLANE: 51, kpax.MODEL_QUADROTOR: 498}
+# dram__bytes_read.sum + dram__bytes_write.sum of one steady-state k_expand launch (2^16 children,
+# L2 flushed before the iteration) in an ncu capture of the default workload; none for the others
+EXPAND_DRAM_BYTES = {kpax.MODEL_QUADROTOR: 1535744 + 0}
 WORKLOADS = {
     "quad": (kpax.PRESET_QUAD, E.quad_scene, "12D quadrotor, building scene (1000 AABBs incl. windowed wall), "
              "2^16 expansions/iteration, 25 RK4 steps of 0.02 s"),
@@ -384,7 +387,10 @@ def run_ours(args) -> None:
     sm_mhz = peaks.get("sm_max_mhz", 1965.0)
     fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
     roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                "traffic": None, "kernel": "k_expand",
+                "traffic": EXPAND_DRAM_BYTES.get(cfg.model), "kernel": "k_expand",
+                "traffic_note": "DRAM bytes read + written by one steady-state 2^16-child k_expand launch of this "
+                                "workload in an ncu capture (profiles/k_expand_quad.md); the tree, regions and grid are "
+                                "L2-resident, so traffic is far below the bytes the kernel touches",
                 "peak_note": "nominal FP32: 148 SM x 128 lanes x 2 FLOP x clocks.max.sm (no measured FP32 peak in "
                              "MEASURED_PEAKS.json)",
                 "work": f"{tot_split['steps']} RK4 steps x {FLOP_PER_STEP[cfg.model]} FLOP over {args.steps} launches",
