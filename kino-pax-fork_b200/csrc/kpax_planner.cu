@@ -626,57 +626,67 @@ void* kpax_planner_stream(kpax_planner* pl) { return pl ? (void*)pl->b.stream : 
 kpax_status kpax_plan(kpax_planner* pl, const float* h_init, const float* h_goal, const float* d_obstacles, uint32_t n_obs,
                       int32_t save_tree, kpax_result* out)
 {
-    (void)save_tree;  // the tree always stays on the device; kpax_export_tree copies it out
-    if(!pl) return set_error("kpax_plan: null planner"), KPAX_EINVAL;
-    PlanBatch& b = pl->b;
-    kpax_status st = b.begin(h_init, h_goal, 0, &d_obstacles, &n_obs, b.cfg[0].max_iter, 1u);
-    if(st != KPAX_OK) return st;
-    st = b.run(plan_guard(b, b.cfg[0].max_iter));
-    kpax_status st2 = b.finish(out);
-    return st != KPAX_OK ? st : st2;
+    return no_throw("kpax_plan", [&]() -> kpax_status {
+        (void)save_tree;  // the tree always stays on the device; kpax_export_tree copies it out
+        if(!pl) return set_error("kpax_plan: null planner"), KPAX_EINVAL;
+        PlanBatch& b = pl->b;
+        kpax_status st = b.begin(h_init, h_goal, 0, &d_obstacles, &n_obs, b.cfg[0].max_iter, 1u);
+        if(st != KPAX_OK) return st;
+        st = b.run(plan_guard(b, b.cfg[0].max_iter));
+        kpax_status st2 = b.finish(out);
+        return st != KPAX_OK ? st : st2;
+    });
 }
 
 kpax_status kpax_plan_host(kpax_planner* pl, const float* h_init, const float* h_goal, const float* h_obstacles, uint32_t n_obs,
                            kpax_result* out)
 {
-    if(!pl || (n_obs && !h_obstacles)) return set_error("kpax_plan_host: null argument"), KPAX_EINVAL;
-    PlanBatch& b = pl->b;
-    if(n_obs > pl->obs_host_cap) {
-        if(pl->d_obs_host) cudaFree(pl->d_obs_host), pl->d_obs_host = nullptr;
-        KPAX_CUDA(cudaMalloc(&pl->d_obs_host, sizeof(float) * 6 * n_obs));
-        pl->obs_host_cap = n_obs;
-    }
-    KPAX_CUDA(cudaEventRecord(b.ev0, b.stream));
-    if(n_obs)
-        KPAX_CUDA(cudaMemcpyAsync(pl->d_obs_host, h_obstacles, sizeof(float) * 6 * n_obs, cudaMemcpyHostToDevice, b.stream));
-    const float* d = pl->d_obs_host;
-    kpax_status st = b.begin(h_init, h_goal, 0, &d, &n_obs, b.cfg[0].max_iter, 1u, false);
-    if(st != KPAX_OK) return st;
-    st = b.run(plan_guard(b, b.cfg[0].max_iter));
-    kpax_status st2 = b.finish(out);
-    return st != KPAX_OK ? st : st2;
+    return no_throw("kpax_plan_host", [&]() -> kpax_status {
+        if(!pl || (n_obs && !h_obstacles)) return set_error("kpax_plan_host: null argument"), KPAX_EINVAL;
+        PlanBatch& b = pl->b;
+        if(n_obs > pl->obs_host_cap) {
+            if(pl->d_obs_host) cudaFree(pl->d_obs_host), pl->d_obs_host = nullptr;
+            KPAX_CUDA(cudaMalloc(&pl->d_obs_host, sizeof(float) * 6 * n_obs));
+            pl->obs_host_cap = n_obs;
+        }
+        KPAX_CUDA(cudaEventRecord(b.ev0, b.stream));
+        if(n_obs)
+            KPAX_CUDA(cudaMemcpyAsync(pl->d_obs_host, h_obstacles, sizeof(float) * 6 * n_obs, cudaMemcpyHostToDevice, b.stream));
+        const float* d = pl->d_obs_host;
+        kpax_status st = b.begin(h_init, h_goal, 0, &d, &n_obs, b.cfg[0].max_iter, 1u, false);
+        if(st != KPAX_OK) return st;
+        st = b.run(plan_guard(b, b.cfg[0].max_iter));
+        kpax_status st2 = b.finish(out);
+        return st != KPAX_OK ? st : st2;
+    });
 }
 
 kpax_status kpax_plan_begin(kpax_planner* pl, const float* h_init, const float* h_goal, const float* d_obstacles, uint32_t n_obs)
 {
-    if(!pl) return set_error("kpax_plan_begin: null planner"), KPAX_EINVAL;
-    kpax_status st = pl->b.begin(h_init, h_goal, 0, &d_obstacles, &n_obs, 0u, 0u);
-    if(st != KPAX_OK) return st;
-    return pl->b.sync_ctl();
+    return no_throw("kpax_plan_begin", [&]() -> kpax_status {
+        if(!pl) return set_error("kpax_plan_begin: null planner"), KPAX_EINVAL;
+        kpax_status st = pl->b.begin(h_init, h_goal, 0, &d_obstacles, &n_obs, 0u, 0u);
+        if(st != KPAX_OK) return st;
+        return pl->b.sync_ctl();
+    });
 }
 
 kpax_status kpax_plan_iterate(kpax_planner* pl, uint32_t n_iters, int32_t stop_at_goal)
 {
-    if(!pl || !pl->b.begun) return set_error("kpax_plan_iterate: call kpax_plan_begin first"), KPAX_EINVAL;
-    if(!n_iters) return KPAX_OK;
-    return pl->b.iterate(n_iters, stop_at_goal ? 1u : 0u);
+    return no_throw("kpax_plan_iterate", [&]() -> kpax_status {
+        if(!pl || !pl->b.begun) return set_error("kpax_plan_iterate: call kpax_plan_begin first"), KPAX_EINVAL;
+        if(!n_iters) return KPAX_OK;
+        return pl->b.iterate(n_iters, stop_at_goal ? 1u : 0u);
+    });
 }
 
 kpax_status kpax_plan_iterate_timed(kpax_planner* pl, uint32_t n_iters, uint64_t flush_bytes, int32_t split,
                                     kpax_iter_timing* h_times, uint64_t* h_totals)
 {
-    if(!pl || !pl->b.begun) return set_error("kpax_plan_iterate_timed: call kpax_plan_begin first"), KPAX_EINVAL;
-    return pl->b.iterate_timed(n_iters, flush_bytes, split != 0, h_times, h_totals);
+    return no_throw("kpax_plan_iterate_timed", [&]() -> kpax_status {
+        if(!pl || !pl->b.begun) return set_error("kpax_plan_iterate_timed: call kpax_plan_begin first"), KPAX_EINVAL;
+        return pl->b.iterate_timed(n_iters, flush_bytes, split != 0, h_times, h_totals);
+    });
 }
 
 kpax_status kpax_write_rows_csv(const float* h_rows, uint32_t rows, uint32_t cols, const char* filename, int32_t append)
@@ -701,11 +711,13 @@ kpax_status kpax_write_rows_csv(const float* h_rows, uint32_t rows, uint32_t col
 
 kpax_status kpax_write_solution_csv(kpax_planner* pl, const char* filename, int32_t append)
 {
-    if(!pl || !pl->b.begun) return set_error("kpax_write_solution_csv: no plan"), KPAX_EINVAL;
-    kpax_result r{};
-    kpax_status st = pl->b.finish(&r);
-    if(st != KPAX_OK) return st;
-    return kpax_write_rows_csv(r.h_path, r.path_len, (uint32_t)pl->b.prm[0].S, filename, append);
+    return no_throw("kpax_write_solution_csv", [&]() -> kpax_status {
+        if(!pl || !pl->b.begun) return set_error("kpax_write_solution_csv: no plan"), KPAX_EINVAL;
+        kpax_result r{};
+        kpax_status st = pl->b.finish(&r);
+        if(st != KPAX_OK) return st;
+        return kpax_write_rows_csv(r.h_path, r.path_len, (uint32_t)pl->b.prm[0].S, filename, append);
+    });
 }
 
 }  // extern "C"
@@ -831,8 +843,10 @@ kpax_status kpax_plan_bench(kpax_planner* pl, const float* h_init, const float* 
 
 kpax_status kpax_plan_result(kpax_planner* pl, kpax_result* out)
 {
-    if(!pl || !pl->b.begun) return set_error("kpax_plan_result: no plan"), KPAX_EINVAL;
-    return pl->b.finish(out);
+    return no_throw("kpax_plan_result", [&]() -> kpax_status {
+        if(!pl || !pl->b.begun) return set_error("kpax_plan_result: no plan"), KPAX_EINVAL;
+        return pl->b.finish(out);
+    });
 }
 
 static kpax_status export_tree_body(kpax_planner* pl, float* h_rows, int32_t* h_parents, float* h_costs, uint32_t max_rows,
@@ -881,84 +895,94 @@ static kpax_status export_tree_body(kpax_planner* pl, float* h_rows, int32_t* h_
 
 kpax_status kpax_export_regions(kpax_planner* pl, int32_t* h_counter, int32_t* h_valid, float* h_scores, uint32_t* h_r2_bits)
 {
-    if(!pl) return set_error("kpax_export_regions: null planner"), KPAX_EINVAL;
-    PlanBatch& b = pl->b;
-    const KParams& p = b.prm[0];
-    const RegDev& rg = b.hq[0].rg;
-    if(h_counter) KPAX_CUDA(cudaMemcpyAsync(h_counter, rg.counter, sizeof(int32_t) * p.num_r1, cudaMemcpyDeviceToHost, b.stream));
-    if(h_valid) KPAX_CUDA(cudaMemcpyAsync(h_valid, rg.valid, sizeof(int32_t) * p.num_r1, cudaMemcpyDeviceToHost, b.stream));
-    if(h_scores) KPAX_CUDA(cudaMemcpyAsync(h_scores, rg.score, sizeof(float) * p.num_r1, cudaMemcpyDeviceToHost, b.stream));
-    if(h_r2_bits) KPAX_CUDA(cudaMemcpyAsync(h_r2_bits, rg.cur, sizeof(uint32_t) * p.r2_words, cudaMemcpyDeviceToHost, b.stream));
-    kpax_status st = b.sync_ctl();
-    if(st != KPAX_OK) return st;
-    if(h_scores) {  // stored raw (negative = no valid sample); normalised as region_score does
-        const float total = b.h_ctl[0].score_total;
-        const bool ready = b.h_ctl[0].scores_ready != 0u;
-        for(int r = 0; r < p.num_r1; ++r) {
-            const float raw = h_scores[r];
-            h_scores[r] = !ready ? 0.0f : (raw < 0.0f ? 1.0f : p.eps + raw / total);
+    return no_throw("kpax_export_regions", [&]() -> kpax_status {
+        if(!pl) return set_error("kpax_export_regions: null planner"), KPAX_EINVAL;
+        PlanBatch& b = pl->b;
+        const KParams& p = b.prm[0];
+        const RegDev& rg = b.hq[0].rg;
+        if(h_counter) KPAX_CUDA(cudaMemcpyAsync(h_counter, rg.counter, sizeof(int32_t) * p.num_r1, cudaMemcpyDeviceToHost, b.stream));
+        if(h_valid) KPAX_CUDA(cudaMemcpyAsync(h_valid, rg.valid, sizeof(int32_t) * p.num_r1, cudaMemcpyDeviceToHost, b.stream));
+        if(h_scores) KPAX_CUDA(cudaMemcpyAsync(h_scores, rg.score, sizeof(float) * p.num_r1, cudaMemcpyDeviceToHost, b.stream));
+        if(h_r2_bits) KPAX_CUDA(cudaMemcpyAsync(h_r2_bits, rg.cur, sizeof(uint32_t) * p.r2_words, cudaMemcpyDeviceToHost, b.stream));
+        kpax_status st = b.sync_ctl();
+        if(st != KPAX_OK) return st;
+        if(h_scores) {  // stored raw (negative = no valid sample); normalised as region_score does
+            const float total = b.h_ctl[0].score_total;
+            const bool ready = b.h_ctl[0].scores_ready != 0u;
+            for(int r = 0; r < p.num_r1; ++r) {
+                const float raw = h_scores[r];
+                h_scores[r] = !ready ? 0.0f : (raw < 0.0f ? 1.0f : p.eps + raw / total);
+            }
         }
-    }
-    return KPAX_OK;
+        return KPAX_OK;
+    });
 }
 
 kpax_status kpax_export_frontier(kpax_planner* pl, uint8_t* h_repeat, int32_t* h_r1, uint32_t max_rows)
 {
-    if(!pl) return set_error("kpax_export_frontier: null planner"), KPAX_EINVAL;
-    PlanBatch& b = pl->b;
-    kpax_status st = b.sync_ctl();
-    if(st != KPAX_OK) return st;
-    const uint32_t n = std::min(b.h_ctl[0].tree, max_rows);
-    if(b.h_ctl[0].tree_old) {
-        k_reactivate<<<(b.h_ctl[0].tree_old + 255) / 256, 256, 0, b.stream>>>(b.dq);
-        KPAX_CHECK_LAUNCH();
-        count_launch();
-    }
-    if(n && h_repeat) KPAX_CUDA(cudaMemcpyAsync(h_repeat, b.hq[0].t.rep, n, cudaMemcpyDeviceToHost, b.stream));
-    if(n && h_r1) KPAX_CUDA(cudaMemcpyAsync(h_r1, b.hq[0].t.r1, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, b.stream));
-    KPAX_CUDA(cudaStreamSynchronize(b.stream));
-    return KPAX_OK;
+    return no_throw("kpax_export_frontier", [&]() -> kpax_status {
+        if(!pl) return set_error("kpax_export_frontier: null planner"), KPAX_EINVAL;
+        PlanBatch& b = pl->b;
+        kpax_status st = b.sync_ctl();
+        if(st != KPAX_OK) return st;
+        const uint32_t n = std::min(b.h_ctl[0].tree, max_rows);
+        if(b.h_ctl[0].tree_old) {
+            k_reactivate<<<(b.h_ctl[0].tree_old + 255) / 256, 256, 0, b.stream>>>(b.dq);
+            KPAX_CHECK_LAUNCH();
+            count_launch();
+        }
+        if(n && h_repeat) KPAX_CUDA(cudaMemcpyAsync(h_repeat, b.hq[0].t.rep, n, cudaMemcpyDeviceToHost, b.stream));
+        if(n && h_r1) KPAX_CUDA(cudaMemcpyAsync(h_r1, b.hq[0].t.r1, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, b.stream));
+        KPAX_CUDA(cudaStreamSynchronize(b.stream));
+        return KPAX_OK;
+    });
 }
 
 kpax_status kpax_debug_capture(kpax_planner* pl, int32_t enable)
 {
-    if(!pl) return set_error("kpax_debug_capture: null planner"), KPAX_EINVAL;
-    return pl->b.set_capture(enable != 0);
+    return no_throw("kpax_debug_capture", [&]() -> kpax_status {
+        if(!pl) return set_error("kpax_debug_capture: null planner"), KPAX_EINVAL;
+        return pl->b.set_capture(enable != 0);
+    });
 }
 
 kpax_status kpax_export_children(kpax_planner* pl, float* h_rows, uint8_t* h_valid, int32_t* h_r1, int32_t* h_r2,
                                  uint8_t* h_next, int32_t* h_parent, uint32_t max_rows, uint32_t* n_children)
 {
-    if(!pl || !pl->b.capture_on) return set_error("kpax_export_children: capture is off"), KPAX_EINVAL;
-    PlanBatch& b = pl->b;
-    kpax_status st = b.sync_ctl();
-    if(st != KPAX_OK) return st;
-    const uint32_t n = std::min(b.h_ctl[0].n, max_rows);
-    if(n_children) *n_children = n;
-    if(!n) return KPAX_OK;
-    const CaptureDev& c = b.cap;
-    if(h_rows) KPAX_CUDA(cudaMemcpyAsync(h_rows, c.rows, sizeof(float) * n * b.prm[0].S, cudaMemcpyDeviceToHost, b.stream));
-    if(h_valid) KPAX_CUDA(cudaMemcpyAsync(h_valid, c.valid, n, cudaMemcpyDeviceToHost, b.stream));
-    if(h_r1) KPAX_CUDA(cudaMemcpyAsync(h_r1, c.r1, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, b.stream));
-    if(h_r2) KPAX_CUDA(cudaMemcpyAsync(h_r2, c.r2, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, b.stream));
-    if(h_next) KPAX_CUDA(cudaMemcpyAsync(h_next, c.next, n, cudaMemcpyDeviceToHost, b.stream));
-    if(h_parent) KPAX_CUDA(cudaMemcpyAsync(h_parent, c.parent, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, b.stream));
-    KPAX_CUDA(cudaStreamSynchronize(b.stream));
-    return KPAX_OK;
+    return no_throw("kpax_export_children", [&]() -> kpax_status {
+        if(!pl || !pl->b.capture_on) return set_error("kpax_export_children: capture is off"), KPAX_EINVAL;
+        PlanBatch& b = pl->b;
+        kpax_status st = b.sync_ctl();
+        if(st != KPAX_OK) return st;
+        const uint32_t n = std::min(b.h_ctl[0].n, max_rows);
+        if(n_children) *n_children = n;
+        if(!n) return KPAX_OK;
+        const CaptureDev& c = b.cap;
+        if(h_rows) KPAX_CUDA(cudaMemcpyAsync(h_rows, c.rows, sizeof(float) * n * b.prm[0].S, cudaMemcpyDeviceToHost, b.stream));
+        if(h_valid) KPAX_CUDA(cudaMemcpyAsync(h_valid, c.valid, n, cudaMemcpyDeviceToHost, b.stream));
+        if(h_r1) KPAX_CUDA(cudaMemcpyAsync(h_r1, c.r1, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, b.stream));
+        if(h_r2) KPAX_CUDA(cudaMemcpyAsync(h_r2, c.r2, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, b.stream));
+        if(h_next) KPAX_CUDA(cudaMemcpyAsync(h_next, c.next, n, cudaMemcpyDeviceToHost, b.stream));
+        if(h_parent) KPAX_CUDA(cudaMemcpyAsync(h_parent, c.parent, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, b.stream));
+        KPAX_CUDA(cudaStreamSynchronize(b.stream));
+        return KPAX_OK;
+    });
 }
 
 kpax_status kpax_export_proposal(kpax_planner* pl, float* h_mix, uint32_t max_entries, uint32_t* n_entries)
 {
-    if(!pl || !pl->b.hq[0].mix) return set_error("kpax_export_proposal: the learned proposal is off"), KPAX_EINVAL;
-    PlanBatch& b = pl->b;
-    kpax_status st = b.sync_ctl();
-    if(st != KPAX_OK) return st;
-    const uint32_t n = std::min(b.h_ctl[0].E, max_entries);
-    if(n_entries) *n_entries = n;
-    if(n && h_mix)
-        KPAX_CUDA(cudaMemcpyAsync(h_mix, b.hq[0].mix, sizeof(float) * n * mlp::kMixFloats, cudaMemcpyDeviceToHost, b.stream));
-    KPAX_CUDA(cudaStreamSynchronize(b.stream));
-    return KPAX_OK;
+    return no_throw("kpax_export_proposal", [&]() -> kpax_status {
+        if(!pl || !pl->b.hq[0].mix) return set_error("kpax_export_proposal: the learned proposal is off"), KPAX_EINVAL;
+        PlanBatch& b = pl->b;
+        kpax_status st = b.sync_ctl();
+        if(st != KPAX_OK) return st;
+        const uint32_t n = std::min(b.h_ctl[0].E, max_entries);
+        if(n_entries) *n_entries = n;
+        if(n && h_mix)
+            KPAX_CUDA(cudaMemcpyAsync(h_mix, b.hq[0].mix, sizeof(float) * n * mlp::kMixFloats, cudaMemcpyDeviceToHost, b.stream));
+        KPAX_CUDA(cudaStreamSynchronize(b.stream));
+        return KPAX_OK;
+    });
 }
 
 // ---------------------------------------------------------------- batches of queries
@@ -989,49 +1013,55 @@ kpax_status kpax_batch_destroy(kpax_batch* b)
 
 kpax_status kpax_set_proposal(kpax_planner* pl, kpax_mlp* net, float epsilon)
 {
-    if(!pl) return set_error("kpax_set_proposal: null planner"), KPAX_EINVAL;
-    if(net && pl->b.prm[0].model != KPAX_MODEL_QUADROTOR)
-        return set_error("kpax_set_proposal: the proposal network is defined for the quadrotor"), KPAX_EINVAL;
-    return pl->b.set_proposal(net, epsilon, nullptr);
+    return no_throw("kpax_set_proposal", [&]() -> kpax_status {
+        if(!pl) return set_error("kpax_set_proposal: null planner"), KPAX_EINVAL;
+        if(net && pl->b.prm[0].model != KPAX_MODEL_QUADROTOR)
+            return set_error("kpax_set_proposal: the proposal network is defined for the quadrotor"), KPAX_EINVAL;
+        return pl->b.set_proposal(net, epsilon, nullptr);
+    });
 }
 
 kpax_status kpax_batch_set_proposal(kpax_batch* bt, kpax_mlp* net, float epsilon, const uint8_t* enable)
 {
-    if(!bt) return set_error("kpax_batch_set_proposal: null batch"), KPAX_EINVAL;
-    return bt->b.set_proposal(net, epsilon, enable);
+    return no_throw("kpax_batch_set_proposal", [&]() -> kpax_status {
+        if(!bt) return set_error("kpax_batch_set_proposal: null batch"), KPAX_EINVAL;
+        return bt->b.set_proposal(net, epsilon, enable);
+    });
 }
 
 kpax_status kpax_batch_plan(kpax_batch* bt, const float* h_inits, const float* h_goals, uint32_t row_stride,
                             const float* const* d_obstacles, const uint32_t* n_obs, kpax_result* results,
                             kpax_batch_stats* stats)
 {
-    if(!bt || !d_obstacles || !n_obs) return set_error("kpax_batch_plan: null argument"), KPAX_EINVAL;
-    PlanBatch& b = bt->b;
-    if(row_stride < b.s_max) return set_error("kpax_batch_plan: row_stride %u < %u", row_stride, b.s_max), KPAX_EINVAL;
-    uint32_t max_iter = 0;
-    for(const kpax_config& c : b.cfg) max_iter = std::max(max_iter, c.max_iter);
-    kpax_status st = b.begin(h_inits, h_goals, row_stride, d_obstacles, n_obs, max_iter, 1u);
-    if(st != KPAX_OK) return st;
-    // each query stops at its own max_iter
-    if((st = b.sync_ctl()) != KPAX_OK) return st;
-    for(uint32_t q = 0; q < b.nq; ++q) b.h_ctl[q].max_iters = b.cfg[q].max_iter;
-    if((st = b.write_ctl()) != KPAX_OK) return st;
-    st = b.run(plan_guard(b, max_iter));
-    double ms = 0.0;
-    kpax_status st2 = b.finish(results, &ms);
-    if(stats) {
-        memset(stats, 0, sizeof(*stats));
-        stats->ms = ms;
-        for(uint32_t q = 0; q < b.nq; ++q) {
-            const Ctl& c = b.h_ctl[q];
-            stats->iters = std::max(stats->iters, c.iters_done);
-            stats->found += c.goal_idx != kNone;
-            stats->expansions += c.n_exp;
-            stats->valid_expansions += c.n_valid;
-            stats->steps += c.n_steps;
+    return no_throw("kpax_batch_plan", [&]() -> kpax_status {
+        if(!bt || !d_obstacles || !n_obs) return set_error("kpax_batch_plan: null argument"), KPAX_EINVAL;
+        PlanBatch& b = bt->b;
+        if(row_stride < b.s_max) return set_error("kpax_batch_plan: row_stride %u < %u", row_stride, b.s_max), KPAX_EINVAL;
+        uint32_t max_iter = 0;
+        for(const kpax_config& c : b.cfg) max_iter = std::max(max_iter, c.max_iter);
+        kpax_status st = b.begin(h_inits, h_goals, row_stride, d_obstacles, n_obs, max_iter, 1u);
+        if(st != KPAX_OK) return st;
+        // each query stops at its own max_iter
+        if((st = b.sync_ctl()) != KPAX_OK) return st;
+        for(uint32_t q = 0; q < b.nq; ++q) b.h_ctl[q].max_iters = b.cfg[q].max_iter;
+        if((st = b.write_ctl()) != KPAX_OK) return st;
+        st = b.run(plan_guard(b, max_iter));
+        double ms = 0.0;
+        kpax_status st2 = b.finish(results, &ms);
+        if(stats) {
+            memset(stats, 0, sizeof(*stats));
+            stats->ms = ms;
+            for(uint32_t q = 0; q < b.nq; ++q) {
+                const Ctl& c = b.h_ctl[q];
+                stats->iters = std::max(stats->iters, c.iters_done);
+                stats->found += c.goal_idx != kNone;
+                stats->expansions += c.n_exp;
+                stats->valid_expansions += c.n_valid;
+                stats->steps += c.n_steps;
+            }
         }
-    }
-    return st != KPAX_OK ? st : st2;
+        return st != KPAX_OK ? st : st2;
+    });
 }
 
 }  // extern "C"
