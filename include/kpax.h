@@ -290,7 +290,7 @@ kpax_status kpax_rekino_plan(kpax_rekino* planner, const float* h_init, const fl
 kpax_status kpax_write_rows_csv(const float* h_rows, uint32_t rows, uint32_t cols,
                                 const char* filename, int32_t append);
 /* The last plan's solution (KPAX.cu:621-627, controlPathToGoal.csv): SAMPLE_DIM columns, the goal
- * node first and the root last (every row; the reference writes h_itr_ rows, Q12).  No file
+ * node first and the root last (every row; the reference copies h_itr_ rows, which can drop the root).  No file
  * content is written when no path was found (an empty file unless appending). */
 kpax_status kpax_write_solution_csv(kpax_planner* planner, const char* filename, int32_t append);
 /* planBench (KPAX.cu:243-300) with the reference's per-iteration dumps (writeDeviceVectorsToCSV,

@@ -188,7 +188,8 @@ __device__ __forceinline__ int region_r1(const KParams& p, const float* s)
 // C_MIN + i*C_R1_SIZE (double, tabulated) and V_MIN + i*V_R1_SIZE (float), as Graph.cu:69-95.
 // The R1 id's cell digits are decoded as they are consumed, least significant first.  In compat
 // mode the id is decoded the way initializeRegions_kernel lays out its table (Graph.cu:58-96:
-// workspace part fastest, C_R1^2 attitude cells, then velocity); otherwise in getRegion's order (Q5).
+// workspace part fastest, C_R1^2 attitude cells, then velocity); otherwise in getRegion's order
+// (workspace part slowest).
 template <int SD>
 __device__ __forceinline__ int region_r2(const KParams& p, const float* s, int r1)
 {
@@ -332,7 +333,7 @@ __device__ __forceinline__ StepParams step_params(const KParams& p)
     return {p.h, p.hh, p.h6, p.vmin, p.vmax, p.ws_lo, p.ws_hi, p.pitch_lo, p.pitch_hi};
 }
 
-// Double integrator, statePropagatorSpatialHash.cu:72-134 (Q1: x += h(5v + 2ah)/6).  The terms
+// Double integrator, statePropagatorSpatialHash.cu:72-134 (x += h(5v + 2ah)/6, not textbook RK4).  The terms
 // that depend on the segment's acceleration only (a*h/2, a*h and the velocity increment
 // (a + 2a + 2a + a)*h/6) are computed once per segment, with the same rounded operations.
 struct DIConsts {

@@ -1,12 +1,14 @@
 // kpax_env.cu — obstacle grid build and the kernel-level batch entry points.
 //
 // The reference keeps a fixed 16-slot list per 5 m cell and rebuilds it with atomics every
-// iteration (spatialHash.cu:9-67, KPAX.cu:306), silently dropping entries past 16 (Q2).  Here
+// iteration (spatialHash.cu:9-67, KPAX.cu:306), silently dropping entries past 16 in nondeterministic order.  Here
 // the grid is compressed sparse rows (count -> scan -> fill), holds every (cell, obstacle)
 // pair and is built once per plan.  Query verdicts equal the brute-force isMotionValid
 // (collisionCheck.cu:49-62) for every box: the cell map is monotone, so any strictly
 // overlapping obstacle shares at least one cell with the box.
 #include <stdio.h>
+#include <limits.h>
+#include <algorithm>
 #include <string.h>
 
 #include <mutex>
@@ -167,13 +169,18 @@ __global__ void __launch_bounds__(256, 4) k_propagate_batch(KParams p, Grid g, c
     if(steps_out) steps_out[i] = done;
 }
 
-// Large batches run in two phases so that lanes do not idle behind their warp's longest segment:
-// the head runs every segment for its first kHeadSteps steps and finishes the segments that end
-// there (a fifth of them fail in their first steps); the others are appended, state and controls,
-// to a compact list that the tail carries to the end with full warps.  Both phases run the same
-// per-step code in the same order, so rows, verdicts and step counts equal the one-pass kernel's.
+// Large batches run in phases so that lanes do not idle behind their warp's longest segment: the
+// head runs every segment for its first kHeadSteps steps and finishes the segments that end there
+// (a fifth of them fail in their first steps); the others are appended, state and controls, to a
+// compact list.  A middle phase carries that list to 3/5 of the longest segment (mid_steps),
+// finishes the segments that end by then and appends the rest to a second list, which the tail
+// carries to the end, each with full warps.  Every phase runs the same per-step code in the same
+// order, so rows, verdicts and step counts equal the one-pass kernel's.  Dubins microbench, 2^22
+// segments of 20 steps: 2.15 G valid segments/s in two phases; 2.15 / 2.18 / 2.19 G/s with the
+// middle phase ending after step 6 / 8 / 12.
 constexpr int kHeadSteps = 2;
-constexpr uint32_t kTwoPhaseMin = 1u << 18;  // segments; below this the one-pass kernel is used
+inline int mid_steps(const KParams& p) { return std::max(kHeadSteps + 1, (p.nsteps + 1) * 3 / 5); }
+constexpr uint32_t kPhasedMin = 1u << 18;   // segments; below this the one-pass kernel is used
 
 struct LiveList {
     uint32_t* count;
@@ -199,6 +206,28 @@ __device__ __forceinline__ void write_segment(const KParams& p, uint32_t i, cons
     dst[SD + CD] = __fmul_rn(p.h, (float)steps);
     valid[i] = ok ? 1 : 0;
     if(steps_out) steps_out[i] = done;
+}
+
+// Appends the warp's live segments to `live` (one atomic per warp); called by all 32 lanes.
+template <int SD>
+__device__ __forceinline__ void append_live(const LiveList& live, bool alive, int lane, uint32_t i, int steps, const float* c,
+                                            const float* s)
+{
+    const uint32_t m = __ballot_sync(0xffffffffu, alive);
+    if(!m) return;
+    const int leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if(lane == leader) base = atomicAdd(live.count, (uint32_t)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if(alive) {
+        const uint32_t j = base + __popc(m & ((1u << lane) - 1u));
+        live.idx[j] = i;
+        live.steps[j] = steps;
+#pragma unroll
+        for(int k = 0; k < 4; ++k) live.ctl[(size_t)j * 4 + k] = c[k];
+#pragma unroll
+        for(int k = 0; k < SD; ++k) live.state[(size_t)j * SD + k] = s[k];
+    }
 }
 
 template <int M>
@@ -237,50 +266,54 @@ __global__ void __launch_bounds__(256, 4) k_propagate_head(KParams p, Grid g, co
         alive = ok && done < steps;
         if(!alive) write_segment<M>(p, i, s, c, steps, ok, done, rows, valid, steps_out);
     }
-    // append the live segments, one atomic per warp
-    const uint32_t m = __ballot_sync(0xffffffffu, alive);
-    if(m) {
-        const int leader = __ffs(m) - 1;
-        uint32_t base = 0;
-        if(lane == leader) base = atomicAdd(live.count, (uint32_t)__popc(m));
-        base = __shfl_sync(0xffffffffu, base, leader);
-        if(alive) {
-            const uint32_t j = base + __popc(m & ((1u << lane) - 1u));
-            live.idx[j] = i;
-            live.steps[j] = steps;
-#pragma unroll
-            for(int k = 0; k < 4; ++k) live.ctl[(size_t)j * 4 + k] = c[k];
-#pragma unroll
-            for(int k = 0; k < SD; ++k) live.state[(size_t)j * SD + k] = s[k];
-        }
-    }
+    append_live<SD>(live, alive, lane, i, steps, c, s);
 }
 
 template <int M>
 __global__ void __launch_bounds__(256, 4) k_propagate_tail(KParams p, Grid g, float* __restrict__ rows,
                                                         uint8_t* __restrict__ valid, int32_t* __restrict__ steps_out,
-                                                        LiveList live)
+                                                        LiveList live, int from, int until, LiveList next)
 {
     constexpr int SD = ModelDims<M>::SD;
+    const uint32_t count = *live.count;
+    if(blockIdx.x * blockDim.x >= count) return;  // whole block past the list: the ballot below needs full warps
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if(j >= *live.count) return;
-    const uint32_t i = live.idx[j];
-    const int steps = live.steps[j];
+    const int lane = threadIdx.x & 31;
+    bool alive = false;
+    uint32_t i = 0;
+    int steps = 0;
     float s[SD], c[4];
+    if(j < count) {
+        i = live.idx[j];
+        steps = live.steps[j];
 #pragma unroll
-    for(int k = 0; k < 4; ++k) c[k] = live.ctl[(size_t)j * 4 + k];
+        for(int k = 0; k < 4; ++k) c[k] = live.ctl[(size_t)j * 4 + k];
 #pragma unroll
-    for(int k = 0; k < SD; ++k) s[k] = live.state[(size_t)j * SD + k];
-    const auto kc = segment_consts<M>(p, c);
-    const StepParams sp = step_params(p);
-    bool ok = true;
-    int done = kHeadSteps;
-    while(done < steps) {
-        ok = model_step<M>(sp, g, s, c, kc);
-        ++done;
-        if(!ok) break;
+        for(int k = 0; k < SD; ++k) s[k] = live.state[(size_t)j * SD + k];
+        const auto kc = segment_consts<M>(p, c);
+        const StepParams sp = step_params(p);
+        bool ok = true;
+        int done = from;
+        while(done < steps && done < until) {
+            ok = model_step<M>(sp, g, s, c, kc);
+            ++done;
+            if(!ok) break;
+        }
+        alive = next.count && ok && done < steps;
+        if(!alive) write_segment<M>(p, i, s, c, steps, ok, done, rows, valid, steps_out);
     }
-    write_segment<M>(p, i, s, c, steps, ok, done, rows, valid, steps_out);
+    if(next.count) append_live<SD>(next, alive, lane, i, steps, c, s);
+}
+
+template <int M>
+void launch_phases(const KParams& p, const Grid& g, const float* parents, const float* draws, uint32_t stream_id, uint32_t n,
+                   float* rows, uint8_t* valid, int32_t* steps_out, const LiveList& first, const LiveList& second,
+                   const LiveList& none, uint32_t blocks, cudaStream_t s)
+{
+    k_propagate_head<M><<<blocks, 256, 0, s>>>(p, g, parents, draws, stream_id, n, rows, valid, steps_out, first);
+    const int mid = mid_steps(p);
+    k_propagate_tail<M><<<blocks, 256, 0, s>>>(p, g, rows, valid, steps_out, first, kHeadSteps, mid, second);
+    k_propagate_tail<M><<<blocks, 256, 0, s>>>(p, g, rows, valid, steps_out, second, mid, INT_MAX, none);
 }
 
 __global__ void k_collide_batch(Grid g, const float* __restrict__ bbmin, const float* __restrict__ bbmax, uint32_t n,
@@ -470,43 +503,48 @@ kpax_status kpax_propagate_batch(const kpax_config* cfg, kpax_env* env, const fl
     if(st != KPAX_OK) return st;
     if(p.gdim != env->env.dim || p.cell != env->env.cell || p.wmin != env->env.wmin)
         return set_error("kpax_propagate_batch: env was built for another workspace grid"), KPAX_EINVAL;
-    if(n < kTwoPhaseMin)
+    if(n < kPhasedMin)
         return launch_propagate(p, env->env.view(), d_parents, d_draws, draw_stream, n, d_rows, d_valid, d_steps,
                                 (cudaStream_t)stream);
-    // two phases: the live list lives in the env's scratch, grown on demand
+    // phases: the two live lists live in the env's scratch, grown on demand (counts at bytes 0 and
+    // 128, then each list's index, step-count, control and state arrays)
     Env& e = env->env;
     auto align = [](size_t b) { return (b + 255) / 256 * 256; };
-    const size_t o_idx = 256, o_steps = o_idx + align(4ull * n), o_ctl = o_steps + align(4ull * n),
-                 o_state = o_ctl + align(16ull * n), bytes = o_state + align(4ull * p.sd * n);
+    const size_t l_idx = 0, l_steps = align(4ull * n), l_ctl = l_steps + align(4ull * n), l_state = l_ctl + align(16ull * n),
+                 l_bytes = l_state + align(4ull * p.sd * n), bytes = 256 + 2 * l_bytes;
     if(bytes > e.live_cap) {
         if(e.d_live) cudaFree(e.d_live), e.d_live = nullptr, e.live_cap = 0;
         KPAX_CUDA(cudaMalloc(&e.d_live, bytes));
         e.live_cap = bytes;
     }
     char* base = static_cast<char*>(e.d_live);
-    const LiveList live{reinterpret_cast<uint32_t*>(base), reinterpret_cast<uint32_t*>(base + o_idx),
-                        reinterpret_cast<int32_t*>(base + o_steps), reinterpret_cast<float*>(base + o_ctl),
-                        reinterpret_cast<float*>(base + o_state)};
+    auto list = [&](int k) {
+        char* l = base + 256 + (size_t)k * l_bytes;
+        return LiveList{reinterpret_cast<uint32_t*>(base + 128 * k), reinterpret_cast<uint32_t*>(l + l_idx),
+                        reinterpret_cast<int32_t*>(l + l_steps), reinterpret_cast<float*>(l + l_ctl),
+                        reinterpret_cast<float*>(l + l_state)};
+    };
+    const LiveList first = list(0), second = list(1), none{};
     cudaStream_t s = (cudaStream_t)stream;
-    KPAX_CUDA(cudaMemsetAsync(live.count, 0, sizeof(uint32_t), s));
+    KPAX_CUDA(cudaMemsetAsync(base, 0, 256, s));
     const Grid g = e.view();
     const uint32_t blocks = (n + 255) / 256;
     switch(p.model) {
         case KPAX_MODEL_DOUBLE_INTEGRATOR:
-            k_propagate_head<KPAX_MODEL_DOUBLE_INTEGRATOR><<<blocks, 256, 0, s>>>(p, g, d_parents, d_draws, draw_stream, n, d_rows, d_valid, d_steps, live);
-            k_propagate_tail<KPAX_MODEL_DOUBLE_INTEGRATOR><<<blocks, 256, 0, s>>>(p, g, d_rows, d_valid, d_steps, live);
+            launch_phases<KPAX_MODEL_DOUBLE_INTEGRATOR>(p, g, d_parents, d_draws, draw_stream, n, d_rows, d_valid, d_steps, first,
+                                                       second, none, blocks, s);
             break;
         case KPAX_MODEL_DUBINS_AIRPLANE:
-            k_propagate_head<KPAX_MODEL_DUBINS_AIRPLANE><<<blocks, 256, 0, s>>>(p, g, d_parents, d_draws, draw_stream, n, d_rows, d_valid, d_steps, live);
-            k_propagate_tail<KPAX_MODEL_DUBINS_AIRPLANE><<<blocks, 256, 0, s>>>(p, g, d_rows, d_valid, d_steps, live);
+            launch_phases<KPAX_MODEL_DUBINS_AIRPLANE>(p, g, d_parents, d_draws, draw_stream, n, d_rows, d_valid, d_steps, first,
+                                                     second, none, blocks, s);
             break;
         default:
-            k_propagate_head<KPAX_MODEL_QUADROTOR><<<blocks, 256, 0, s>>>(p, g, d_parents, d_draws, draw_stream, n, d_rows, d_valid, d_steps, live);
-            k_propagate_tail<KPAX_MODEL_QUADROTOR><<<blocks, 256, 0, s>>>(p, g, d_rows, d_valid, d_steps, live);
+            launch_phases<KPAX_MODEL_QUADROTOR>(p, g, d_parents, d_draws, draw_stream, n, d_rows, d_valid, d_steps, first, second,
+                                               none, blocks, s);
             break;
     }
     KPAX_CHECK_LAUNCH();
-    count_launch(2);
+    count_launch(3);
     return KPAX_OK;
 }
 

@@ -57,7 +57,7 @@ struct Env {
     uint32_t* h_total = nullptr;  // pinned
     uint32_t obs_cap = 0, ent_cap = 0;
     bool owned_by_planner = false;
-    void* d_live = nullptr;  // scratch of the two-phase segment batch (grown on demand)
+    void* d_live = nullptr;  // scratch of the phased segment batch (grown on demand)
     size_t live_cap = 0;
 
     Grid view() const { return Grid{d_obs, d_off, d_ent, wmin, 1.0f / cell, dim}; }

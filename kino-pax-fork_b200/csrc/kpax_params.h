@@ -29,7 +29,7 @@ struct KParams {
     float cthr1[kMaxThr];   // attitude R1 index = #{k : c >= cthr1[k]}
     float cthr2[kMaxThr];   // attitude R2 index = #{k : C2*(c - m) >= cthr2[k]}
     int r1_mulW, r1_mulA, r2_mulW, r2_mulA, P, num_r1;
-    int compat;             // R1 min corners decoded as initializeRegions_kernel does (Q5)
+    int compat;             // R1 min corners decoded as initializeRegions_kernel does (w fastest)
     float cmin_tab[kMaxThr + 1];  // (float)(C_MIN + i * C_R1_SIZE), evaluated in double
     uint32_t r2_words;      // ceil(num_r1 * P / 32)
     // spatial hash (spatialHash.cuh:9-13)

@@ -240,7 +240,7 @@ float ko_separation(const float* obs, uint32_t n, const float bmin[3], const flo
 int ko_controls(const kpax_config* cfg, const float* u, float* ctrl_row, int32_t* steps)
 {
     int N = cfg->max_propagation_duration;
-    /* statePropagatorSpatialHash.cu:77 — 1 + (int)(u * N); u == 1 gives N + 1 (Q3) */
+    /* statePropagatorSpatialHash.cu:77 — 1 + (int)(u * N); u == 1 gives N + 1 */
     if(steps) *steps = cfg->fixed_steps ? N : 1 + f2i(u[4] * (float)N);
     float c[4] = {0, 0, 0, 0};
     for(int i = 0; i < cfg->control_dim; ++i) {
@@ -295,7 +295,7 @@ static int fail(seg_ctx* s, int kind)
     return 0;
 }
 
-/* Double integrator, statePropagatorSpatialHash.cu:72-134 (update Q1: x += h(5v + 2ah)/6). */
+/* Double integrator, statePropagatorSpatialHash.cu:72-134 (the reference's update x += h(5v + 2ah)/6, not textbook RK4). */
 static int prop_di(seg_ctx* s, const float* x0, const float* c, int steps, float* x1, int* done)
 {
     const float h = s->cfg->step_size, vmin = s->cfg->v_min, vmax = s->cfg->v_max, W = s->cfg->w_size;
@@ -543,7 +543,7 @@ void ko_integrate_f64(const kpax_config* cfg, const double* x0, const float* ctr
 int ko_table_cols(const kpax_config* cfg) { return 3 + cfg->c_dim + cfg->v_dim; }
 
 /* R1 min-corner table.  region_compat = 1 restates initializeRegions_kernel (Graph.cu:53-97),
- * whose id decomposition (w fastest, C_R1^2 attitude cells) differs from getRegion's (Q5). */
+ * whose id decomposition (w fastest, C_R1^2 attitude cells) differs from getRegion's (w slowest). */
 void ko_region_table(const kpax_config* cfg, float* table)
 {
     uint32_t n1, P;

@@ -14,11 +14,16 @@
  * Semantics that the reference leaves undefined are fixed here and followed by the CUDA path:
  *  - random numbers: Philox4x32-10 (Salmon et al., SC'11), u = ((x >> 8) + 1) * 2^-24 in (0,1];
  *  - float->int conversion saturates and maps NaN to 0 (the reference's device behaviour);
- *  - a state with a non-finite component after a step ends the segment as invalid (Q4);
- *  - R2 "first visit" tests read a snapshot taken at the start of the iteration (Q9);
- *  - the goal node is the lowest tree index that reached the goal ball (Q10);
- *  - children per iteration are clamped to the budget and to the free tree capacity (Q11);
- *  - region scores use a fixed-order float sum (Q6-Q8 make the reference's sum undefined).
+ *  - a state with a non-finite component after a step ends the segment as invalid (the
+ *    reference's NaN comparisons let it pass);
+ *  - R2 "first visit" tests read a snapshot taken at the start of the iteration (the
+ *    reference's read-then-exchange is racy);
+ *  - the goal node is the lowest tree index that reached the goal ball (the reference's
+ *    concurrent path writes race);
+ *  - children per iteration are clamped to the budget and to the free tree capacity (the reference
+ *    can write past MAX_TREE_SIZE);
+ *  - region scores use a fixed-order float sum (the reference's block reductions are
+ *    mis-sized and its total is never reset, so its sum is undefined).
  */
 #ifndef KPAX_ORACLE_H_
 #define KPAX_ORACLE_H_
@@ -71,7 +76,7 @@ void ko_propagate_batch(const kpax_config* cfg, const ko_env* env, const float* 
                         uint8_t* valid, int32_t* steps, ko_seg_diag* diag, int nthreads);
 /* FP64 integration of the same segment for error reports.  mode 0: the model's discrete
  * update exactly as written, in double; mode 1: classical RK4 of the continuous ODE (for the
- * double integrator this differs from the reference's update, Q1).  Integrates `steps` steps
+ * double integrator this differs from the reference's update x += h(5v + 2ah)/6).  Integrates `steps` steps
  * with no checks; writes state_dim doubles. */
 void ko_integrate_f64(const kpax_config* cfg, const double* x0, const float* ctrl, int steps,
                       int mode, double* out);

@@ -32,7 +32,7 @@ QUAD_SCENES = ("quadTrees", "quadHouse", "quadPillars")
 
 def edge_draws(cfg, n: int, seed: int) -> np.ndarray:
     d = E.uniform_draws(n, seed)
-    d[0, :] = 1.0  # u == 1: steps = N + 1 (Q3) and controls at their maxima
+    d[0, :] = 1.0  # u == 1: steps = N + 1 and controls at their maxima
     d[1, :] = 2.0 ** -24  # smallest draw
     if cfg.fixed_steps:
         N_ = cfg.max_propagation_duration

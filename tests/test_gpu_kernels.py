@@ -216,9 +216,9 @@ def test_sincos_within_a_few_ulp_of_cuda(cuda):
 
 
 @pytest.mark.parametrize("name", list(PRESETS))
-def test_two_phase_large_batch_equals_one_pass(cuda, name):
-    """Batches of 2^18 segments or more run in two phases (the first steps of every segment, then
-    the live ones compacted); rows, verdicts and step counts equal the one-pass kernel's, which
+def test_phased_large_batch_equals_one_pass(cuda, name):
+    """Batches of 2^18 segments or more run in phases (the first steps of every segment, then the
+    live ones compacted, twice); rows, verdicts and step counts equal the one-pass kernel's, which
     smaller batches use: here the same draws propagated in slices of 2^17."""
     import torch
 

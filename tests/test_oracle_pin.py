@@ -63,7 +63,7 @@ def test_golden_vectors_reproduced(name):
     assert np.array_equal(valid, g["valid_brute"])  # no cell overflows in these scenes
     r1, r2 = O.regions(cfg, g["rows"])
     assert np.array_equal(r1, g["r1"]) and np.array_equal(r2, g["r2"])
-    # Q3: a duration draw of exactly 1 runs N + 1 steps where steps are drawn
+    # a duration draw of exactly 1 runs N + 1 steps where steps are drawn
     if not cfg.fixed_steps:
         assert steps[0] <= cfg.max_propagation_duration + 1
         assert g["rows"][0, -1] == np.float32(cfg.step_size) * (cfg.max_propagation_duration + 1)
@@ -131,7 +131,7 @@ def test_collision_hash_equals_brute_force():
 
 
 def test_reference_cell_overflow_is_listed_separately():
-    """Q2: the reference drops entries past 16 per 5 m cell; the oracle keeps them all.  Segments
+    """The reference drops entries past 16 per 5 m cell; the oracle keeps them all.  Segments
     whose reference verdict differs from the brute-force verdict must touch an overflowing cell."""
     cfg = kpax.preset(kpax.PRESET_DI)
     if not ref_available(cfg.model):
