@@ -527,7 +527,9 @@ def run_segments(args) -> None:
     fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
     achieved = n_steps * FLOP_PER_STEP[cfg.model] / t_s / 1e12
     roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                "traffic": None, "kernel": "k_propagate_batch<Dubins>",
+                "traffic": None,
+                "kernel": "k_propagate_head + 2 x k_propagate_tail<Dubins> (phased batch)" if n >= 1 << 18
+                          else "k_propagate_batch<Dubins>",
                 "peak_note": "nominal FP32: 148 SM x 128 lanes x 2 FLOP x clocks.max.sm (no measured FP32 peak in "
                              "MEASURED_PEAKS.json); plus 12 transcendental per step on the MUFU pipe",
                 "work": f"{n_steps} RK4 steps x {FLOP_PER_STEP[cfg.model]} FLOP over {args.steps} launches",
