@@ -48,6 +48,9 @@ FLOP_PER_STEP = {kpax.MODEL_DOUBLE_INTEGRATOR: 18, kpax.MODEL_DUBINS_AIRPLANE: 5
 # dram__bytes_read.sum + dram__bytes_write.sum of one steady-state k_expand launch (2^16 children,
 # L2 flushed before the iteration) in an ncu capture of the default workload; none for the others
 EXPAND_DRAM_BYTES = {kpax.MODEL_QUADROTOR: 1535744 + 0}
+# the same sum over the three phase kernels of one 2^20-segment Dubins batch (L2 flushed before the
+# step), per segment: scaled by the segment count, as the traffic grows with it
+PHASED_DRAM_BYTES_PER_SEGMENT = (118480128 + 29827072) / (1 << 20)
 WORKLOADS = {
     "quad": (kpax.PRESET_QUAD, E.quad_scene, "12D quadrotor, building scene (1000 AABBs incl. windowed wall), "
              "2^16 expansions/iteration, 25 RK4 steps of 0.02 s"),
@@ -527,7 +530,11 @@ def run_segments(args) -> None:
     fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
     achieved = n_steps * FLOP_PER_STEP[cfg.model] / t_s / 1e12
     roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                "traffic": None,
+                "traffic": int(PHASED_DRAM_BYTES_PER_SEGMENT * n) if n >= 1 << 18 else None,
+                "traffic_note": "DRAM bytes read + written per step by the three phase kernels, from an ncu capture of "
+                                "2^20 segments scaled to the segment count (profiles/k_propagate_batch_dubins_segments.md); "
+                                "the algorithmic bytes are 69 per segment (parent 24, row 40, verdict 1, steps 4), the rest "
+                                "is the survivors' round trips and partial-sector fills of rows written out of order",
                 "kernel": "k_propagate_head + 2 x k_propagate_tail<Dubins> (phased batch)" if n >= 1 << 18
                           else "k_propagate_batch<Dubins>",
                 "peak_note": "nominal FP32: 148 SM x 128 lanes x 2 FLOP x clocks.max.sm (no measured FP32 peak in "
