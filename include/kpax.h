@@ -287,6 +287,15 @@ kpax_status kpax_rekino_destroy(kpax_rekino* planner);
 kpax_status kpax_rekino_plan(kpax_rekino* planner, const float* h_init, const float* h_goal,
                              const float* d_obstacles, uint32_t n_obs, kpax_result* out);
 
+/* ---- environment input (readObstaclesFromCSV, helper.cu:13-39) ----------------------------
+ * Every float of the file, read as the reference reads it: line by line, a float taken off the
+ * line by stream extraction and one comma skipped after it; the first token that does not read as
+ * a float ends its line.  Up to `capacity` floats go to h_values (NULL to count only) and the number
+ * read to *n_values; the obstacles are the first n_values / 6 rows (the reference's numObstacles,
+ * workspaceDim 3; a trailing partial row is read but is not an obstacle).  KPAX_EINVAL when the
+ * file cannot be opened, where the reference exits the process. */
+kpax_status kpax_read_obstacles_csv(const char* filename, float* h_values, uint64_t capacity, uint64_t* n_values);
+
 /* ---- solution output (copyAndWriteVectorToCSV / writeVectorToCSV, helper.cuh:56-93) ------
  * Rows of `cols` floats as CSV, each value printed "%.6f" (std::fixed, setprecision 6) and
  * separated by commas, one row per line; append = 1 appends as the reference's append mode. */

@@ -87,4 +87,21 @@ private:
     std::vector<float> path_;
 };
 
+/* readObstaclesFromCSV (src/helper/helper.cu:13-39) with the reference's signature: every float of
+ * the file, numObstacles = floats / (2 * workspaceDim).  Throws std::runtime_error where the
+ * reference exits (the file cannot be opened). */
+inline std::vector<float> readObstaclesFromCSV(const std::string& filename, int& numObstacles, int workspaceDim)
+{
+    auto check = [](kpax_status s) {
+        if(s != KPAX_OK) throw std::runtime_error(std::string("kpax: ") + kpax_last_error());
+    };
+    uint64_t n = 0, m = 0;
+    check(kpax_read_obstacles_csv(filename.c_str(), nullptr, 0, &n));
+    std::vector<float> v(n);
+    check(kpax_read_obstacles_csv(filename.c_str(), v.data(), n, &m));
+    v.resize(m < n ? m : n);
+    numObstacles = (int)(v.size() / (2 * (size_t)workspaceDim));
+    return v;
+}
+
 #endif /* KPAX_HPP_ */

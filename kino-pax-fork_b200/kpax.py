@@ -167,6 +167,7 @@ _SIGNATURES = {
     "kpax_mlp_last_propose_ms": (ctypes.c_float, [_VP]),
     "kpax_set_proposal": (_I32, [_VP, _VP, ctypes.c_float]),
     "kpax_write_rows_csv": (_I32, [_VP, _U32, _U32, ctypes.c_char_p, _I32]),
+    "kpax_read_obstacles_csv": (_I32, [ctypes.c_char_p, _VP, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]),
     "kpax_rekino_defaults": (_I32, [_VP]),
     "kpax_rekino_create": (_I32, [ctypes.POINTER(Config), _VP, ctypes.POINTER(_VP)]),
     "kpax_rekino_destroy": (_I32, [_VP]),
@@ -568,6 +569,24 @@ class MLP:
             self.close()
         except Exception:
             pass
+
+
+def read_csv_floats(filename) -> np.ndarray:
+    """Every float of an obstacle CSV file through the C ABI (readObstaclesFromCSV's token rule)."""
+    L, name = load(), os.fsencode(filename)
+    n, m = ctypes.c_uint64(0), ctypes.c_uint64(0)
+    check(L.kpax_read_obstacles_csv(name, None, 0, ctypes.byref(n)), "kpax_read_obstacles_csv")
+    out = np.zeros(n.value, np.float32)
+    check(L.kpax_read_obstacles_csv(name, _ptr(out) if n.value else None, n.value, ctypes.byref(m)),
+          "kpax_read_obstacles_csv")
+    return out[: min(n.value, m.value)]
+
+
+def read_obstacles_csv(filename) -> np.ndarray:
+    """Obstacles of a CSV file (n x 6 float32) through the C ABI: the first n // 6 rows of its floats."""
+    v = read_csv_floats(filename)
+    k = v.size // 6
+    return v[: 6 * k].reshape(k, 6)
 
 
 def write_rows_csv(rows: np.ndarray, filename, append: bool = False) -> None:

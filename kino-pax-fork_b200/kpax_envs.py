@@ -14,13 +14,82 @@ import numpy as np
 W_MIN, W_MAX = 0.0, 100.0
 
 
+_WS = " \t\n\v\f\r"
+_DIGITS = "0123456789"
+_strtof = None
+
+
+def _to_float32(token: str):
+    """The float a C++ stream extracts from a complete numeric token (strtof in the "C" locale),
+    or None where the extraction fails (|value| beyond the float range)."""
+    global _strtof
+    if _strtof is None:
+        import ctypes
+
+        libc = ctypes.CDLL(None)
+        _strtof = libc.strtof
+        _strtof.restype, _strtof.argtypes = ctypes.c_float, [ctypes.c_char_p, ctypes.c_void_p]
+    v = np.float32(_strtof(token.encode(), None))
+    return None if np.isinf(v) else v
+
+
+def _line_floats(line: str) -> list:
+    """Floats of one line as readObstaclesFromCSV takes them (helper.cu:13-39): `ss >> value` after
+    skipping white space accepts [sign] digits [. digits] [e|E [sign] digits] (at least one mantissa
+    digit; an exponent only after one, and then with at least one digit), and one comma right
+    after a value is skipped.  The first token that does not extract ends the line."""
+    out, i, n = [], 0, len(line)
+    while True:
+        while i < n and line[i] in _WS:
+            i += 1
+        j = i
+        if j < n and line[j] in "+-":
+            j += 1
+        d0 = j
+        while j < n and line[j] in _DIGITS:
+            j += 1
+        digits = j > d0
+        if j < n and line[j] == ".":
+            j += 1
+            f0 = j
+            while j < n and line[j] in _DIGITS:
+                j += 1
+            digits = digits or j > f0
+        if not digits:
+            return out
+        if j < n and line[j] in "eE":
+            k = j + 1
+            if k < n and line[k] in "+-":
+                k += 1
+            e0 = k
+            while k < n and line[k] in _DIGITS:
+                k += 1
+            if k == e0:  # "1e" or "1e+": the collected token does not convert
+                return out
+            j = k
+        v = _to_float32(line[i:j])
+        if v is None:
+            return out
+        out.append(v)
+        i = j + 1 if j < n and line[j] == "," else j
+
+
+def read_csv_floats(path: str | Path) -> np.ndarray:
+    """Every float of an obstacle file, read line by line as readObstaclesFromCSV (helper.cu:13-39)
+    reads it (the same rule as kpax_read_obstacles_csv in the C ABI)."""
+    vals: list = []
+    text = Path(path).read_bytes().decode("latin-1")  # bytes as they are; lines end at "\n" only, as std::getline's
+    for line in text.split("\n"):
+        vals.extend(_line_floats(line))
+    return np.asarray(vals, np.float32)
+
+
 def read_obstacles_csv(path: str | Path) -> np.ndarray:
-    """Comma-separated floats, 6 per obstacle (readObstaclesFromCSV, helper.cu:13-39)."""
-    vals: list[float] = []
-    for line in Path(path).read_text().splitlines():
-        vals.extend(float(t) for t in line.replace(",", " ").split())
-    n = len(vals) // 6
-    return np.asarray(vals[: 6 * n], np.float32).reshape(n, 6)
+    """Obstacles of a CSV file, 6 floats each (readObstaclesFromCSV, helper.cu:13-39): the first
+    n // 6 rows of its floats; a trailing partial row is not an obstacle."""
+    vals = read_csv_floats(path)
+    n = vals.size // 6
+    return vals[: 6 * n].reshape(n, 6)
 
 
 def write_obstacles_csv(path: str | Path, obs: np.ndarray) -> None:

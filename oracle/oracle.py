@@ -253,6 +253,7 @@ class RefLib:
             ("kref_expand", ctypes.c_longlong, [_VP, ctypes.c_int, _VP, ctypes.c_int, _VP, _VP, _VP, _VP, _VP, _VP,
                                                 ctypes.c_int]),
             ("kref_max_threads", ctypes.c_int, []),
+            ("kref_read_obstacles_csv", ctypes.c_int, [ctypes.c_char_p, _VP, ctypes.c_int, _VP]),
         ]:
             fn = getattr(L, name)
             fn.restype, fn.argtypes = res, args
@@ -261,6 +262,15 @@ class RefLib:
         (self.model, self.state_dim, self.control_dim, self.sample_dim, self.grid_size, self.slots, self.num_r1,
          self.r2_per_r1, self.max_duration, self.grid_dim) = info
         self.obs = np.zeros((0, 6), np.float32)
+
+    def read_obstacles_csv(self, path, cap: int = 1 << 16):
+        """readObstaclesFromCSV (helper.cu:13-39): every float read and numObstacles."""
+        out = np.zeros(cap, np.float32)
+        n_obs = ctypes.c_int(0)
+        n = self.L.kref_read_obstacles_csv(str(path).encode(), _p(out), cap, ctypes.byref(n_obs))
+        if n < 0:
+            raise FileNotFoundError(path)
+        return out[: min(n, cap)].copy(), n_obs.value
 
     def set_obstacles(self, obs: np.ndarray) -> int:
         self.obs = np.ascontiguousarray(obs, np.float32).reshape(-1, 6)

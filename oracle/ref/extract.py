@@ -10,6 +10,7 @@ generated file is a build artefact (git-ignored) and is never committed.
 Extracted (paths relative to the reference root):
   src/collisionCheck/spatialHash.cu : isMotionValidSpatialHash   (spatialHash.cu:145-194)
   src/graphs/Graph.cu               : getRegion, getSubRegion    (Graph.cu:99-205)
+  src/helper/helper.cu              : readObstaclesFromCSV       (helper.cu:13-39)
 """
 import re
 import sys
@@ -19,6 +20,7 @@ FUNCTIONS = [
     ("src/collisionCheck/spatialHash.cu", r"^__device__ bool isMotionValidSpatialHash\("),
     ("src/graphs/Graph.cu", r"^__host__ __device__ int getRegion\(float\* coord\)"),
     ("src/graphs/Graph.cu", r"^__device__ int getSubRegion\(float\* coord, int r1, float\* minRegion\)"),
+    ("src/helper/helper.cu", r"^std::vector<float> readObstaclesFromCSV\("),
 ]
 
 
@@ -45,6 +47,7 @@ def main() -> None:
     parts = [
         "// generated by oracle/ref/extract.py from the reference sources; do not edit\n",
         '#include "statePropagator/statePropagatorSpatialHash.cuh"\n',
+        "#include <fstream>\n#include <iostream>\n#include <sstream>\n#include <string>\n#include <vector>\n",
     ]
     for rel, anchor in FUNCTIONS:
         parts.append(extract(root / rel, anchor))

@@ -7,6 +7,7 @@
  *   src/statePropagator/statePropagator.cu             (brute-force propagateAndCheck*, ode)
  *   src/collisionCheck/collisionCheck.cu               (isBroadPhaseValid, isMotionValid)
  *   spatialHash.cu:145-194 and Graph.cu:99-205         (extracted by extract.py)
+ *   helper.cu:13-39 (readObstaclesFromCSV)             (extracted by extract.py)
  * This file only adds what the reference implements as kernels or host code that cannot be
  * compiled for the CPU: the grid build (spatialHash.cu:9-67, run serially in obstacle order),
  * the region min-corner table (initializeRegions_kernel, Graph.cu:53-97) and the per-child
@@ -14,13 +15,16 @@
  */
 #include "statePropagator/statePropagatorSpatialHash.cuh"
 #include <stdint.h>
+#include <stdio.h>
 #include <string.h>
+#include <string>
 #include <vector>
 #include <algorithm>
 #include <omp.h>
 
 int getRegion(float* coord);
 int getSubRegion(float* coord, int r1, float* minRegion);
+std::vector<float> readObstaclesFromCSV(const std::string& filename, int& numObstacles, int workspaceDim);
 
 namespace {
 std::vector<int> g_starts(GRID_SIZE), g_counts(GRID_SIZE), g_idx(GRID_SIZE * MAX_OBSTACLES_PER_CELL);
@@ -223,5 +227,19 @@ long long kref_expand(const float* parents, int per_parent, const float* draws, 
 }
 
 int kref_max_threads(void) { return omp_get_max_threads(); }
+
+/* readObstaclesFromCSV (helper.cu:13-39) on a file that exists (it exits the process otherwise):
+ * returns the number of floats read and copies up to `cap` of them; *n_obstacles as it sets. */
+int kref_read_obstacles_csv(const char* path, float* out, int cap, int* n_obstacles)
+{
+    FILE* f = fopen(path, "r");
+    if(!f) return -1;
+    fclose(f);
+    int n = 0;
+    const std::vector<float> v = readObstaclesFromCSV(path, n, 3);
+    memcpy(out, v.data(), sizeof(float) * std::min<size_t>(v.size(), (size_t)cap));
+    *n_obstacles = n;
+    return (int)v.size();
+}
 
 }  // extern "C"
