@@ -456,6 +456,7 @@ kpax_status kpax_test_sincos(const float* d_x, uint32_t n, float* d_out, void* s
 
 kpax_status kpax_env_create(const kpax_config* cfg, const float* d_obstacles, uint32_t n_obs, void* stream, kpax_env** out)
 {
+    NvtxRange range("kpax_env_create");
     if(!cfg || !out || (n_obs && !d_obstacles)) return set_error("kpax_env_create: null argument"), KPAX_EINVAL;
     *out = nullptr;
     kpax_env* e = new(std::nothrow) kpax_env();
@@ -496,6 +497,7 @@ kpax_status kpax_propagate_batch(const kpax_config* cfg, kpax_env* env, const fl
                                  uint32_t draw_stream, uint32_t n, float* d_rows, uint8_t* d_valid, int32_t* d_steps,
                                  void* stream)
 {
+    NvtxRange range("kpax_propagate_batch");
     if(!cfg || !env || (n && (!d_parents || !d_rows || !d_valid)))
         return set_error("kpax_propagate_batch: null argument"), KPAX_EINVAL;
     KParams p;

@@ -1,6 +1,7 @@
 // kpax_internal.h — host-side objects shared by the environment, batch and planner units.
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
 #include <atomic>
@@ -23,11 +24,21 @@
 #define KPAX_CHECK_LAUNCH() KPAX_CUDA(cudaGetLastError())
 
 namespace kpax {
-// Runs f() and turns a C++ exception (a failed host allocation above all) into a status, so
-// nothing thrown crosses the C ABI.
+// An NVTX range over a host call (shown by Nsight Systems; without a tool attached the push and
+// pop return at once).
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
+// Runs f() inside an NVTX range named `what` and turns a C++ exception (a failed host allocation
+// above all) into a status, so nothing thrown crosses the C ABI.
 template <class F>
 kpax_status no_throw(const char* what, F&& f)
 {
+    NvtxRange range(what);
     try {
         return f();
     } catch(const std::bad_alloc&) {

@@ -442,6 +442,7 @@ struct PlanBatch {
     // poll = false all launches are queued first and the stream is synchronised once.
     kpax_status run(uint32_t guard, bool poll = true)
     {
+        NvtxRange range("kpax plan iterations");
         for(uint32_t g = 0; g < guard; ++g) {
             KPAX_CUDA(cudaGraphLaunch(graph, stream));
             count_launch(kernels_per_iteration() * (uint64_t)unroll);
