@@ -265,8 +265,10 @@ def train(X, Y, steps: int, cfg: kpax.Config, batch: int = 4096, lr: float = 1e-
 # ---------------------------------------------------------------------------------------------
 # evaluation
 
-def evaluate(seeds, cfg: kpax.Config, net: kpax.MLP | None = None, eps: float = 0.2, progress: bool = False):
-    """Plans every held-out scene; returns per-scene found / ms / iters / tree size."""
+def evaluate(seeds, cfg: kpax.Config, net: kpax.MLP | None = None, eps: float = 0.2, progress: bool = False,
+             family: dict | None = None):
+    """Plans every held-out scene (kpax_envs.learned_family with the `family` keywords: obstacle
+    range, start-goal separation); returns per-scene found / ms / iters / tree size."""
     import torch
 
     planner = kpax.KPAX(cfg)
@@ -274,7 +276,7 @@ def evaluate(seeds, cfg: kpax.Config, net: kpax.MLP | None = None, eps: float = 
         planner.set_proposal(net, eps)
     out = []
     for sd in seeds:
-        obs, start, goal = E.learned_family(int(sd))
+        obs, start, goal = E.learned_family(int(sd), **(family or {}))
         d_obs = torch.from_numpy(obs).cuda()
         r = planner.plan(start, goal, d_obs.data_ptr(), obs.shape[0])
         rec = {"seed": int(sd), "found": int(r.found), "ms": float(r.ms), "iters": int(r.iters), "tree": int(r.tree_size),
@@ -328,6 +330,10 @@ def main(argv=None):
     e.add_argument("--max-iter", type=int, default=0)
     e.add_argument("--expansions-log2", type=int, default=0, help="expansions per iteration (log2; 0 = preset)")
     e.add_argument("--tree-log2", type=int, default=0, help="tree capacity (log2; 0 = preset)")
+    e.add_argument("--obs", type=int, nargs=2, default=(200, 2000), metavar=("MIN", "MAX"),
+                   help="obstacle count range of the held-out scenes")
+    e.add_argument("--sep", type=float, nargs=2, default=(25.0, 45.0), metavar=("MIN", "MAX"),
+                   help="start-goal separation range (m) of the held-out scenes")
     pp = sub.add_parser("propose", help="time the tensor-core proposal pass on random states")
     pp.add_argument("--weights", type=Path, default=DEFAULT_WEIGHTS)
     pp.add_argument("--rows", type=int, default=1 << 16)
@@ -384,9 +390,10 @@ def main(argv=None):
             cfg.expansions_per_iter = 1 << a.expansions_log2
         if a.tree_log2:
             cfg.max_tree_size = 1 << a.tree_log2
-        plain = summarize(evaluate(seeds, cfg))
-        learned = summarize(evaluate(seeds, cfg, net, a.eps))
-        print(json.dumps({"plain": plain, "learned": learned}))
+        fam = {"obs_range": tuple(a.obs), "min_sep": a.sep[0], "max_sep": a.sep[1]}
+        plain = summarize(evaluate(seeds, cfg, family=fam))
+        learned = summarize(evaluate(seeds, cfg, net, a.eps, family=fam))
+        print(json.dumps({"family": fam, "plain": plain, "learned": learned}))
 
 
 if __name__ == "__main__":
