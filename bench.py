@@ -392,7 +392,7 @@ def run_ours(args) -> None:
     roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                 "traffic": EXPAND_DRAM_BYTES.get(cfg.model), "kernel": "k_expand",
                 "traffic_note": "DRAM bytes read + written by one steady-state 2^16-child k_expand launch of this "
-                                "workload in an ncu capture (profiles/k_expand_quad.md); the tree, regions and grid are "
+                                "workload in an ncu capture (summary under profiles/); the tree, regions and grid are "
                                 "L2-resident, so traffic is far below the bytes the kernel touches",
                 "peak_note": "nominal FP32: 148 SM x 128 lanes x 2 FLOP x clocks.max.sm (no measured FP32 peak in "
                              "MEASURED_PEAKS.json)",
@@ -535,7 +535,7 @@ def run_segments(args) -> None:
     roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                 "traffic": int(PHASED_DRAM_BYTES_PER_SEGMENT * n) if n >= 1 << 18 else None,
                 "traffic_note": "DRAM bytes read + written per step by the three phase kernels, from an ncu capture of "
-                                "2^20 segments scaled to the segment count (profiles/k_propagate_batch_dubins_segments.md); "
+                                "2^20 segments scaled to the segment count (summary under profiles/); "
                                 "the algorithmic bytes are 69 per segment (parent 24, row 40, verdict 1, steps 4), the rest "
                                 "is the survivors' round trips and partial-sector fills of rows written out of order",
                 "kernel": "k_propagate_head + 2 x k_propagate_tail<Dubins> (phased batch)" if n >= 1 << 18
