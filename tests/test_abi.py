@@ -94,6 +94,45 @@ def test_cpp_wrapper_header_compiles():
         assert r.returncode == 0, r.stderr
 
 
+def test_cpp_driver_reads_obstacle_files(tmp_path):
+    """A reference-style driver built against kpax.hpp and libkpax.so reads an obstacle file with
+    readObstaclesFromCSV(filename, numObstacles, workspaceDim), as examples/gpu/main.cu does."""
+    import shutil
+    import subprocess
+
+    gxx = next((g for g in ("/usr/bin/g++", shutil.which("g++")) if g and Path(g).exists()), None)
+    lib = ROOT / "kino-pax-fork_b200" / "libkpax.so"
+    if not gxx or not lib.exists():
+        pytest.skip("no g++ or libkpax.so")
+    (tmp_path / "obstacles.csv").write_text("x0,y0,z0,x1,y1,z1\n1,2,3,4,5,6\n7.5, 8, 9,10,11,12\n13,14\n")
+    src = """#include "kpax.hpp"
+#include <cstdio>
+int main(int argc, char** argv)
+{
+    int numObstacles = 0;
+    std::vector<float> obstacles = readObstaclesFromCSV(argv[1], numObstacles, 3);
+    std::printf("%d %zu", numObstacles, obstacles.size());
+    for(float v : obstacles) std::printf(" %g", v);
+    try {
+        readObstaclesFromCSV(std::string(argv[1]) + ".absent", numObstacles, 3);
+    } catch(const std::runtime_error&) {
+        std::printf(" missing-file-throws");
+    }
+    return 0;
+}
+"""
+    (tmp_path / "driver.cpp").write_text(src)
+    exe = tmp_path / "driver"
+    r = subprocess.run([gxx, "-std=c++17", f"-I{ROOT / 'include'}", str(tmp_path / "driver.cpp"), "-o", str(exe),
+                        f"-L{lib.parent}", "-lkpax", f"-Wl,-rpath,{lib.parent}"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    out = subprocess.run([str(exe), str(tmp_path / "obstacles.csv")], capture_output=True, text=True, timeout=60)
+    assert out.returncode == 0, out.stderr
+    # the header line reads nothing; white space before a value is skipped ("7.5, 8, 9"); the
+    # partial row's floats are read but are not an obstacle
+    assert out.stdout == "2 14 1 2 3 4 5 6 7.5 8 9 10 11 12 13 14 missing-file-throws", out.stdout
+
+
 def test_pruning_parameters_are_validated():
     """PruneKPAX's goal-progress pruning needs a positive progress scale and finite biases."""
     cfg = kpax.preset(kpax.PRESET_DI)
