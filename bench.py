@@ -698,6 +698,15 @@ def run_learned(args) -> None:
         t2 = time.perf_counter()
     launches = kpax.kernel_launches() - launches0
     sp, sl = L.summarize(plain), L.summarize(learned)
+    # the metric at >= 95 % success: the same seeds on a family whose goals lie within the trees'
+    # reach (start and goal 6-12 m apart, 100-300 boxes)
+    near = {"obs_range": (100, 300), "min_sep": 6.0, "max_sep": 12.0}
+    np_ = L.summarize(L.evaluate(seeds, cfg, family=near))
+    nl_ = L.summarize(L.evaluate(seeds, cfg, net, args.eps, family=near))
+    at95 = {"family": "building scenes of 100-300 AABBs, start/goal 6-12 m apart", "plain": np_, "learned": nl_,
+            "both_at_95": bool(np_["success"] >= 0.95 and nl_["success"] >= 0.95),
+            "p50_ratio_learned_to_plain": nl_["p50_ms"] / np_["p50_ms"] if np_["p50_ms"] > 0 else None,
+            "mean_ratio_learned_to_plain": nl_["mean_ms"] / np_["mean_ms"] if np_["mean_ms"] > 0 else None}
     # tensor-core proposal pass: 2^16 frontier entries (the quadrotor budget), device-timed
     obs, start, goal = E.learned_family(seeds[0])
     d_obs = torch.from_numpy(obs).cuda()
@@ -743,6 +752,7 @@ def run_learned(args) -> None:
                    "network": "51-256-256-88 SiLU, 8-component mixture", "training": meta},
         "plain": sp, "learned": sl,
         "success_gain": sl["success"] - sp["success"],
+        "at_95_success": at95,
         "proposal_pass": {"rows": n, "ms": prop_ms, "tflops": flop / (prop_ms * 1e-3) / 1e12},
         "roofline": {"bound": "tensor", "achieved": flop / (prop_ms * 1e-3) / 1e12, "peak": peak_tf, "unit": "TFLOP/s",
                      "frac": flop / (prop_ms * 1e-3) / 1e12 / peak_tf, "traffic": None,
