@@ -257,6 +257,24 @@ kpax_status kpax_collide_batch(kpax_env* env, const float* d_bbmin, const float*
  * d_states: n x state_dim floats; d_r2 may be NULL. */
 kpax_status kpax_region_batch(const kpax_config* cfg, const float* d_states, uint32_t n,
                               int32_t* d_r1, int32_t* d_r2, void* stream);
+/* Frontier compaction of the planner (the entry list of propagateFrontier / updateFrontier,
+ * KPAX.cu:310-351 with Planner.cu:52-80) on a caller's repeat counts, through the planner's own
+ * kernels.  Node i owns d_repeat[i] consecutive entries (0 = not in the frontier; 255, the
+ * planner's mark for a node added in the last iteration, counts as cfg->sparse_repeat).  With R
+ * entries in all and a children budget B, each entry gets k = children_per_entry children, or
+ * max(1, B / R) when R k > B, and E = min(R, B / k) entries are taken, evenly spaced over the
+ * frontier in node order (entry j is virtual entry floor(j R / E)); d_entries (room for B) receives
+ * their E node ids and every node with an entry taken gets repeat 0.  At most 2^24 nodes.  Waits
+ * for the stream. */
+typedef struct kpax_frontier_stats {
+    uint32_t R;  /* entries in the frontier */
+    uint32_t k;  /* children per entry taken */
+    uint32_t E;  /* entries taken */
+    uint32_t n;  /* children: E * k */
+} kpax_frontier_stats;
+kpax_status kpax_frontier_compact(const kpax_config* cfg, uint8_t* d_repeat, uint32_t n_nodes,
+                                  uint32_t budget, uint32_t* d_entries, kpax_frontier_stats* out,
+                                  void* stream);
 /* Test hook: for each x, writes (sin, cos) of the propagation kernels' sine/cosine and
  * (sin, cos) of CUDA's sincosf, 4 floats per input, so tests can bound their difference. */
 kpax_status kpax_test_sincos(const float* d_x, uint32_t n, float* d_out, void* stream);

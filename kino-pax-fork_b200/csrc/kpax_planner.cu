@@ -1065,4 +1065,65 @@ kpax_status kpax_batch_plan(kpax_batch* bt, const float* h_inits, const float* h
     });
 }
 
+// ---------------------------------------------------------------- frontier compaction on its own
+
+kpax_status kpax_frontier_compact(const kpax_config* cfg, uint8_t* d_repeat, uint32_t n_nodes, uint32_t budget,
+                                  uint32_t* d_entries, kpax_frontier_stats* out, void* stream)
+{
+    return no_throw("kpax_frontier_compact", [&]() -> kpax_status {
+        if(!cfg || !out || (n_nodes && !d_repeat) || (budget && !d_entries))
+            return set_error("kpax_frontier_compact: null argument"), KPAX_EINVAL;
+        if(n_nodes > (1u << 24)) return set_error("kpax_frontier_compact: %u nodes (at most 2^24)", n_nodes), KPAX_EINVAL;
+        KParams p;
+        kpax_status st = derive_params(*cfg, &p);
+        if(st != KPAX_OK) return st;
+        // the count pass takes B = min(budget, cap - tree): a capacity of tree + budget leaves B = budget
+        budget = std::min<uint32_t>(budget, 0xFFFFFFFFu - n_nodes);
+        p.budget = budget;
+        p.cap = n_nodes + budget;
+        // one query whose tree is the caller's repeat bytes: region ids 0, region 0 without valid
+        // samples (a pending node counts as sparse), no re-activation (tree_old = 0)
+        const uint32_t ntiles = std::max<uint32_t>(1, (n_nodes + kTile - 1) / kTile);
+        auto al = [](size_t b) { return (b + kAlign - 1) / kAlign * kAlign; };
+        const size_t o_ctl = al(sizeof(QueryDev)), o_tiles = o_ctl + al(sizeof(Ctl)), o_small = o_tiles + al(4ull * ntiles),
+                     o_r1 = o_small + kAlign, bytes = o_r1 + al(4ull * std::max<uint32_t>(n_nodes, 1));
+        char* mem = nullptr;
+        KPAX_CUDA(cudaMalloc(&mem, bytes));
+        struct Free {
+            char* m;
+            ~Free() { cudaFree(m); }
+        } free_mem{mem};
+        cudaStream_t s = (cudaStream_t)stream;
+        QueryDev q{};
+        q.p = p;
+        q.t.rep = d_repeat;
+        q.t.r1 = reinterpret_cast<int32_t*>(mem + o_r1);
+        q.rg.score = reinterpret_cast<float*>(mem + o_small);
+        q.rg.valid = reinterpret_cast<int32_t*>(mem + o_small + 16);
+        q.farr = reinterpret_cast<uint32_t*>(mem + o_small + 32);
+        uint32_t* d_active = reinterpret_cast<uint32_t*>(mem + o_small + 48);
+        q.ctl = reinterpret_cast<Ctl*>(mem + o_ctl);
+        q.tiles = reinterpret_cast<uint32_t*>(mem + o_tiles);
+        q.entries = d_entries;
+        Ctl c{};
+        c.tree = n_nodes;
+        c.iter = 1u;
+        c.score_total = 1.0f;
+        c.goal_idx = kNone;
+        KPAX_CUDA(cudaMemsetAsync(mem + o_small, 0, bytes - o_small, s));
+        KPAX_CUDA(cudaMemcpyAsync(mem, &q, sizeof(q), cudaMemcpyHostToDevice, s));
+        KPAX_CUDA(cudaMemcpyAsync(q.ctl, &c, sizeof(c), cudaMemcpyHostToDevice, s));
+        const QueryDev* dq = reinterpret_cast<const QueryDev*>(mem);
+        const uint32_t gx = std::min<uint32_t>(ntiles, kFrontierCTAs);
+        k_frontier_count<<<dim3(gx, 1), kFrontierBS, 0, s>>>(dq, d_active);
+        k_frontier_write<<<dim3(gx, 1), kFrontierBS, 0, s>>>(dq);
+        KPAX_CHECK_LAUNCH();
+        count_launch(2);
+        KPAX_CUDA(cudaMemcpyAsync(&c, q.ctl, sizeof(c), cudaMemcpyDeviceToHost, s));
+        KPAX_CUDA(cudaStreamSynchronize(s));
+        out->R = c.R, out->k = c.k, out->E = c.E, out->n = c.n;
+        return KPAX_OK;
+    });
+}
+
 }  // extern "C"

@@ -105,6 +105,10 @@ class Result(ctypes.Structure):
     ]
 
 
+class FrontierStats(ctypes.Structure):
+    _fields_ = [("R", ctypes.c_uint32), ("k", ctypes.c_uint32), ("E", ctypes.c_uint32), ("n", ctypes.c_uint32)]
+
+
 class BatchStats(ctypes.Structure):
     _fields_ = [("ms", ctypes.c_double), ("iters", ctypes.c_uint32), ("found", ctypes.c_uint32),
                 ("expansions", ctypes.c_uint64), ("valid_expansions", ctypes.c_uint64), ("steps", ctypes.c_uint64)]
@@ -145,6 +149,7 @@ _SIGNATURES = {
                                              _VP]),
     "kpax_collide_batch": (_I32, [_VP, _VP, _VP, _U32, _VP, _VP]),
     "kpax_region_batch": (_I32, [ctypes.POINTER(Config), _VP, _U32, _VP, _VP, _VP]),
+    "kpax_frontier_compact": (_I32, [ctypes.POINTER(Config), _VP, _U32, _U32, _VP, ctypes.POINTER(FrontierStats), _VP]),
     "kpax_kernel_launches": (ctypes.c_uint64, []),
     "kpax_batch_create": (_I32, [_VP, _U32, ctypes.POINTER(_VP)]),
     "kpax_batch_destroy": (_I32, [_VP]),
@@ -280,6 +285,15 @@ def collide_batch(env: Env, d_bbmin: int, d_bbmax: int, n: int, d_free: int, str
 
 def region_batch(cfg: Config, d_states: int, n: int, d_r1: int, d_r2: int | None, stream: int = 0) -> None:
     check(load().kpax_region_batch(ctypes.byref(cfg), d_states, n, d_r1, d_r2 or None, stream), "kpax_region_batch")
+
+
+def frontier_compact(cfg: Config, d_repeat: int, n_nodes: int, budget: int, d_entries: int, stream: int = 0) -> dict:
+    """The planner's frontier compaction on repeat bytes at d_repeat (kpax_frontier_compact):
+    entry node ids to d_entries, repeats of the nodes taken set to 0; returns R, k, E, n."""
+    st = FrontierStats()
+    check(load().kpax_frontier_compact(ctypes.byref(cfg), d_repeat, n_nodes, budget, d_entries or None, ctypes.byref(st),
+                                       stream), "kpax_frontier_compact")
+    return {"R": st.R, "k": st.k, "E": st.E, "n": st.n}
 
 
 def kernel_launches() -> int:

@@ -710,6 +710,53 @@ static float goal_dist(const float* x, const float* g)
     return sqrtf(dx * dx + dy * dy + dz * dz);
 }
 
+/* Children per entry k and entries taken E for R frontier entries under a children budget B > 0
+ * (KPAX.cu:323-350 as the CUDA path resolves it: k = CHILDREN_PER_ENTRY, or B / R (at least 1)
+ * when the entries would exceed the budget; E = min(R, B / k)). */
+static void budget_split(uint64_t R, uint32_t B, uint32_t per_entry, uint32_t* k_out, uint32_t* E_out)
+{
+    uint32_t k = per_entry;
+    if(R * k > B) {
+        k = (uint32_t)(B / (R ? R : 1));
+        if(k == 0) k = 1;
+    }
+    *k_out = k;
+    *E_out = R == 0 ? 0 : (uint32_t)(R < B / k ? R : B / k);
+}
+
+/* Entry list (repeatInd, Planner.cu:68-80).  Node i owns virtual entries [a, a + rep[i]).  When
+ * the R entries exceed the budget (E < R), entry j is virtual entry floor(j * R / E): E entries
+ * evenly spaced over the whole frontier (the reference gives every entry at least one child
+ * instead, KPAX.cu:323-336).  A node leaves the frontier when at least one of its entries is
+ * taken (KPAX.cu:372). */
+static void take_entries(uint8_t* rep, uint32_t tree, uint64_t R, uint32_t E, uint32_t* entry)
+{
+    uint64_t a = 0;
+    for(uint32_t i = 0; i < tree; ++i) {
+        const uint32_t cnt = rep[i];
+        if(!cnt) continue;
+        const uint64_t b = a + cnt;
+        const uint64_t lo = (a * E + R - 1) / R, hi = (b * E + R - 1) / R;
+        for(uint64_t j = lo; j < hi; ++j) entry[j] = i;
+        if(lo < hi) rep[i] = 0;
+        a = b;
+    }
+}
+
+void ko_frontier_compact(const kpax_config* cfg, uint8_t* rep, uint32_t n, uint32_t budget, uint32_t* entries,
+                         uint32_t stats[4])
+{
+    uint64_t R = 0;
+    for(uint32_t i = 0; i < n; ++i) {  /* a pending node of a region without valid samples */
+        if(rep[i] == KO_PENDING) rep[i] = 0 < cfg->sparse_valid_threshold ? (uint8_t)cfg->sparse_repeat : 1;
+        R += rep[i];
+    }
+    uint32_t k = cfg->children_per_entry, E = 0;
+    if(budget) budget_split(R, budget, cfg->children_per_entry, &k, &E);
+    take_entries(rep, n, R, E, entries);
+    stats[0] = (uint32_t)R, stats[1] = k, stats[2] = E, stats[3] = E * k;
+}
+
 int ko_plan(const kpax_config* cfg, const float* init, const float* goal, const float* obs, uint32_t n_obs,
             uint32_t plan_idx, uint32_t max_iters, int stop_at_goal, ko_plan_out* out)
 {
@@ -753,28 +800,10 @@ int ko_plan(const kpax_config* cfg, const float* init, const float* goal, const 
         }
         uint32_t B = cap - tree < budget_max ? cap - tree : budget_max;
         if(B == 0) { full = 1; it -= 1; break; }
-        uint32_t k = cfg->children_per_entry;
-        if(R * k > B) {
-            k = (uint32_t)(B / (R ? R : 1));
-            if(k == 0) k = 1;
-        }
-        uint32_t E = (uint32_t)(R < B / k ? R : B / k), n = E * k;
-        if(R == 0) E = 0, n = 0;
-        /* entry list (repeatInd, Planner.cu:68-80).  Node i owns virtual entries [a, a + rep[i]).
-         * When the R entries exceed the budget (E < R, one child each), entry j is virtual entry
-         * floor(j * R / E): E entries evenly spaced over the whole frontier (the reference gives
-         * every entry at least one child instead, KPAX.cu:323-336).  A node leaves the frontier
-         * when at least one of its entries is taken (KPAX.cu:372). */
-        uint64_t a = 0;
-        for(uint32_t i = 0; i < tree; ++i) {
-            const uint32_t cnt = rep[i];
-            if(!cnt) continue;
-            const uint64_t b = a + cnt;
-            const uint64_t lo = (a * E + R - 1) / R, hi = (b * E + R - 1) / R;
-            for(uint64_t j = lo; j < hi; ++j) entry[j] = i;
-            if(lo < hi) rep[i] = 0;
-            a = b;
-        }
+        uint32_t k, E;
+        budget_split(R, B, cfg->children_per_entry, &k, &E);
+        const uint32_t n = E * k;
+        take_entries(rep, tree, R, E, entry);
         memcpy(nxt, cur, sizeof(uint32_t) * words);
         /* propagateFrontier_kernel1 body (KPAX.cu:381-396) with snapshot R2 reads */
         for(uint32_t c = 0; c < n; ++c) {

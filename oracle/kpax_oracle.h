@@ -112,6 +112,10 @@ typedef struct ko_plan_out {
     /* results */
     kpax_result result;
 } ko_plan_out;
+/* Frontier compaction on its own (kpax_frontier_compact): repeat bytes in place (255 = pending,
+ * resolved as a node of a region without valid samples), entries[0..E), stats = {R, k, E, n}. */
+void ko_frontier_compact(const kpax_config* cfg, uint8_t* rep, uint32_t n, uint32_t budget, uint32_t* entries,
+                         uint32_t stats[4]);
 int ko_plan(const kpax_config* cfg, const float* init, const float* goal, const float* obs,
             uint32_t n_obs, uint32_t plan_idx, uint32_t max_iters, int stop_at_goal,
             ko_plan_out* out);

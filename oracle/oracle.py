@@ -58,6 +58,7 @@ def lib() -> ctypes.CDLL:
             "ko_region_r2": (ctypes.c_int, [_VP, _VP, _VP, ctypes.c_int]),
             "ko_scores": (None, [_VP, _VP, _VP, _VP, _VP]),
             "ko_faccept": (_F32, [_VP, _U32, _U32]),
+            "ko_frontier_compact": (None, [_VP, _VP, _U32, _U32, _VP, _VP]),
             "ko_plan": (ctypes.c_int, [_VP, _VP, _VP, _VP, _U32, _U32, _U32, ctypes.c_int, _VP]),
             "ko_sizes": (ctypes.c_int, [_VP, _VP, _VP, _VP]),
         }
@@ -165,6 +166,16 @@ def region_table(cfg) -> np.ndarray:
     t = np.zeros((n1, cols), np.float32)
     lib().ko_region_table(_c(cfg), _p(t))
     return t
+
+
+def frontier_compact(cfg, repeat: np.ndarray, budget: int):
+    """Frontier compaction on its own: (repeat bytes after, entry node ids, {R, k, E, n})."""
+    rep = np.ascontiguousarray(repeat, np.uint8).copy()
+    entries = np.zeros(max(int(budget), 1), np.uint32)
+    stats = np.zeros(4, np.uint32)
+    lib().ko_frontier_compact(_c(cfg), _p(rep), rep.size, int(budget), _p(entries), _p(stats))
+    R, k, E, n = (int(x) for x in stats)
+    return rep, entries[:E].copy(), {"R": R, "k": k, "E": E, "n": n}
 
 
 def regions(cfg, states: np.ndarray):

@@ -247,3 +247,26 @@ def test_phased_large_batch_equals_one_pass(cuda, name):
     assert np.array_equal(bits(a[0]), bits(b[0])), f"{name}: rows differ"
     assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2]), f"{name}: verdicts or step counts differ"
     assert 0 < a[1].mean() < 1
+
+
+@pytest.mark.parametrize("n,density", [(0, 0.3), (1, 1.0), (5000, 0.3), ((1 << 20) + 37, 0.2)])
+def test_frontier_compaction_bit_exact(cuda, n, density):
+    """kpax_frontier_compact (the planner's two frontier kernels on a caller's repeat bytes) against
+    the oracle: R, k, E, n, the entry list and the repeat bytes after, for budgets from 0 to all
+    entries (k = children per entry), through k = 2 and one child each with strided entries."""
+    import torch
+
+    cfg = kpax.preset(kpax.PRESET_QUAD)
+    rng = np.random.default_rng(n)
+    rep = np.where(rng.random(n) < density, rng.integers(1, 16, n), 0).astype(np.uint8)
+    rep[rng.random(n) < 0.02] = 255  # pending: counts as the sparse repeat
+    R = int(np.where(rep == 255, cfg.sparse_repeat, rep).sum())
+    for budget in sorted({0, 1, 7, max(R - 1, 1), 2 * R + 5, R * cfg.children_per_entry, 1 << 16}):
+        d_rep = torch.from_numpy(rep.copy()).cuda() if n else torch.zeros(1, dtype=torch.uint8, device="cuda")
+        d_ent = torch.full((max(budget, 1),), -1, dtype=torch.int32, device="cuda")
+        st = kpax.frontier_compact(cfg, d_rep.data_ptr(), n, budget, d_ent.data_ptr())
+        o_rep, o_ent, o_st = O.frontier_compact(cfg, rep, budget)
+        assert st == o_st, (budget, st, o_st)
+        assert np.array_equal(d_ent[: st["E"]].cpu().numpy().view(np.uint32), o_ent), budget
+        assert np.array_equal(d_rep.cpu().numpy()[:n], o_rep), budget
+        assert st["E"] == budget or st["E"] == R or st["E"] * st["k"] <= budget
