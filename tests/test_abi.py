@@ -159,4 +159,10 @@ def test_null_arguments_are_rejected_without_a_gpu():
     assert lib.kpax_plan(None, None, None, None, 0, 0, None) == kpax.EINVAL
     assert lib.kpax_plan_bench(None, None, None, None, 0, 0, None, None) == kpax.EINVAL
     assert lib.kpax_export_tree(None, None, None, None, 0, None) == kpax.EINVAL
+    st = kpax.FrontierStats()
+    assert lib.kpax_frontier_compact(None, None, 0, 0, None, ctypes.byref(st), None) == kpax.EINVAL
+    assert lib.kpax_frontier_compact(ctypes.byref(cfg), None, 10, 0, None, ctypes.byref(st), None) == kpax.EINVAL
+    assert lib.kpax_frontier_compact(ctypes.byref(cfg), 16, 10, 5, None, ctypes.byref(st), None) == kpax.EINVAL
+    assert lib.kpax_frontier_compact(ctypes.byref(cfg), 16, (1 << 24) + 1, 0, None, ctypes.byref(st), None) == kpax.EINVAL
+    assert b"2^24" in lib.kpax_last_error()
     assert lib.kpax_last_error()
