@@ -14,11 +14,12 @@ the reference's own counter (sum of d_validCounterArray_, src/planners/KPAX.cu:3
          host (oracle/_ref, OpenMP over all cores) on a bounded sample of the same children.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload quad|dubins|di|segments|learned|batch]
+                  [--workload quad|dubins|di|segments|collide|learned|batch]
 
 Other workloads: dubins / di (the same iteration on the other models), segments (2^22 independent
-Dubins segments through kpax_propagate_batch), learned (learned-vs-plain A/B on 256 held-out
-scenes, tensor-core pass and training rates), batch (1024 mixed queries in one batched plan).
+Dubins segments through kpax_propagate_batch), collide (2^22 swept-box queries through
+kpax_collide_batch), learned (learned-vs-plain A/B on 256 held-out scenes, tensor-core pass and
+training rates), batch (1024 mixed queries in one batched plan).
 The reference arm has no counterpart for learned and batch and says so.
 """
 from __future__ import annotations
@@ -59,6 +60,12 @@ WORKLOADS = {
     "di": (kpax.PRESET_DI, E.di_scene, "6D double integrator, 20 AABBs, 2^14 expansions/iteration, U{1..10} steps of 0.1 s"),
 }
 FLUSH_BYTES = 256 << 20  # > 126 MB L2
+COLLIDE_DESC = ("swept-box queries against the spatial hash (isMotionValidSpatialHash): 2^22 boxes, corners uniform in "
+                "[0,100]^3, extents U[0,0.2] m per axis (one integration step), building scene of 1000 AABBs")
+COLLIDE_BYTES_PER_BOX = 25  # algorithmic: two corners in (6 floats), one verdict byte out
+# DRAM bytes (read + write) per box of one k_collide_batch launch on 2^20 boxes, L2 flushed before it,
+# in an ncu capture (dram__bytes.sum.per_second x gpu__time_duration.sum / boxes)
+COLLIDE_DRAM_BYTES_PER_BOX = 937.433526e9 * 27.68e-6 / (1 << 20)
 SEGMENTS_DESC = ("Dubins airplane propagation/collision microbench: 2^22 independent segments, parents uniform within "
                  "the bounds, forest of 200 columns, 20 RK4 steps of 0.05 s")
 
@@ -226,6 +233,137 @@ def cpu_segments_rate(budget_s: float, n: int = 1 << 16, steps: int = 3):
             f"{runs} runs of {n} segments (20 steps each), {tot_v / (runs * n):.2f} valid, {tot_t:.1f} s", 1000 * tot_t / runs)
 
 
+def collide_inputs(n: int, seed: int):
+    """Boxes of the collision microbench and the scene, with the quadrotor preset's hash cell."""
+    cfg = kpax.preset(kpax.PRESET_QUAD)
+    obs, _, _ = E.quad_scene()
+    rng = np.random.default_rng(seed)
+    lo = rng.uniform(0.0, 100.0, (n, 3)).astype(np.float32)
+    hi = (lo + rng.uniform(0.0, 0.2, (n, 3))).astype(np.float32)
+    return cfg, obs, lo, hi
+
+
+def cpu_collide_rate(budget_s: float, n: int = 1 << 18):
+    """The reference's own isMotionValidSpatialHash (oracle/_ref, OpenMP, all host threads) on the
+    microbench's boxes: queries per second, threads, sample description, ms per run."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    cfg, obs, lo, hi = collide_inputs(n, 11)
+    ref = O.RefLib(cfg.model)
+    ref.set_obstacles(obs)
+    threads = ref.L.kref_max_threads()
+    tot_t, runs = 0.0, 0
+    while runs < 3 or tot_t < budget_s:
+        t0 = time.perf_counter()
+        ref.collide_batch(lo, hi, use_hash=True, nthreads=threads)
+        tot_t += time.perf_counter() - t0
+        runs += 1
+        if tot_t > 4 * budget_s:
+            break
+    return n * runs / tot_t, threads, f"{runs} runs of {n} boxes (reference 5 m / 16-slot grid), {tot_t:.1f} s", 1000 * tot_t / runs
+
+
+def run_collide(args) -> None:
+    """2^22 swept-box queries per step through kpax_collide_batch (the expansion's per-step query)."""
+    import torch
+
+    ws, rank, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    n = 1 << args.boxes_log2
+    cfg, obs, lo, hi = collide_inputs(n, 13 + rank)
+    if not args.no_tune:
+        import kpax_autotune
+
+        cfg, _ = kpax_autotune.tuned(cfg, obs.shape[0])
+    d_obs = torch.from_numpy(obs).cuda()
+    env = kpax.Env(cfg, d_obs.data_ptr(), obs.shape[0])
+    d_lo, d_hi = torch.from_numpy(lo).cuda(), torch.from_numpy(hi).cuda()
+    free = torch.empty(n, dtype=torch.uint8, device="cuda")
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def launch():
+        kpax.collide_batch(env, d_lo.data_ptr(), d_hi.data_ptr(), n, free.data_ptr(), stream=stream.cuda_stream)
+
+    for _ in range(max(args.warmup, 3)):
+        launch()
+    launches0 = kpax.kernel_launches()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with Clocks(local) as clk:
+        for i in range(args.steps):
+            flush.fill_(i & 0xFF)  # evict the 126 MB L2 between steps, outside the events
+            ev[i][0].record(stream)
+            launch()
+            ev[i][1].record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    launches = kpax.kernel_launches() - launches0
+    t_s = sum(a.elapsed_time(b) for a, b in ev) / 1000.0
+    t_job, boxes_all = combine_over_ranks(dist, "cuda", t_s, n * args.steps)
+    value = boxes_all / t_job
+    free_fraction = float(free.float().mean().item())
+    peaks = load_peaks()
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = COLLIDE_BYTES_PER_BOX * n * args.steps / t_s / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                "traffic": int(COLLIDE_DRAM_BYTES_PER_BOX * n),
+                "traffic_note": "DRAM bytes per launch from an ncu capture of 2^20 boxes (summary under profiles/), scaled "
+                                "to the box count: 24.7 B per box against 25 algorithmic, no re-reads",
+                "kernel": "k_collide_batch", "work": f"{COLLIDE_BYTES_PER_BOX} algorithmic bytes per box (corners in, "
+                "verdict out); the grid's offsets, entries and boxes are read from L2",
+                "peak_source": "measured copy" if "fallback" not in peaks else "fallback",
+                "ms_per_launch": 1000 * t_s / args.steps}
+    # end to end through the C ABI from pinned host buffers: corners in, verdicts out
+    h_lo, h_hi = torch.from_numpy(lo).pin_memory(), torch.from_numpy(hi).pin_memory()
+    h_free = torch.empty(n, dtype=torch.uint8).pin_memory()
+    e_steps = max(2, min(args.steps, 5))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(e_steps):
+        d_lo.copy_(h_lo, non_blocking=True)
+        d_hi.copy_(h_hi, non_blocking=True)
+        launch()
+        h_free.copy_(free, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e = {"value": n * e_steps / (e0.elapsed_time(e1) / 1000.0), "unit": "queries/s",
+           "h2d_bytes_per_step": int(2 * lo.nbytes), "d2h_bytes_per_step": int(h_free.numel())}
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        try:
+            rate, cores, sample, _ = cpu_collide_rate(args.cpu_seconds)
+            cpu = {"value": rate, "unit": "queries/s", "cores": cores, "kind": "reference", "sample": sample}
+        except (FileNotFoundError, OSError) as exc:
+            cpu = {"value": None, "unit": "queries/s", "cores": 0, "kind": "reference", "sample": f"unavailable: {exc}"}
+    if rank == 0:
+        line = {
+            "metric": "swept-box queries/s", "value": value, "unit": "queries/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000 * t_job / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": COLLIDE_DESC if n == 1 << 22 else COLLIDE_DESC.replace("2^22", f"2^{args.boxes_log2}"),
+                       "boxes_per_step": n, "hash_cell_size": cfg.hash_cell_size, "free_fraction": free_fraction,
+                       "l2": "flushed before each timed step (256 MiB write, outside the events)",
+                       "parallelism": f"replicas x{ws}"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
 def run_reference(args) -> None:
     ws, rank, _ = dist_setup(args.gpus)
     if rank != 0:
@@ -235,6 +373,18 @@ def run_reference(args) -> None:
                "the reference plans one query per plan() call with a compile-time model; its per-child routines are "
                "timed by the single-query workloads")
         print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
+        return
+    if args.workload == "collide":
+        rate, threads, sample, ms = cpu_collide_rate(min(20.0, 2.0 * max(args.steps, 1)))
+        line = {
+            "impl": "reference", "metric": "swept-box queries/s", "value": rate, "unit": "queries/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32", "data": "synthetic",
+            "config": {"workload": COLLIDE_DESC, "boxes_per_step": 1 << 18, "parallelism": "host OpenMP"},
+            "cpu_baseline": {"value": rate, "unit": "queries/s", "cores": threads, "kind": "reference", "sample": sample},
+            "e2e": {"value": rate, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
         return
     if args.workload == "segments":
         rate, threads, sample, ms = cpu_segments_rate(min(20.0, 2.0 * max(args.steps, 1)), steps=max(args.steps, 1))
@@ -776,7 +926,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "learned", "segments"], default="quad")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "learned", "segments", "collide"], default="quad")
     ap.add_argument("--seeds", type=int, default=256, help="held-out scenes of the learned workload")
     ap.add_argument("--eps", type=float, default=0.2, help="uniform fraction of the learned proposal")
     ap.add_argument("--proposal", choices=["on", "off"], default="on", help="learned proposal for batched quadrotor queries")
@@ -786,6 +936,7 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="ignore the autotuner's cached launch parameters")
     ap.add_argument("--segments-log2", type=int, default=22, help="segments per step of the segments workload (log2)")
+    ap.add_argument("--boxes-log2", type=int, default=22, help="box queries per step of the collide workload (log2)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -795,6 +946,8 @@ def main() -> None:
         run_learned(args)
     elif args.workload == "segments":
         run_segments(args)
+    elif args.workload == "collide":
+        run_collide(args)
     else:
         run_ours(args)
 

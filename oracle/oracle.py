@@ -265,6 +265,7 @@ class RefLib:
                                                 ctypes.c_int]),
             ("kref_max_threads", ctypes.c_int, []),
             ("kref_read_obstacles_csv", ctypes.c_int, [ctypes.c_char_p, _VP, ctypes.c_int, _VP]),
+            ("kref_collide_batch", None, [_VP, _VP, ctypes.c_int, ctypes.c_int, _VP, ctypes.c_int]),
         ]:
             fn = getattr(L, name)
             fn.restype, fn.argtypes = res, args
@@ -313,6 +314,14 @@ class RefLib:
         lo = np.ascontiguousarray(lo, np.float32).reshape(-1, 3)
         hi = np.ascontiguousarray(hi, np.float32).reshape(-1, 3)
         return np.array([self.L.kref_collide(_p(lo[i]), _p(hi[i]), int(use_hash)) for i in range(lo.shape[0])], np.uint8)
+
+    def collide_batch(self, lo, hi, use_hash: bool = True, nthreads: int = 1) -> np.ndarray:
+        """kref_collide over n boxes with OpenMP: 1 = free."""
+        lo = np.ascontiguousarray(lo, np.float32).reshape(-1, 3)
+        hi = np.ascontiguousarray(hi, np.float32).reshape(-1, 3)
+        out = np.zeros(lo.shape[0], np.uint8)
+        self.L.kref_collide_batch(_p(lo), _p(hi), lo.shape[0], int(use_hash), _p(out), nthreads)
+        return out
 
     def expand(self, parents, per_parent, draws, scores, r2flags, counter, valid_counter, nthreads):
         parents = np.ascontiguousarray(parents, np.float32)

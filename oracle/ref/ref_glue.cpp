@@ -173,6 +173,13 @@ int kref_collide(const float* bbmin, const float* bbmax, int use_hash)
     return isMotionValid(lo, hi, lo, hi, g_obs.data(), g_nobs) ? 1 : 0;
 }
 
+/* kref_collide over n boxes (n x 3 floats each side), OpenMP over the boxes. */
+void kref_collide_batch(const float* bbmin, const float* bbmax, int n, int use_hash, uint8_t* out, int nthreads)
+{
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for(int i = 0; i < n; ++i) out[i] = (uint8_t)kref_collide(bbmin + 3 * (size_t)i, bbmax + 3 * (size_t)i, use_hash);
+}
+
 #if MODEL == 3
 /* The quadrotor right-hand side (statePropagator.cu:325-370). */
 void kref_ode(float* xdot, const float* x0, const float* h, const float* ctrl, int itr)

@@ -30,6 +30,14 @@ def test_segments_reference_line():
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
 
 
+@pytest.mark.skipif(not (ROOT / "oracle" / "_ref" / "libkref_quad.so").exists(), reason="reference routines not built")
+def test_collide_reference_line():
+    d = run("--workload", "collide", "--steps", "1", "--warmup", "1")
+    assert d["impl"] == "reference" and d["metric"] == "swept-box queries/s" and d["unit"] == "queries/s"
+    assert d["value"] > 0 and d["cpu_baseline"]["value"] == d["value"] and d["cpu_baseline"]["cores"] >= 1
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
 @pytest.mark.parametrize("workload", ["learned", "batch"])
 def test_no_counterpart_lines(workload):
     d = run("--workload", workload)
