@@ -275,6 +275,11 @@ typedef struct kpax_frontier_stats {
 kpax_status kpax_frontier_compact(const kpax_config* cfg, uint8_t* d_repeat, uint32_t n_nodes,
                                   uint32_t budget, uint32_t* d_entries, kpax_frontier_stats* out,
                                   void* stream);
+/* Test hook of the bounded device waits: one warp runs the expansion's look-back wait
+ * (tile 1 waiting for tile 0, which nothing publishes) with a limit of spin_limit polls
+ * (1 .. 2^22); it gives up, the kernel stores a timeout status and returns, and the call returns
+ * KPAX_ETIMEOUT with *h_status = 1.  The context stays usable. */
+kpax_status kpax_test_wait_timeout(uint32_t spin_limit, uint32_t* h_status, void* stream);
 /* Test hook: for each x, writes (sin, cos) of the propagation kernels' sine/cosine and
  * (sin, cos) of CUDA's sincosf, 4 floats per input, so tests can bound their difference. */
 kpax_status kpax_test_sincos(const float* d_x, uint32_t n, float* d_out, void* stream);

@@ -142,7 +142,8 @@ __device__ __forceinline__ void lb_publish(unsigned long long* slot, uint32_t ep
 // Exclusive prefix of tile b, computed by the 32 lanes of one warp: each probe reads the status
 // of 32 predecessors at once and stops at the nearest inclusive prefix.  Returns false when a
 // predecessor never published (bounded wait).
-__device__ __forceinline__ bool lb_exclusive(unsigned long long* lb, uint32_t b, uint32_t epoch, uint32_t& excl)
+__device__ __forceinline__ bool lb_exclusive(unsigned long long* lb, uint32_t b, uint32_t epoch, uint32_t& excl,
+                                             uint32_t spin_limit = kSpinLimit)
 {
     const uint32_t tag = epoch & 0x3FFFFFFFu;
     const int lane = threadIdx.x & 31;
@@ -160,7 +161,7 @@ __device__ __forceinline__ bool lb_exclusive(unsigned long long* lb, uint32_t b,
         const int first = incl ? __ffs(incl) - 1 : 31;
         const uint32_t need = first == 31 ? 0xffffffffu : ((2u << first) - 1u);
         if((ready & need) != need) {
-            if(++spins > kSpinLimit) {
+            if(++spins > spin_limit) {
                 excl = acc;
                 return false;
             }

@@ -1065,6 +1065,47 @@ kpax_status kpax_batch_plan(kpax_batch* bt, const float* h_inits, const float* h
     });
 }
 
+}  // extern "C"
+
+namespace {
+// Tile 1 of a look-back whose tile 0 never publishes: the expansion's bounded wait runs out after
+// spin_limit polls and reports a timeout instead of spinning on.
+__global__ void k_test_lookback_timeout(unsigned long long* lb, uint32_t spin_limit, uint32_t* status)
+{
+    uint32_t excl = 0;
+    const bool ok = lb_exclusive(lb, 1u, 1u, excl, spin_limit);
+    if(threadIdx.x == 0) *status = ok ? 0u : kErrTimeout;
+}
+}  // namespace
+
+extern "C" {
+
+kpax_status kpax_test_wait_timeout(uint32_t spin_limit, uint32_t* h_status, void* stream)
+{
+    return no_throw("kpax_test_wait_timeout", [&]() -> kpax_status {
+        if(!h_status || spin_limit == 0 || spin_limit > kSpinLimit)
+            return set_error("kpax_test_wait_timeout: need a status pointer and 1 <= spin_limit <= %u", kSpinLimit),
+                   KPAX_EINVAL;
+        char* mem = nullptr;
+        KPAX_CUDA(cudaMalloc(&mem, 64));
+        struct Free {
+            char* m;
+            ~Free() { cudaFree(m); }
+        } free_mem{mem};
+        cudaStream_t s = (cudaStream_t)stream;
+        KPAX_CUDA(cudaMemsetAsync(mem, 0, 64, s));  // status words of tiles 0 and 1: never published
+        uint32_t* d_status = reinterpret_cast<uint32_t*>(mem + 32);
+        k_test_lookback_timeout<<<1, 32, 0, s>>>(reinterpret_cast<unsigned long long*>(mem), spin_limit, d_status);
+        KPAX_CHECK_LAUNCH();
+        count_launch(1);
+        KPAX_CUDA(cudaMemcpyAsync(h_status, d_status, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        KPAX_CUDA(cudaStreamSynchronize(s));
+        if(*h_status & kErrTimeout)
+            return set_error("kpax_test_wait_timeout: the look-back wait gave up after %u polls", spin_limit), KPAX_ETIMEOUT;
+        return KPAX_OK;
+    });
+}
+
 // ---------------------------------------------------------------- frontier compaction on its own
 
 kpax_status kpax_frontier_compact(const kpax_config* cfg, uint8_t* d_repeat, uint32_t n_nodes, uint32_t budget,

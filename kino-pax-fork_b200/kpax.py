@@ -150,6 +150,7 @@ _SIGNATURES = {
     "kpax_collide_batch": (_I32, [_VP, _VP, _VP, _U32, _VP, _VP]),
     "kpax_region_batch": (_I32, [ctypes.POINTER(Config), _VP, _U32, _VP, _VP, _VP]),
     "kpax_frontier_compact": (_I32, [ctypes.POINTER(Config), _VP, _U32, _U32, _VP, ctypes.POINTER(FrontierStats), _VP]),
+    "kpax_test_wait_timeout": (_I32, [_U32, ctypes.POINTER(_U32), _VP]),
     "kpax_kernel_launches": (ctypes.c_uint64, []),
     "kpax_batch_create": (_I32, [_VP, _U32, ctypes.POINTER(_VP)]),
     "kpax_batch_destroy": (_I32, [_VP]),
@@ -294,6 +295,13 @@ def frontier_compact(cfg: Config, d_repeat: int, n_nodes: int, budget: int, d_en
     check(load().kpax_frontier_compact(ctypes.byref(cfg), d_repeat, n_nodes, budget, d_entries or None, ctypes.byref(st),
                                        stream), "kpax_frontier_compact")
     return {"R": st.R, "k": st.k, "E": st.E, "n": st.n}
+
+
+def test_wait_timeout(spin_limit: int, stream: int = 0) -> None:
+    """Runs the expansion's look-back wait against a tile that never publishes (kpax_test_wait_timeout):
+    raises KpaxError with status ETIMEOUT once the wait gives up."""
+    st = ctypes.c_uint32(0)
+    check(load().kpax_test_wait_timeout(spin_limit, ctypes.byref(st), stream), "kpax_test_wait_timeout")
 
 
 def kernel_launches() -> int:

@@ -165,4 +165,8 @@ def test_null_arguments_are_rejected_without_a_gpu():
     assert lib.kpax_frontier_compact(ctypes.byref(cfg), 16, 10, 5, None, ctypes.byref(st), None) == kpax.EINVAL
     assert lib.kpax_frontier_compact(ctypes.byref(cfg), 16, (1 << 24) + 1, 0, None, ctypes.byref(st), None) == kpax.EINVAL
     assert b"2^24" in lib.kpax_last_error()
+    status = ctypes.c_uint32(0)
+    assert lib.kpax_test_wait_timeout(0, ctypes.byref(status), None) == kpax.EINVAL
+    assert lib.kpax_test_wait_timeout(16, None, None) == kpax.EINVAL
+    assert lib.kpax_test_wait_timeout((1 << 22) + 1, ctypes.byref(status), None) == kpax.EINVAL
     assert lib.kpax_last_error()

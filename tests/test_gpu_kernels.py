@@ -270,3 +270,25 @@ def test_frontier_compaction_bit_exact(cuda, n, density):
         assert np.array_equal(d_ent[: st["E"]].cpu().numpy().view(np.uint32), o_ent), budget
         assert np.array_equal(d_rep.cpu().numpy()[:n], o_rep), budget
         assert st["E"] == budget or st["E"] == R or st["E"] * st["k"] <= budget
+
+
+def test_bounded_wait_gives_up_and_context_stays_usable(cuda):
+    """A device-side wait that nothing ends (the expansion's look-back wait on a tile that never
+    publishes) gives up after its poll limit: the kernel stores a timeout status and returns, the
+    call reports ETIMEOUT, and the context keeps working (a batch then matches the oracle)."""
+    import time
+
+    import torch
+
+    t0 = time.perf_counter()
+    with pytest.raises(kpax.KpaxError) as e:
+        kpax.test_wait_timeout(1 << 12)
+    assert e.value.status == kpax.ETIMEOUT and "gave up" in str(e.value)
+    assert time.perf_counter() - t0 < 10.0
+    cfg = kpax.preset(kpax.PRESET_DI)
+    obs, _, _ = E.di_scene()
+    par = E.sample_states(cfg.model, 256, 7)
+    draws = E.uniform_draws(256, 8)
+    rows, valid, _, _ = gpu_propagate(torch, cfg, obs, par, draws)
+    orow, oval, *_ = O.propagate(cfg, obs, par, draws)
+    assert np.array_equal(valid, oval) and np.array_equal(bits(rows), bits(orow))
