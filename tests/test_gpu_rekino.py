@@ -55,3 +55,23 @@ def test_quad_rekino_path_is_a_valid_trajectory(cuda):
         x = O.integrate_f64(cfg, a[:12], b[12:], steps, mode=0)
         assert np.all(np.abs(x - b[:12]) <= 1e-4 * np.maximum(np.abs(x), 1.0))
     print({"iters": r.iters, "path_len": r.path_len, "ms": r.ms, "samples": r.expansions})
+
+
+def test_give_up_deadline_stops_every_warp(cuda):
+    """The 6-second give-up of ReKinoLite (ReKinoLite.cu:120-124, 300-313) is a %globaltimer
+    deadline checked every 100 iterations: with a 0.1 ms deadline and a goal no state can reach
+    (outside the workspace, which every propagated state must stay in), every warp stops at its
+    100th iteration — exactly warps x 100 x 32 samples propagated — and the plan ends in
+    milliseconds instead of running its 20000 iterations."""
+    import torch
+
+    cfg = kpax.preset(kpax.PRESET_QUAD)
+    obs, s, g = E.quad_scene()
+    g = g.copy()
+    g[:3] = (500.0, 500.0, 500.0)
+    d_obs = torch.from_numpy(obs).cuda()
+    rk = kpax.ReKinoLite(cfg, num_warps=64, timeout_ms=0.1, max_iterations=20000)
+    r, path = rk.plan(s, g, d_obs.data_ptr(), obs.shape[0])
+    assert r.found == 0 and path.shape[0] == 0
+    assert r.expansions == 64 * 100 * 32, r.expansions
+    assert r.ms < 500.0, r.ms
