@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define KPAX_ABI_VERSION 2
+#define KPAX_ABI_VERSION 3
 
 typedef enum kpax_status {
     KPAX_OK = 0,
@@ -100,7 +100,11 @@ typedef struct kpax_config {
     float prune_goal_bias;          /* h_goalBias_ (0.7, PruneKPAX.cu:36) */
     float prune_exploration_bias;   /* h_explorationBias_ (0.3, PruneKPAX.cu:35) */
     float prune_progress_scale;     /* h_progressScale_ (10, PruneKPAX.cu:34) */
-    int32_t reserved[3];
+    /* 0: a single plan without the learned proposal runs each iteration as one persistent launch
+     * (frontier passes, expansion and scores separated by bounded grid-wide barriers); 1: one launch
+     * per stage (as batches and the learned proposal always do).  Plans are identical either way. */
+    int32_t iteration_kernels;
+    int32_t reserved[2];
 } kpax_config;
 
 /* Result of kpax_plan (the reference exposes these as public fields h_pathToGoal_, h_itr_,
@@ -240,10 +244,14 @@ kpax_status kpax_propagate_batch(const kpax_config* cfg, kpax_env* env, const fl
  * Limits: at most 4096 obstacles, 131072 grid cells and 262144 (cell, obstacle) pairs; larger
  * inputs return KPAX_ECAPACITY with a message.  All calls share that one array and each call
  * overwrites it, so calls whose GPU work overlaps (other streams, other host threads) race; issue
- * them one after another on one stream.  The call synchronises `stream` once, after counting the
- * grid entries.  The first call on a device looks up the array's device address, so make it
- * before any stream capture.  Arguments as kpax_propagate_batch, with the obstacles (n_obs x 6
- * device floats) in place of an environment. */
+ * them one after another on one stream.  A call with obstacles blocks the calling thread once: it
+ * waits for `stream` to finish counting the grid entries and reads the count back to the host, to
+ * check it against the limit.  Set-up: the first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) and keeps it for the life of the process, so make that first call
+ * before any stream capture begins, and do not call the entry on a device again after a
+ * cudaDeviceReset of it.  Batches of any size run the one-pass propagation kernel (no phase
+ * scratch).  Arguments as kpax_propagate_batch, with the obstacles (n_obs x 6 device floats) in
+ * place of an environment. */
 kpax_status kpax_propagate_batch_noalloc(const kpax_config* cfg, const float* d_obstacles,
                                          uint32_t n_obs, const float* d_parents,
                                          const float* d_draws, uint32_t draw_stream, uint32_t n,

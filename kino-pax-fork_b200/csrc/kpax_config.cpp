@@ -292,6 +292,7 @@ kpax_status kpax_config_validate(const kpax_config* c)
                            isfinite(c->prune_goal_bias) && isfinite(c->prune_exploration_bias)),
              "pruning needs a positive progress scale and finite biases");
     KPAX_REQ(c->unroll_iters >= 0 && c->unroll_iters <= 64, "unroll_iters in [0,64]");
+    KPAX_REQ(c->iteration_kernels == 0 || c->iteration_kernels == 1, "iteration_kernels must be 0 or 1");
 #undef KPAX_REQ
     return KPAX_OK;
 }

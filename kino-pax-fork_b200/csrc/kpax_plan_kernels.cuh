@@ -71,7 +71,10 @@ struct alignas(16) Ctl {
     float score_total, pad1[3];
     unsigned long long n_exp, n_valid, n_steps;
     unsigned long long t_begin_ns, t_done_ns;
-    double path_cost;
+    float path_cost, pad2;
+    // k_iterate: device-clock nanoseconds spent in its phases (frontier, expansion, scores), summed
+    // over launches
+    unsigned long long t_front_ns, t_expand_ns, t_score_ns, pad3;
 };
 
 // Everything a kernel needs about one query.
@@ -88,6 +91,8 @@ struct alignas(16) QueryDev {
     unsigned long long* lb;  // look-back status of k_expand, one per block
     float* partials;      // kPartials partial score sums
     uint32_t* sarr;       // arrival counter of k_scores
+    uint32_t* bar;        // grid barrier of k_iterate: arrivals, generation
+    uint32_t* ctas;       // per-CTA repeat sums of k_iterate's frontier phase
     float* path;
     const float* init_goal;  // init row then goal row, S floats each
     // learned proposal (quadrotor queries that enabled it; null otherwise)
@@ -184,7 +189,7 @@ __device__ __forceinline__ uint32_t popcount_range(const uint32_t* __restrict__ 
     uint32_t n = 0;
     const uint64_t w0 = lo >> 5, w1 = (hi - 1) >> 5;
     for(uint64_t w = w0; w <= w1; ++w) {
-        uint32_t m = bits[w];
+        uint32_t m = __ldcg(bits + w);
         if(w == w0) m &= ~0u << (lo & 31);
         if(w == w1) {
             const uint32_t top = (uint32_t)((hi - 1) & 31);
@@ -265,6 +270,8 @@ __global__ void k_begin(const QueryDev* __restrict__ qs, uint32_t plan_base, uin
     z.goal[0] = ig[p.S], z.goal[1] = ig[p.S + 1], z.goal[2] = ig[p.S + 2];
     z.t_begin_ns = globaltimer();
     *ctl = z;
+    sq.bar[0] = 0u;  // arrivals of k_iterate's grid barrier (a plan ended by a timeout may leave some)
+    *sq.sarr = 0u, *sq.farr = 0u;
 }
 
 __device__ __forceinline__ uint32_t resolve_repeat(const KParams& p, const TreeDev& t, const RegDev& rg, uint32_t i,
@@ -446,32 +453,35 @@ __global__ void __launch_bounds__(kFrontierBS) k_frontier_write(const QueryDev* 
     }
 }
 
-// Expansion of the children of one query (blockIdx.y).  Children form look-back tiles of BS
-// consecutive children; a block processes `spt` tiles in grid-stride rounds (tile = round *
-// gridDim.x + blockIdx.x), so every block's round r only waits on tiles of round r or earlier.
+// Shared-memory scratch of the expansion tiles of one block.
+template <int NW>
+struct ExpandSmem {
+    uint32_t excl, ok;
+    uint32_t wn[NW], wv[NW], ws[NW];
+};
+
+// Expansion of a query's children (KPAX.cu:358-439 with 445-502).  Children form look-back tiles
+// of BS consecutive children; this block processes tiles b = first, first + stride, ... (grid-stride
+// rounds), so every tile only waits on tiles of its own round or earlier.  Per child: draws, RK4 with
+// per-step checks and grid queries, R1/R2 ids, counters, frontier mark; accepted children are
+// appended in child order.  Returns false when a look-back wait gave up (the query is then finished
+// with an error).
 template <int M, int BS>
-__global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_expand(const QueryDev* __restrict__ qs, const uint32_t* __restrict__ qidx,
-                                               uint32_t* __restrict__ active)
+__device__ __forceinline__ bool expand_tiles(QueryDev& sq, uint32_t n, uint32_t k, uint32_t first, uint32_t stride,
+                                             uint32_t* __restrict__ active, ExpandSmem<BS / 32>& sm)
 {
     constexpr int SD = ModelDims<M>::SD, CD = ModelDims<M>::CD, S = SD + CD + 1;
     constexpr int NW = BS / 32;
-    __shared__ QueryDev sq;
-    __shared__ uint32_t s_excl, s_ok;
-    __shared__ uint32_t s_wn[NW], s_wv[NW], s_ws[NW];
-    load_query(qs, qidx, sq);
     const KParams& p = sq.p;
     Ctl* ctl = sq.ctl;
-    wait_predecessor();
-    release_successor();
-    if(__syncthreads_or(ctl->done != 0u)) return;  // one decision for the whole block: barriers follow
-    const uint32_t n = ctl->n, k = ctl->k, tree = ctl->tree, iter = ctl->iter, plan = ctl->plan_idx, epoch = ctl->epoch;
+    const uint32_t tree = ctl->tree, iter = ctl->iter, plan = ctl->plan_idx, epoch = ctl->epoch;
     const uint32_t ready = ctl->scores_ready;
     const float total = ctl->score_total;
     const uint32_t ntile = n ? (n + BS - 1) / BS : 1u;
     const TreeDev& t = sq.t;
     const RegDev& rg = sq.rg;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for(uint32_t b = blockIdx.x; b < ntile; b += gridDim.x) {
+    for(uint32_t b = first; b < ntile; b += stride) {
         const uint32_t c = b * BS + threadIdx.x;
         const bool active_child = c < n;
         bool valid = false, next = false;
@@ -479,7 +489,7 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_expand(co
         uint32_t parent = 0;
         int r1v = 0, r2v = 0, steps = 0, steps_done = 0;
         if(active_child) {
-            parent = sq.entries[c / k];
+            parent = __ldcg(sq.entries + c / k);  // written by other CTAs of a fused launch: through L2
             load_state<SD>(t, parent, s);
             const float d_parent = p.prune ? goal_distance(s, ctl->goal) : 0.0f;
             child_draws(p, plan, iter, c, u);
@@ -514,12 +524,12 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_expand(co
         uint32_t wsteps = active_child ? (uint32_t)steps_done : 0u;  // RK4 steps executed (algorithmic work)
 #pragma unroll
         for(int d = 16; d > 0; d >>= 1) wsteps += __shfl_xor_sync(0xffffffffu, wsteps, d);
-        if(lane == 0) s_wn[warp] = __popc(mn), s_wv[warp] = __popc(mv), s_ws[warp] = wsteps;
+        if(lane == 0) sm.wn[warp] = __popc(mn), sm.wv[warp] = __popc(mv), sm.ws[warp] = wsteps;
         __syncthreads();
         if(warp == 0) {
             uint32_t acc = 0, nv = 0;
             unsigned long long ns = 0;
-            for(int w = 0; w < NW; ++w) acc += s_wn[w], nv += s_wv[w], ns += s_ws[w];
+            for(int w = 0; w < NW; ++w) acc += sm.wn[w], nv += sm.wv[w], ns += sm.ws[w];
             uint32_t excl = 0;
             bool ok = true;
             if(b == 0) {
@@ -537,16 +547,16 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_expand(co
                     finish_query(ctl, active);
                 }
                 if(ok && b == ntile - 1) ctl->appended = excl + acc;
-                s_excl = excl;
-                s_ok = ok;
+                sm.excl = excl;
+                sm.ok = ok;
             }
         }
         __syncthreads();
-        const bool block_ok = s_ok != 0u;
+        const bool block_ok = sm.ok != 0u;
         if(next && block_ok) {
             uint32_t wex = 0;  // accepted children of the lower warps of this tile
-            for(int w = 0; w < warp; ++w) wex += s_wn[w];
-            const uint32_t slot = tree + s_excl + wex + rank;
+            for(int w = 0; w < warp; ++w) wex += sm.wn[w];
+            const uint32_t slot = tree + sm.excl + wex + rank;
             if(slot >= p.cap) {
                 atomicOr(&ctl->error, kErrCapacity);
             } else {
@@ -561,44 +571,54 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_expand(co
                 if(d < p.goal_thresh) atomicMin(&ctl->goal_idx, slot);
             }
         }
-        if(!block_ok) return;
-        __syncthreads();  // s_wn / s_excl are rewritten by the next round
+        if(!block_ok) return false;
+        __syncthreads();  // the shared words are rewritten by the next round
     }
+    return true;
+}
+
+// Expansion kernel of a batch: the children of query blockIdx.y (through qidx), tiles in grid-stride
+// rounds over blockIdx.x.
+template <int M, int BS>
+__global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_expand(const QueryDev* __restrict__ qs, const uint32_t* __restrict__ qidx,
+                                               uint32_t* __restrict__ active)
+{
+    __shared__ QueryDev sq;
+    __shared__ ExpandSmem<BS / 32> sm;
+    load_query(qs, qidx, sq);
+    wait_predecessor();
+    release_successor();
+    if(__syncthreads_or(sq.ctl->done != 0u)) return;  // one decision for the whole block: barriers follow
+    expand_tiles<M, BS>(sq, sq.ctl->n, sq.ctl->k, blockIdx.x, gridDim.x, active, sm);
 }
 
 // Region scores (Graph.cu:233-358): one warp per partial sum j; the warp scores groups of 32
 // consecutive regions (g = j, j + 1024, ...: coalesced loads), adds each group by a xor butterfly
-// and the groups in ascending order; the last CTA adds the 1024 partials with a fixed halving
-// tree, so the total (and every normalised score) is bit-identical to the oracle's.  Raw scores
-// are stored (negative = no valid sample) and normalised where they are read (region_score).
-__global__ void __launch_bounds__(kScoreBS) k_scores(const QueryDev* __restrict__ qs, uint32_t* __restrict__ active)
+// and the groups in ascending order; the total is the 1024 partials added by a fixed halving tree,
+// so it (and every normalised score) is bit-identical to the oracle's whichever warps compute the
+// partials.  Raw scores are stored (negative = no valid sample) and normalised where they are read
+// (region_score).  Threads gtid of gsize also copy the iteration's R2 bits into the snapshot;
+// warps wg of nwarps compute partials.
+__device__ __forceinline__ void score_partials(const QueryDev& sq, uint32_t gtid, uint32_t gsize, int wg, int nwarps)
 {
-    __shared__ QueryDev sq;
-    __shared__ float s_part[kPartials];
-    __shared__ uint32_t s_last;
-    load_query(qs, nullptr, sq);
     const KParams& p = sq.p;
     const RegDev& rg = sq.rg;
-    Ctl* ctl = sq.ctl;
-    const int tid = threadIdx.x, lane = tid & 31;
-    wait_predecessor();
-    release_successor();
-    if(ctl->done) return;
-    const uint32_t gtid = blockIdx.x * blockDim.x + tid, gsize = gridDim.x * blockDim.x;
-    for(uint32_t w = gtid; w < p.r2_words; w += gsize) rg.cur[w] = rg.nxt[w];
-    const int nwarps = gridDim.x * (kScoreBS / 32);
+    const int lane = threadIdx.x & 31;
+    for(uint32_t w = gtid; w < p.r2_words; w += gsize) rg.cur[w] = __ldcg(rg.nxt + w);
     const uint32_t ngroups = (p.num_r1 + 31) / 32;  // 32 consecutive regions per group
     const int used = (int)min(ngroups, (uint32_t)kPartials);  // partials at and above `used` stay 0
-    for(int j = blockIdx.x * (kScoreBS / 32) + (tid >> 5); j < used; j += nwarps) {
+    for(int j = wg; j < used; j += nwarps) {
         float part = 0.0f;
         for(uint32_t grp = j; grp < ngroups; grp += kPartials) {
             const int r = 32 * grp + lane;
             float contrib = 0.0f;
             if(r < p.num_r1) {
-                const int nv = rg.valid[r];
+                // counters and R2 bits were updated by atomics of other CTAs (of the same launch in
+                // k_iterate): read through L2
+                const int nv = __ldcg(rg.valid + r);
                 float stored = -1.0f;  // region without valid samples: score 1
                 if(nv > 0) {           // Graph.cu:241-256, coverage from an exact R2 popcount
-                    const int cnt = rg.counter[r];
+                    const int cnt = __ldcg(rg.counter + r);
                     const uint32_t pc = popcount_range(rg.nxt, (uint64_t)r * p.P, (uint64_t)(r + 1) * p.P);
                     const float cov = __fdiv_rn((float)pc, (float)p.P);
                     const float fnv = __fadd_rn(p.eps, (float)nv);
@@ -614,6 +634,61 @@ __global__ void __launch_bounds__(kScoreBS) k_scores(const QueryDev* __restrict_
         }
         if(lane == 0) sq.partials[j] = part;
     }
+}
+
+// Total of the partials by one block (all threads; s_part holds kPartials floats), then the
+// iteration's bookkeeping by thread 0: tree size, fAccept (KPAX.cu:527-528), counters, stop flags.
+__device__ __forceinline__ void score_finish(const QueryDev& sq, float* s_part, uint32_t* __restrict__ active)
+{
+    const KParams& p = sq.p;
+    Ctl* ctl = sq.ctl;
+    const int tid = threadIdx.x;
+    const uint32_t ngroups = (p.num_r1 + 31) / 32;
+    const int used = (int)min(ngroups, (uint32_t)kPartials);
+    // halving tree over the 1024 partials; the levels whose upper halves hold only the zero
+    // partials at and above `used` leave the lower entries unchanged (x + 0 = x), so the tree
+    // starts at the first power of two not below `used` and gives the same total
+    int half = 1;
+    while(half < used) half <<= 1;
+    for(int j = tid; j < half; j += blockDim.x) s_part[j] = j < used ? ((volatile float*)sq.partials)[j] : 0.0f;
+    __syncthreads();
+    for(int s = half / 2; s > 0; s >>= 1) {
+        for(int j = tid; j < s; j += blockDim.x) s_part[j] = __fadd_rn(s_part[j], s_part[j + s]);
+        __syncthreads();
+    }
+    if(tid == 0) {
+        ctl->score_total = s_part[0];
+        ctl->scores_ready = 1u;
+        // the block may hold the control block's line in L1 from earlier in a fused launch, while
+        // other CTAs updated it since: volatile reads
+        const volatile Ctl* vc = ctl;
+        const uint32_t iter = vc->iter, tree_old = vc->tree, tree_new = tree_old + vc->appended;
+        ctl->tree_old = tree_old;
+        ctl->tree = tree_new;
+        const float a = __fsub_rn(1.0f, __fdiv_rn((float)tree_new, (float)p.cap));  // KPAX.cu:527-528
+        const float a2 = __fmul_rn(a, a), a4 = __fmul_rn(a2, a2), a5 = __fmul_rn(a4, a);
+        ctl->faccept = __fmul_rn(__fmul_rn((float)iter, p.eps), a5);
+        ctl->n_exp = vc->n_exp + vc->n;
+        ctl->iters_done = iter;
+        ctl->iter = iter + 1u;
+        ctl->epoch = vc->epoch + 1u;
+        if((vc->goal_idx != kNone && vc->stop_at_goal) || iter >= vc->max_iters) finish_query(ctl, active);
+    }
+}
+
+// The score pass of a batch: query blockIdx.y; the last CTA of a query adds its partials.
+__global__ void __launch_bounds__(kScoreBS) k_scores(const QueryDev* __restrict__ qs, uint32_t* __restrict__ active)
+{
+    __shared__ QueryDev sq;
+    __shared__ float s_part[kPartials];
+    __shared__ uint32_t s_last;
+    load_query(qs, nullptr, sq);
+    const int tid = threadIdx.x;
+    wait_predecessor();
+    release_successor();
+    if(sq.ctl->done) return;
+    score_partials(sq, blockIdx.x * blockDim.x + tid, gridDim.x * blockDim.x, blockIdx.x * (kScoreBS / 32) + (tid >> 5),
+                   gridDim.x * (kScoreBS / 32));
     __threadfence();
     __syncthreads();
     if(gridDim.x > 1) {  // the last CTA to arrive adds the partials
@@ -621,33 +696,226 @@ __global__ void __launch_bounds__(kScoreBS) k_scores(const QueryDev* __restrict_
         __syncthreads();
         if(!s_last) return;
         __threadfence();
+        if(tid == 0) *sq.sarr = 0u;
     }
-    // halving tree over the 1024 partials; the levels whose upper halves hold only the zero
-    // partials at and above `used` leave the lower entries unchanged (x + 0 = x), so the tree
-    // starts at the first power of two not below `used` and gives the same total
-    int half = 1;
-    while(half < used) half <<= 1;
-    for(int j = tid; j < half; j += kScoreBS) s_part[j] = j < used ? ((volatile float*)sq.partials)[j] : 0.0f;
+    score_finish(sq, s_part, active);
+}
+
+// ---------------------------------------------------------------- fused iteration (single query)
+// k_iterate runs one whole iteration in one launch: frontier count, entry list, expansion and
+// region scores, separated by grid-wide barriers.  Every CTA must be resident (the host sizes the
+// grid by the occupancy of the kernel), every barrier is bounded, and each phase computes exactly
+// what the corresponding per-stage kernel computes (same per-node, per-child and per-region
+// arithmetic, same partial sums), so plans are bit-identical to the per-stage path.
+
+constexpr int kIterMaxCTAs = 1024;  // CTAs of a k_iterate launch
+constexpr int kIterBatch = 8;       // nodes per thread whose loads are issued together
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p)
+{
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Grid-wide barrier of a launch whose CTAs are all resident: bar[0] counts arrivals, bar[1] is the
+// generation.  The last CTA to arrive resets the count and advances the generation; the others poll
+// the generation they read before arriving.  Bounded: returns false after spin_limit polls.
+__device__ __forceinline__ bool grid_barrier(uint32_t* bar, uint32_t nblocks, uint32_t* s_flag,
+                                             uint32_t spin_limit = kSpinLimit)
+{
     __syncthreads();
-    for(int s = half / 2; s > 0; s >>= 1) {
-        for(int j = tid; j < s; j += kScoreBS) s_part[j] = __fadd_rn(s_part[j], s_part[j + s]);
-        __syncthreads();
+    if(threadIdx.x == 0) {
+        const uint32_t gen = ld_acquire(bar + 1);
+        __threadfence();
+        bool ok = true;
+        if(atomicAdd(bar, 1u) == nblocks - 1u) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            uint32_t spins = 0;
+            while(ld_acquire(bar + 1) == gen) {
+                if(++spins > spin_limit) {
+                    ok = false;
+                    break;
+                }
+                if(spins > 16) __nanosleep(32);
+            }
+        }
+        __threadfence();
+        *s_flag = ok ? 1u : 0u;
     }
+    __syncthreads();
+    return *s_flag != 0u;
+}
+
+// Sum of v over the block (all threads call it; s_warp holds one word per warp).
+template <int NW>
+__device__ __forceinline__ uint32_t block_sum(uint32_t v, uint32_t* s_warp)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for(int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xffffffffu, v, d);
+    __syncthreads();
+    if(lane == 0) s_warp[warp] = v;
+    __syncthreads();
+    uint32_t t = 0;
+    for(int w = 0; w < NW; ++w) t += s_warp[w];
+    return t;
+}
+
+template <int M, int BS>
+__global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_iterate(const QueryDev* __restrict__ qs,
+                                                                             uint32_t* __restrict__ active)
+{
+    constexpr int NW = BS / 32;
+    __shared__ QueryDev sq;
+    __shared__ ExpandSmem<NW> sm;
+    __shared__ uint32_t s_flag, s_last;
+    __shared__ uint32_t s_warp[NW], s_warp2[NW];
+    __shared__ float s_part[kPartials];
+    load_query(qs, nullptr, sq);
+    const KParams& p = sq.p;
+    const TreeDev& t = sq.t;
+    const RegDev& rg = sq.rg;
+    Ctl* ctl = sq.ctl;
+    const uint32_t G = gridDim.x, cb = blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    wait_predecessor();
+    if(__syncthreads_or(ctl->done != 0u)) return;  // one decision for the whole grid: barriers follow
+    const unsigned long long t0 = globaltimer();
+    const uint32_t tree = ctl->tree, tree_old = ctl->tree_old, iter = ctl->iter, plan = ctl->plan_idx;
+    const uint32_t ready = ctl->scores_ready;
+    const float fa = ctl->faccept, total = ctl->score_total;
+
+    // ---- frontier count (k_frontier_count): re-activation of the previous iteration
+    // (KPAX.cu:505-517) and repeats of its new nodes (476-479) over this thread's contiguous nodes
+    const uint32_t per_cta = (tree + G - 1) / G, per_thr = (per_cta + BS - 1) / BS;
+    const uint32_t c_lo = min(tree, cb * per_cta), c_hi = min(tree, c_lo + per_cta);
+    const uint32_t lo = min(c_hi, c_lo + (uint32_t)tid * per_thr), hi = min(c_hi, lo + per_thr);
+    uint32_t sum = 0;
+    for(uint32_t i0 = lo; i0 < hi; i0 += kIterBatch) {
+        uint32_t r0[kIterBatch];
+        int32_t reg[kIterBatch], nv[kIterBatch];
+        float raw[kIterBatch];
+#pragma unroll
+        for(int j = 0; j < kIterBatch; ++j) {  // each node's byte and region id, then its region's
+            const uint32_t i = i0 + j;         // score and valid count: two rounds of loads per batch
+            r0[j] = i < hi ? (uint32_t)t.rep[i] : 0u;
+            reg[j] = i < hi ? t.r1[i] : 0;
+        }
+#pragma unroll
+        for(int j = 0; j < kIterBatch; ++j) raw[j] = rg.score[reg[j]], nv[j] = rg.valid[reg[j]];
+#pragma unroll
+        for(int j = 0; j < kIterBatch; ++j) {
+            const uint32_t i = i0 + j;
+            if(i >= hi) continue;
+            uint32_t r = r0[j];
+            if(r == 0u) {
+                if(i < tree_old) {
+                    const float sc = region_score(raw[j], total, ready, p.eps);
+                    if(reactivate_draw(p, plan, iter - 1u, i) <= __fadd_rn(sc, fa)) r = 1u;
+                }
+            } else if(r == kPending) {
+                r = nv[j] < p.sparse_thr ? p.sparse_repeat : 1u;
+            }
+            if(r != r0[j]) t.rep[i] = (uint8_t)r;
+            sum += r;
+        }
+    }
+    // this thread's exclusive prefix inside the CTA, and the CTA's sum
+    uint32_t x = sum;
+#pragma unroll
+    for(int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+        if(lane >= d) x += y;
+    }
+    if(lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    uint32_t wex = 0, cta_sum = 0;
+    for(int w = 0; w < NW; ++w) {
+        wex += w < warp ? s_warp[w] : 0u;
+        cta_sum += s_warp[w];
+    }
+    const uint32_t thr_excl = wex + x - sum;
+    if(tid == 0) sq.ctas[cb] = cta_sum;
+    if(!grid_barrier(sq.bar, G, &s_flag)) {
+        if(tid == 0) atomicOr(&ctl->error, kErrTimeout), finish_query(ctl, active);
+        return;
+    }
+    release_successor();  // every CTA is resident now
+
+    // ---- budget (KPAX.cu:323-350) from the CTA sums, then the entry list (k_frontier_write)
+    uint32_t tot = 0, pre = 0;
+    for(uint32_t j = tid; j < G; j += BS) {
+        const uint32_t v = __ldcg(sq.ctas + j);
+        tot += v;
+        pre += j < cb ? v : 0u;
+    }
+    const uint64_t R = block_sum<NW>(tot, s_warp);
+    const uint32_t a_cta = block_sum<NW>(pre, s_warp2);
+    const uint32_t B = min(p.budget, p.cap - tree);
+    uint32_t k = p.per_entry, E = 0, n = 0;
+    if(B != 0 && R) {
+        if(R * k > B) {
+            k = (uint32_t)(B / R);
+            if(k == 0) k = 1;
+        }
+        E = (uint32_t)(R < (uint64_t)(B / k) ? R : (uint64_t)(B / k));
+        n = E * k;
+    }
+    if(cb == 0 && tid == 0) {
+        ctl->R = (uint32_t)R;
+        ctl->k = k, ctl->E = E, ctl->n = n;
+        if(B == 0) {
+            ctl->full = 1u;
+            finish_query(ctl, active);
+        }
+    }
+    if(B == 0) return;  // every CTA decides alike
+    if(E) {
+        uint64_t a = (uint64_t)a_cta + thr_excl;  // node i owns virtual entries [a, a + rep)
+        for(uint32_t i = lo; i < hi; ++i) {
+            const uint32_t cnt = t.rep[i];
+            if(!cnt) continue;
+            const uint64_t bnd = a + cnt;
+            const uint64_t elo = (a * E + R - 1) / R, ehi = (bnd * E + R - 1) / R;
+            for(uint64_t e = elo; e < ehi; ++e) sq.entries[e] = i;
+            if(elo < ehi) t.rep[i] = 0;
+            a = bnd;
+        }
+    }
+    if(!grid_barrier(sq.bar, G, &s_flag)) {
+        if(tid == 0) atomicOr(&ctl->error, kErrTimeout), finish_query(ctl, active);
+        return;
+    }
+    const unsigned long long t2 = globaltimer();
+
+    // ---- expansion (k_expand); a CTA whose look-back wait gave up has finished the query with an
+    // error and still takes part in the barrier
+    expand_tiles<M, BS>(sq, n, k, cb, G, active, sm);
+    if(!grid_barrier(sq.bar, G, &s_flag)) {
+        if(tid == 0) atomicOr(&ctl->error, kErrTimeout), finish_query(ctl, active);
+        return;
+    }
+    const unsigned long long t3 = globaltimer();
+
+    // ---- region scores (k_scores); the last CTA to finish adds the partials and closes the iteration
+    score_partials(sq, cb * BS + tid, G * BS, (int)(cb * NW) + warp, (int)(G * NW));
+    __threadfence();
+    __syncthreads();
+    if(tid == 0) s_last = atomicAdd(sq.sarr, 1u) == G - 1u;
+    __syncthreads();
+    if(!s_last) return;
+    __threadfence();
+    if(tid == 0) *sq.sarr = 0u;
+    score_finish(sq, s_part, active);
     if(tid == 0) {
-        if(gridDim.x > 1) *sq.sarr = 0u;
-        ctl->score_total = s_part[0];
-        ctl->scores_ready = 1u;
-        const uint32_t iter = ctl->iter, tree_old = ctl->tree, tree_new = tree_old + ctl->appended;
-        ctl->tree_old = tree_old;
-        ctl->tree = tree_new;
-        const float a = __fsub_rn(1.0f, __fdiv_rn((float)tree_new, (float)p.cap));  // KPAX.cu:527-528
-        const float a2 = __fmul_rn(a, a), a4 = __fmul_rn(a2, a2), a5 = __fmul_rn(a4, a);
-        ctl->faccept = __fmul_rn(__fmul_rn((float)iter, p.eps), a5);
-        ctl->n_exp += ctl->n;
-        ctl->iters_done = iter;
-        ctl->iter = iter + 1u;
-        ctl->epoch = ctl->epoch + 1u;
-        if((ctl->goal_idx != kNone && ctl->stop_at_goal) || iter >= ctl->max_iters) finish_query(ctl, active);
+        const unsigned long long t4 = globaltimer();
+        ctl->t_front_ns += t2 - t0;
+        ctl->t_expand_ns += t3 - t2;
+        ctl->t_score_ns += t4 - t3;
     }
 }
 
@@ -711,7 +979,7 @@ __global__ void k_path(const QueryDev* __restrict__ qs)
     Ctl* ctl = sq.ctl;
     int32_t node = ctl->goal_idx == kNone ? -1 : (int32_t)ctl->goal_idx;
     uint32_t len = 0;
-    double cost = 0.0;
+    float cost = 0.0f;  // FP32 like every planner quantity, summed goal to root
     while(node >= 0 && len < sq.path_rows) {
         float s[12] = {0};
         if(p.sd == 12) load_state<12>(t, (uint32_t)node, s);
@@ -723,7 +991,7 @@ __global__ void k_path(const QueryDev* __restrict__ qs)
         for(int k = 0; k < p.cd; ++k) dst[p.sd + k] = cv[k];
         dst[p.S - 1] = t.dur[node];
         const int32_t par = t.parent[node];
-        if(par >= 0) cost += (double)t.dur[node];
+        if(par >= 0) cost = __fadd_rn(cost, t.dur[node]);
         ++len;
         node = par;
     }

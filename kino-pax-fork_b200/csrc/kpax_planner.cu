@@ -67,6 +67,29 @@ void launch_expand(int bs, dim3 grid, cudaStream_t s, const QueryDev* dq, const 
     }
 }
 
+// The fused iteration kernel at one of its block sizes.
+template <int M>
+void* iterate_kernel(int bs)
+{
+    switch(bs) {
+        case 128: return (void*)k_iterate<M, 128>;
+        case 256: return (void*)k_iterate<M, 256>;
+        case 512: return (void*)k_iterate<M, 512>;
+        default: return (void*)k_iterate<M, kExpandBS>;
+    }
+}
+
+template <int M>
+void launch_iterate(int bs, uint32_t gx, cudaStream_t s, const QueryDev* dq, uint32_t* active)
+{
+    switch(bs) {
+        case 128: launch_chained(k_iterate<M, 128>, dim3(gx), 128, 0, s, dq, active); break;
+        case 256: launch_chained(k_iterate<M, 256>, dim3(gx), 256, 0, s, dq, active); break;
+        case 512: launch_chained(k_iterate<M, 512>, dim3(gx), 512, 0, s, dq, active); break;
+        default: launch_chained(k_iterate<M, kExpandBS>, dim3(gx), kExpandBS, 0, s, dq, active); break;
+    }
+}
+
 struct PlanBatch {
     uint32_t nq = 0;
     std::vector<kpax_config> cfg;
@@ -82,6 +105,8 @@ struct PlanBatch {
     uint32_t expand_gx[3] = {0, 0, 0};
     int expand_bs[3] = {kExpandBS, kExpandBS, kExpandBS};  // block size per model group (its first query's)
     uint32_t gx_front = 1, gx_score = 1;
+    bool fused = false;      // single query without the proposal: one k_iterate launch per iteration
+    uint32_t gx_iter = 0;    // its CTAs (all resident), 0 when the kernel cannot be used
     Ctl* d_ctl = nullptr;
     Ctl* h_ctl = nullptr;
     uint32_t* d_active = nullptr;
@@ -153,6 +178,8 @@ struct PlanBatch {
                 d.partials = cv.take<float>(kPartials);
                 d.farr = cv.take<uint32_t>(1);
                 d.sarr = cv.take<uint32_t>(1);
+                d.bar = cv.take<uint32_t>(2);
+                d.ctas = cv.take<uint32_t>(kIterMaxCTAs);
                 d.path_rows = cfg[q].max_iter + 2;
                 path_off[q] = prow;
                 prow += d.path_rows;
@@ -217,12 +244,26 @@ struct PlanBatch {
         const uint32_t groups0 = ((uint32_t)prm[0].num_r1 + 31) / 32;
         gx_score = n == 1 ? std::min<uint32_t>(kScoreCTAs, std::max<uint32_t>(1, (groups0 + 7) / 8))
                           : std::max<uint32_t>(1, 1024 / n);
+        if(n == 1) {  // the fused iteration: as many CTAs as the expansion wants and can stay resident
+            int dev = 0, sms = 148, per_sm = 0;
+            KPAX_CUDA(cudaGetDevice(&dev));
+            KPAX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            const int m = prm[0].model - 1, bs = expand_bs[m];
+            void* fn = m == 0 ? iterate_kernel<KPAX_MODEL_DOUBLE_INTEGRATOR>(bs)
+                              : m == 1 ? iterate_kernel<KPAX_MODEL_DUBINS_AIRPLANE>(bs) : iterate_kernel<KPAX_MODEL_QUADROTOR>(bs);
+            KPAX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, bs, 0));
+            const uint32_t resident = (uint32_t)std::max(per_sm, 0) * (uint32_t)sms;
+            gx_iter = std::min<uint32_t>(std::min<uint32_t>(expand_gx[m], resident), (uint32_t)kIterMaxCTAs);
+        }
+        update_fused();
         // control blocks, counters and arrival flags start at zero; no node is in a frontier
         KPAX_CUDA(cudaMemsetAsync(pool, 0, region_lo, stream));
         KPAX_CUDA(cudaMemsetAsync(d_ctl, 0, sizeof(Ctl) * n, stream));
         KPAX_CUDA(cudaStreamSynchronize(stream));
         return KPAX_OK;
     }
+
+    void update_fused() { fused = nq == 1 && gx_iter > 0 && cfg[0].iteration_kernels == 0 && n_learned == 0; }
 
     void release()
     {
@@ -288,6 +329,14 @@ struct PlanBatch {
     void launch_iteration(cudaEvent_t* ev = nullptr, bool split = true)
     {
         if(ev) cudaEventRecord(ev[0], stream);
+        if(fused) {  // one launch: its phase times come from the device clock (Ctl::t_*_ns)
+            const int m = prm[0].model - 1;
+            if(m == 0) launch_iterate<KPAX_MODEL_DOUBLE_INTEGRATOR>(expand_bs[m], gx_iter, stream, dq, d_active);
+            else if(m == 1) launch_iterate<KPAX_MODEL_DUBINS_AIRPLANE>(expand_bs[m], gx_iter, stream, dq, d_active);
+            else launch_iterate<KPAX_MODEL_QUADROTOR>(expand_bs[m], gx_iter, stream, dq, d_active);
+            if(ev) cudaEventRecord(ev[3], stream);
+            return;
+        }
         launch_chained(k_frontier_count, dim3(gx_front, nq), kFrontierBS, 0, stream, dq, d_active);
         launch_chained(k_frontier_write, dim3(gx_front, nq), kFrontierBS, 0, stream, dq);
         if(ev && split) cudaEventRecord(ev[1], stream);
@@ -373,6 +422,7 @@ struct PlanBatch {
                     if(st != KPAX_OK) return st;
                 }
         }
+        update_fused();
         kpax_status st = upload_descriptors();
         if(st != KPAX_OK) return st;
         KPAX_CUDA(cudaStreamSynchronize(stream));
@@ -381,6 +431,7 @@ struct PlanBatch {
 
     uint64_t kernels_per_iteration() const
     {
+        if(fused) return 1;
         uint64_t k = n_learned ? 4 : 3;  // two frontier passes, the score pass, the proposal pass
         for(int m = 0; m < 3; ++m) k += groups[m].empty() ? 0 : 1;
         return k;
@@ -556,10 +607,19 @@ struct PlanBatch {
             count_launch(kernels_per_iteration());
         }
         KPAX_CUDA(cudaStreamSynchronize(stream));
+        Ctl c1 = {};
+        if(fused) {
+            KPAX_CUDA(cudaMemcpyAsync(&c1, d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, stream));
+            KPAX_CUDA(cudaStreamSynchronize(stream));
+        }
         for(uint32_t i = 0; i < n; ++i) {
             float a = 0, b = 0, d = 0, t = 0;
             cudaEvent_t* e = &tev[4 * (size_t)i];
-            if(split) {
+            if(fused && split) {  // phase times from the device clock, averaged over the n iterations
+                a = (float)((c1.t_front_ns - c0[0].t_front_ns) * 1e-6 / n);
+                b = (float)((c1.t_expand_ns - c0[0].t_expand_ns) * 1e-6 / n);
+                d = (float)((c1.t_score_ns - c0[0].t_score_ns) * 1e-6 / n);
+            } else if(split) {
                 KPAX_CUDA(cudaEventElapsedTime(&a, e[0], e[1]));
                 KPAX_CUDA(cudaEventElapsedTime(&b, e[1], e[2]));
                 KPAX_CUDA(cudaEventElapsedTime(&d, e[2], e[3]));

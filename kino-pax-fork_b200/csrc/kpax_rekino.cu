@@ -324,7 +324,7 @@ static kpax_status rekino_plan_body(kpax_rekino* r, const float* h_init, const f
                                   cudaMemcpyDeviceToHost, r->stream));
         KPAX_CUDA(cudaStreamSynchronize(r->stream));
         r->h_path.assign(rows.size(), 0.0f);  // goal node first, start state last
-        double cost = 0.0;
+        float cost = 0.0f;  // FP32, goal to root, as the planner's path walk
         for(int i = 0; i <= len; ++i) {
             memcpy(r->h_path.data() + (size_t)i * S, rows.data() + (size_t)(len - i) * S, sizeof(float) * S);
             if(i < len) cost += rows[(size_t)(len - i) * S + S - 1];

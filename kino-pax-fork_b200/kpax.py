@@ -17,7 +17,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libkpax.so"
-ABI_VERSION = 2  # KPAX_ABI_VERSION of include/kpax.h this binding was written for
+ABI_VERSION = 3  # KPAX_ABI_VERSION of include/kpax.h this binding was written for
 
 OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, ECAPACITY, ENOTFOUND = range(7)
 MODEL_DOUBLE_INTEGRATOR, MODEL_DUBINS_AIRPLANE, MODEL_QUADROTOR = 1, 2, 3
@@ -76,7 +76,8 @@ class Config(ctypes.Structure):
         ("prune_goal_bias", ctypes.c_float),
         ("prune_exploration_bias", ctypes.c_float),
         ("prune_progress_scale", ctypes.c_float),
-        ("reserved", ctypes.c_int32 * 3),
+        ("iteration_kernels", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 2),
     ]
 
     @property
@@ -202,11 +203,16 @@ def load(path: os.PathLike | None = None) -> ctypes.CDLL:
     if not p.exists():
         raise ImportError(f"{p} is missing: build it with `make -C {HERE}` (no CPU fallback exists)")
     lib = ctypes.CDLL(str(p))
+    # the version first: a library of another version may lack some of the entries bound below
+    ver = getattr(lib, "kpax_abi_version", None)
+    if ver is None:
+        raise ImportError(f"{p} exports no kpax_abi_version: rebuild it")
+    ver.restype, ver.argtypes = ctypes.c_int32, []
+    if ver() != ABI_VERSION:
+        raise ImportError(f"{p} has ABI version {ver()}, this binding expects {ABI_VERSION}: rebuild it")
     for name, (res, args) in _SIGNATURES.items():
         fn = getattr(lib, name)
         fn.restype, fn.argtypes = res, args
-    if lib.kpax_abi_version() != ABI_VERSION:
-        raise ImportError(f"{p} has ABI version {lib.kpax_abi_version()}, this binding expects {ABI_VERSION}: rebuild it")
     if path is None:
         _lib = lib
     return lib

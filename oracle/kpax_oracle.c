@@ -878,7 +878,7 @@ int ko_plan(const kpax_config* cfg, const float* init, const float* goal, const 
         if(found) {
             int32_t node = (int32_t)goal_idx;
             uint32_t len = 0;
-            double pc = 0.0;
+            float pc = 0.0f;  /* FP32, goal to root, as the planner's path walk */
             while(node != -1) {
                 if(out->path) memcpy(out->path + (size_t)len * S, rows + (size_t)node * S, sizeof(float) * S);
                 if(parent[node] != -1) pc += rows[(size_t)node * S + S - 1];

@@ -241,6 +241,38 @@ def layer_bf16(h_in: np.ndarray, W: np.ndarray, b: np.ndarray, act: bool):
     return (silu(z.astype(np.float64)).astype(np.float32) if act else z), z
 
 
+def ulp_bf16(v: np.ndarray) -> np.ndarray:
+    """One BF16 unit in the last place at |v| (8 significant bits)."""
+    e = np.floor(np.log2(np.maximum(np.abs(v), 1e-30)))
+    return 2.0 ** (e - 7)
+
+
+def tc_layer_violation(w: np.ndarray, x: np.ndarray, h1: np.ndarray, h2: np.ndarray, out: np.ndarray) -> dict:
+    """Teacher-forced bounds of the tensor-core pass, each layer fed the pass's own previous layer.
+
+    Hidden layers: BF16 activations within one BF16 ulp of the emulation, plus the error of the
+    kernel's SiLU (h + h tanh(h), h = z / 2, tanh in BF16: |error| < 2^-8 |z|), plus the FP32
+    accumulation error 1e-6 * sum |terms|; their mean difference at most half an ulp.  Outputs:
+    FP32 sums of exact BF16 products within 1e-5 of the terms' magnitude.  Returns the largest
+    excess over each bound (<= 0 everywhere when the pass is within them)."""
+    W1, b1, W2, b2, W3, b3 = unpack(np.asarray(w, np.float32))
+    res = {}
+    for name, h_in, W, b, h_gpu in (("h1", x, W1, b1, h1), ("h2", h1, W2, b2, h2)):
+        act, z = layer_bf16(h_in, W, b, act=True)
+        want = bf16(act)
+        bound = np.abs(bf16(h_in).astype(np.float64)) @ np.abs(bf16(W).astype(np.float64)).T
+        diff = np.abs(np.asarray(h_gpu, np.float64) - want)
+        tol = ulp_bf16(want) * 1.01 + 2.0 ** -8 * np.abs(z) + 1e-6 * bound
+        res[name] = float((diff - tol).max())
+        res[name + "_mean"] = float(np.mean(diff) - 0.5 * np.mean(ulp_bf16(want)))
+    z = bf16(h2).astype(np.float64) @ bf16(W3).astype(np.float64).T
+    bound = np.abs(bf16(h2).astype(np.float64)) @ np.abs(bf16(W3).astype(np.float64)).T
+    want = (z + b3)[:, :OUT]
+    tol = 1e-5 * bound[:, :OUT] + 1e-5 * np.abs(b3[:OUT]) + 1e-6
+    res["out"] = float((np.abs(np.asarray(out, np.float64)[:, :OUT] - want) - tol).max())
+    return res
+
+
 def mixture_parts(o: np.ndarray):
     """Softmax weights (n x 8), means and sigmas (n x 8 x 5) of rows of outputs (float64)."""
     o = np.asarray(o, np.float64)

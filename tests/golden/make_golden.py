@@ -13,6 +13,7 @@ the brute-force propagateAndCheck*, and r1/r2 from getRegion/getSubRegion of the
 quad_<scene>.npz do the same for the quadrotor in the reference's own obstacle files
 (include/config/obstacles/<scene>/obstacles.csv, read with the reference's CSV format).
 """
+import os
 import sys
 from pathlib import Path
 
@@ -26,7 +27,9 @@ import kpax_envs as E  # noqa: E402
 import oracle as O  # noqa: E402
 
 N = 512
-REF_SCENES = Path("/root/reference/include/config/obstacles")
+# the reference tree: $KPAX_REFERENCE_ROOT, else a `reference` directory beside the repository
+REF_ROOT = Path(os.environ.get("KPAX_REFERENCE_ROOT", ROOT.parent / "reference"))
+REF_SCENES = REF_ROOT / "include" / "config" / "obstacles"
 QUAD_SCENES = ("quadTrees", "quadHouse", "quadPillars")
 
 

@@ -30,7 +30,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_abi_version():
-    assert kpax.load().kpax_abi_version() == kpax.ABI_VERSION == 2
+    assert kpax.load().kpax_abi_version() == kpax.ABI_VERSION == 3
 
 
 @pytest.mark.parametrize("which", [kpax.PRESET_DI, kpax.PRESET_DUBINS, kpax.PRESET_QUAD, kpax.PRESET_QUAD_REF])

@@ -60,6 +60,27 @@ def test_noalloc_matches_regular_entry_on_two_calls_in_a_row(cuda):
         assert 0.05 < valid.mean() < 0.95
 
 
+def test_noalloc_matches_phased_regular_entry_on_a_large_batch(cuda):
+    """From 2^18 segments on, the regular entry runs the phased kernels (head, middle, tail with
+    survivor lists in the environment's scratch) while the allocation-free entry keeps the
+    one-pass kernel: both must give the same rows, verdicts and step counts."""
+    import torch
+
+    cfg = kpax.preset(kpax.PRESET_DUBINS)
+    obs, _, _ = E.dubins_scene()
+    n = (1 << 18) + 4099  # above the phased threshold, ragged last block
+    par = E.sample_states(cfg.model, n, 23, cfg.v_min, cfg.v_max)
+    d_par = torch.from_numpy(par).cuda()
+    for call in range(2):
+        want_rows, want_valid, want_steps = _regular(torch, cfg, obs, d_par, n, 60 + call)
+        rows, valid, steps = _noalloc(torch, cfg, obs, d_par, n, 60 + call)
+        assert np.array_equal(valid, want_valid), f"call {call}: validity differs"
+        assert np.array_equal(steps, want_steps), f"call {call}: executed steps differ"
+        err = np.abs(rows.astype(np.float64) - want_rows) / np.maximum(np.abs(want_rows), 1.0)
+        assert float(err.max()) <= REL_TOL, f"call {call}: max relative error {float(err.max())}"
+        assert 0.05 < valid.mean() < 0.95
+
+
 def test_noalloc_rejects_inputs_beyond_its_limits(cuda):
     import torch
 
