@@ -446,6 +446,87 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def query_outcomes(pl, queries: np.ndarray, obs: np.ndarray) -> dict:
+    """Whole plans of a query set (rows: start xyz, goal xyz) through kpax_plan_host from host
+    buffers: success (goal reached), time to solution (host clock of the call), path costs."""
+    S = pl.sample_dim
+    tts, all_ms, costs, found = [], [], [], 0
+    valid, secs = 0, 0.0
+    for q in queries:
+        st, gl = np.zeros(S, np.float32), np.zeros(S, np.float32)
+        st[:3], gl[:3] = q[:3], q[3:6]
+        t0 = time.perf_counter()
+        r = pl.plan_host(st, gl, obs)
+        dt = 1000.0 * (time.perf_counter() - t0)
+        all_ms.append(dt if r.found else float("inf"))
+        valid += r.valid_expansions
+        secs += dt / 1000.0
+        if r.found:
+            found += 1
+            tts.append(dt)
+            costs.append(float(r.path_cost))
+    n = len(queries)
+    return {"queries": n, "success_rate": found / max(n, 1),
+            "tts_ms_p50": float(np.percentile(tts, 50)) if tts else None,
+            "tts_ms_p95": float(np.percentile(tts, 95)) if tts else None,
+            "tts_ms_p50_all": float(np.percentile(all_ms, 50)) if n else None,
+            "tts_ms_p95_all": float(np.percentile(all_ms, 95)) if n else None,
+            "path_cost_median": float(np.median(costs)) if costs else None,
+            "valid_expansions_per_s": valid / secs if secs > 0 else None}
+
+
+def reference_cuda_leg(cfg, obs, start, goal, queries, args) -> dict:
+    """The reference's own CUDA planner (KPAX::plan compiled unmodified for sm_100a, run as a
+    subprocess by oracle/refcuda) on this workload at the reference's duration draw (steps
+    1 + (int)(u * 25)), beside this library at the same configuration: whole plans of the fixed pair
+    (valid expansions per second of plan time), the rate of its large iterations, and the outcomes
+    of the query set."""
+    sys.path.insert(0, str(ROOT / "oracle" / "refcuda"))
+    import refcuda
+
+    pair = [[*start[:3], *goal[:3]]]
+    res = refcuda.run("quad_c2", obs, pair, iteration_cap=cfg.max_iter, repeats=args.ref_cuda_plans, timeout_s=300)
+    summ = refcuda.summarise(res)
+    if "unavailable" in summ:
+        return summ
+    out = {"value": summ["value"], "unit": UNIT, "kind": "reference CUDA build: KPAX::plan from its own sources, sm_100a",
+           "config": "12D quadrotor, building scene, h 0.02 s, steps 1 + (int)(u * 25) (the reference's draw), "
+                     "Zc in [0, 2g], torques in [-0.1, 0.1], tree capacity 2^20, 300 iterations",
+           "plans": summ["plans"], "iterations": summ["iterations"], "capacity_stops": summ["capacity_stops"],
+           "children": summ["children"], "valid": summ["valid"], "seconds": summ["seconds"], "steady": summ["steady"],
+           "timing": "host clock around KPAX::plan, less the harness's own check before each iteration"}
+    # this library at the same configuration (drawn steps), the same plans through kpax_plan
+    c = cfg.copy()
+    c.fixed_steps = 0
+    import torch
+
+    d_obs = torch.from_numpy(obs).cuda()
+    pl = kpax.KPAX(c)
+    pl.plan(start, goal, d_obs.data_ptr(), obs.shape[0])  # warm-up (graph capture)
+    v, t = 0, 0.0
+    for _ in range(args.ref_cuda_plans):
+        t0 = time.perf_counter()
+        r = pl.plan(start, goal, d_obs.data_ptr(), obs.shape[0])
+        t += time.perf_counter() - t0
+        v += r.valid_expansions
+    out["ours_same_config"] = {"value": v / t if t > 0 else None, "unit": UNIT, "plans": args.ref_cuda_plans,
+                               "note": "kpax_plan with the reference's duration draw, 2^16 children per iteration, "
+                                       "host clock around the call"}
+    # plan outcomes on the query set, both sides at that configuration
+    if len(queries):
+        rq = refcuda.summarise(refcuda.run("quad_c2", obs, queries, iteration_cap=cfg.max_iter, repeats=1, timeout_s=300))
+        if "unavailable" not in rq:
+            tts = rq["tts_ms"]
+            out["query_set"] = {"queries": rq["plans"], "success_rate": rq["success_rate"],
+                                "tts_ms_p50": float(np.percentile(tts, 50)) if tts else None,
+                                "tts_ms_p95": float(np.percentile(tts, 95)) if tts else None,
+                                "path_cost_median": float(np.median(rq["path_costs"])) if rq["path_costs"] else None,
+                                "capacity_stops": rq["capacity_stops"]}
+        out["ours_same_config"]["query_set"] = query_outcomes(pl, queries, obs)
+    pl.close()
+    return out
+
+
 def run_ours(args) -> None:
     import torch
 
@@ -482,6 +563,9 @@ def run_ours(args) -> None:
     with Clocks(local) as clk:
         # whole iterations, events only between them: the kernels overlap their launches as in a plan
         times, tot = pl.iterate_timed(args.steps, FLUSH_BYTES, split=False)
+        torch.cuda.synchronize()
+        # the FP32 roofline's denominator: an FMA-chain kernel on the same GPU and clocks
+        fp32_peak = max(kpax.fp32_peak(1 << 16)[0] for _ in range(3))
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -538,14 +622,16 @@ def run_ours(args) -> None:
     flops = tot_split["steps"] * FLOP_PER_STEP[cfg.model]
     achieved = flops / t_exp / 1e12
     sm_mhz = peaks.get("sm_max_mhz", 1965.0)
-    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    nominal = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
     roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                 "traffic": EXPAND_DRAM_BYTES.get(cfg.model), "kernel": "k_expand",
                 "traffic_note": "DRAM bytes read + written by one steady-state 2^16-child k_expand launch of this "
                                 "workload in an ncu capture (summary under profiles/); the tree, regions and grid are "
                                 "L2-resident, so traffic is far below the bytes the kernel touches",
-                "peak_note": "nominal FP32: 148 SM x 128 lanes x 2 FLOP x clocks.max.sm (no measured FP32 peak in "
-                             "MEASURED_PEAKS.json)",
+                "peak_note": "measured: kpax_fp32_peak (8 independent FMA chains per thread, 2048 threads per SM, "
+                             "CUDA events) on this GPU inside the clock-sampling window; MEASURED_PEAKS.json has no "
+                             "FP32 figure",
+                "nominal_peak": nominal,
                 "work": f"{tot_split['steps']} RK4 steps x {FLOP_PER_STEP[cfg.model]} FLOP over {args.steps} launches",
                 "expand_ms_per_launch": 1000 * t_exp / args.steps,
                 "latency_floor_ms": chain_floor_ms,
@@ -577,7 +663,19 @@ def run_ours(args) -> None:
                    "per plan; plan-level success and time to solution over seeded query sets are the learned and "
                    "batch workloads' figures"}
 
+    if args.query_set > 0 and args.workload == "quad":
+        qs = E.free_queries(obs, args.query_set, seed=5, min_sep=6.0, max_sep=15.0)
+        e2e["query_set"] = query_outcomes(pl, qs, obs)
+        e2e["query_set"]["queries_desc"] = (f"{args.query_set} seeded start/goal pairs in the free space of the same scene "
+                                            "(>= 1 m from every box), 6-15 m apart; success = goal ball reached; "
+                                            "time to solution = host clock of kpax_plan_host from host buffers")
+    else:
+        qs = np.zeros((0, 6), np.float32)
+
     clocks = clk.summary()
+    ref_cuda = None
+    if rank == 0 and ws == 1 and args.workload == "quad" and not args.no_ref_cuda:
+        ref_cuda = reference_cuda_leg(cfg, obs, start, goal, qs, args)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         try:
@@ -598,6 +696,7 @@ def run_ours(args) -> None:
                        "children_per_step": tot["children"] // args.steps, "l2": "flushed before each timed iteration "
                        "(256 MiB write, outside the events)", "parallelism": f"replicas x{ws}"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
+            "reference_cuda": ref_cuda,
             "breakdown_ms_per_step": {"frontier": float(times_split[:, 1].mean()), "expand": float(times_split[:, 2].mean()),
                                       "scores": float(times_split[:, 3].mean()),
                                       "total_with_split_events": float(times_split[:, 0].mean()),
@@ -932,6 +1031,9 @@ def main() -> None:
     ap.add_argument("--proposal", choices=["on", "off"], default="on", help="learned proposal for batched quadrotor queries")
     ap.add_argument("--queries", type=int, default=1024)
     ap.add_argument("--plans", type=int, default=8)
+    ap.add_argument("--query-set", type=int, default=32, help="seeded start/goal pairs of the e2e query set (quad)")
+    ap.add_argument("--ref-cuda-plans", type=int, default=3, help="plans of the reference CUDA leg (quad)")
+    ap.add_argument("--no-ref-cuda", action="store_true", help="skip the reference CUDA build's leg")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="ignore the autotuner's cached launch parameters")

@@ -291,6 +291,10 @@ kpax_status kpax_test_wait_timeout(uint32_t spin_limit, uint32_t* h_status, void
 /* Test hook: for each x, writes (sin, cos) of the propagation kernels' sine/cosine and
  * (sin, cos) of CUDA's sincosf, 4 floats per input, so tests can bound their difference. */
 kpax_status kpax_test_sincos(const float* d_x, uint32_t n, float* d_out, void* stream);
+/* FP32 issue rate of this GPU: an FMA-chain kernel (8 independent chains per thread, 2048 threads
+ * per SM, iters FMAs per chain) timed with CUDA events on `stream` after one warm-up launch;
+ * *h_tflops = 16 x iters x threads / time.  The denominator of the propagation roofline. */
+kpax_status kpax_fp32_peak(uint32_t iters, double* h_tflops, double* h_ms, void* stream);
 /* Number of propagation kernels (and other library kernels) launched since load; the
  * benchmark reports it as evidence that the device path ran. */
 uint64_t kpax_kernel_launches(void);

@@ -454,6 +454,57 @@ kpax_status kpax_test_sincos(const float* d_x, uint32_t n, float* d_out, void* s
     return KPAX_OK;
 }
 
+// FP32 issue-rate microkernel: every thread advances kChains independent FMA chains `iters` times
+// (2 FLOP per FMA); the values stay bounded (|a| < 1) and are folded into one store the compiler
+// cannot drop.  The measured rate is the denominator of the propagation kernels' roofline.
+constexpr int kFmaChains = 8;
+__global__ void __launch_bounds__(512) k_fma_peak(float* __restrict__ out, uint32_t iters, float a, float b)
+{
+    float x[kFmaChains];
+#pragma unroll
+    for(int j = 0; j < kFmaChains; ++j) x[j] = (float)(threadIdx.x + j) * 1e-3f;
+    for(uint32_t i = 0; i < iters; i += 16) {
+#pragma unroll
+        for(int u = 0; u < 16; ++u)
+#pragma unroll
+            for(int j = 0; j < kFmaChains; ++j) x[j] = fmaf(x[j], a, b);
+    }
+    float s = 0.0f;
+#pragma unroll
+    for(int j = 0; j < kFmaChains; ++j) s += x[j];
+    if(s == -1.0f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;  // never true; keeps the chains live
+}
+
+kpax_status kpax_fp32_peak(uint32_t iters, double* h_tflops, double* h_ms, void* stream)
+{
+    if(!h_tflops || iters < 16) return set_error("kpax_fp32_peak: need h_tflops and iters >= 16"), KPAX_EINVAL;
+    iters = iters / 16 * 16;
+    int dev = 0, sms = 0;
+    KPAX_CUDA(cudaGetDevice(&dev));
+    KPAX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const uint32_t blocks = (uint32_t)sms * 4u, threads = 512;  // 2048 threads per SM
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    KPAX_CUDA(cudaEventCreate(&e0));
+    KPAX_CUDA(cudaEventCreate(&e1));
+    float ms = 0.0f;
+    for(int rep = 0; rep < 2; ++rep) {  // the first launch warms up
+        cudaEventRecord(e0, s);
+        k_fma_peak<<<blocks, threads, 0, s>>>(nullptr, iters, 0.99999f, 1e-6f);
+        cudaEventRecord(e1, s);
+        count_launch();
+    }
+    cudaError_t err = cudaEventSynchronize(e1);
+    if(err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if(err != cudaSuccess) return set_error("kpax_fp32_peak: %s", cudaGetErrorString(err)), KPAX_ECUDA;
+    const double flop = 2.0 * kFmaChains * (double)iters * blocks * threads;
+    *h_tflops = ms > 0.0f ? flop / (ms * 1e-3) / 1e12 : 0.0;
+    if(h_ms) *h_ms = ms;
+    return KPAX_OK;
+}
+
 kpax_status kpax_env_create(const kpax_config* cfg, const float* d_obstacles, uint32_t n_obs, void* stream, kpax_env** out)
 {
     NvtxRange range("kpax_env_create");

@@ -146,6 +146,7 @@ _SIGNATURES = {
     "kpax_env_destroy": (_I32, [_VP]),
     "kpax_env_stats": (_I32, [_VP, _VP, _VP]),
     "kpax_propagate_batch": (_I32, [ctypes.POINTER(Config), _VP, _VP, _VP, _U32, _U32, _VP, _VP, _VP, _VP]),
+    "kpax_fp32_peak": (_I32, [ctypes.c_uint32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), _VP]),
     "kpax_propagate_batch_noalloc": (_I32, [ctypes.POINTER(Config), _VP, _U32, _VP, _VP, _U32, _U32, _VP, _VP, _VP,
                                              _VP]),
     "kpax_collide_batch": (_I32, [_VP, _VP, _VP, _U32, _VP, _VP]),
@@ -308,6 +309,13 @@ def test_wait_timeout(spin_limit: int, stream: int = 0) -> None:
     raises KpaxError with status ETIMEOUT once the wait gives up."""
     st = ctypes.c_uint32(0)
     check(load().kpax_test_wait_timeout(spin_limit, ctypes.byref(st), stream), "kpax_test_wait_timeout")
+
+
+def fp32_peak(iters: int = 1 << 16, stream: int = 0) -> tuple[float, float]:
+    """Measured FP32 rate of the GPU (TFLOP/s) and the timed launch's ms (kpax_fp32_peak)."""
+    t, ms = ctypes.c_double(), ctypes.c_double()
+    check(load().kpax_fp32_peak(iters, ctypes.byref(t), ctypes.byref(ms), stream), "kpax_fp32_peak")
+    return t.value, ms.value
 
 
 def kernel_launches() -> int:

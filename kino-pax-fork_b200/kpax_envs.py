@@ -267,6 +267,30 @@ def batch_queries(n: int = 1024, seed: int = 4, mix=(0.4, 0.3, 0.3), obs_range=(
     return out
 
 
+def free_queries(obs: np.ndarray, n: int, seed: int, min_sep: float = 6.0, max_sep: float = 15.0, margin: float = 1.0,
+                 lo: float = 5.0, hi: float = 95.0) -> np.ndarray:
+    """n start/goal pairs (rows: start xyz, goal xyz) in the free space of a fixed scene: points
+    uniform in [lo, hi]^3 at least `margin` from every box, start and goal min_sep..max_sep apart."""
+    rng = np.random.default_rng(seed)
+    b = np.asarray(obs, np.float32).reshape(-1, 6)
+    lo_b, hi_b = b[:, :3] - margin, b[:, 3:] + margin
+
+    def free(p):
+        return not np.any(np.all(lo_b <= p, axis=1) & np.all(p <= hi_b, axis=1))
+
+    out = []
+    while len(out) < n:
+        a = rng.uniform(lo, hi, 3)
+        if not free(a):
+            continue
+        d = rng.normal(0.0, 1.0, 3)
+        g = a + d / np.linalg.norm(d) * rng.uniform(min_sep, max_sep)
+        if np.any(g < lo) or np.any(g > hi) or not free(g):
+            continue
+        out.append(np.concatenate([a, g]))
+    return np.asarray(out, np.float32)
+
+
 def learned_family(seed: int, obs_range=(200, 2000), min_sep: float = 25.0, max_sep: float = 45.0, fixed: bool = False):
     """The learned-proposal family of the 12D quadrotor: a 'building' scene (windowed wall at
     x = 50 plus random boxes) with a seeded obstacle count uniform in obs_range.  Start and goal
