@@ -181,13 +181,16 @@ __global__ void __launch_bounds__(256, 4) k_propagate_batch(KParams p, Grid g, c
 constexpr int kHeadSteps = 2;
 inline int mid_steps(const KParams& p) { return std::max(kHeadSteps + 1, (p.nsteps + 1) * 3 / 5); }
 constexpr uint32_t kPhasedMin = 1u << 18;   // segments; below this the one-pass kernel is used
+// Segments per round of the three phases: a round's survivor lists (<= 64 B per segment), parents
+// and rows stay within the 126 MB L2 between the phases, so the lists do not round-trip through HBM.
+constexpr uint32_t kPhaseChunk = 1u << 19;
 
 struct LiveList {
     uint32_t* count;
     uint32_t* idx;
-    int32_t* steps;
-    float* ctl;    // 4 per entry
-    float* state;  // SD per entry
+    int32_t* steps;  // unused (null) for fixed-step models
+    float* ctl;      // CD per entry
+    float* state;    // SD per entry
 };
 
 template <int M>
@@ -209,7 +212,7 @@ __device__ __forceinline__ void write_segment(const KParams& p, uint32_t i, cons
 }
 
 // Appends the warp's live segments to `live` (one atomic per warp); called by all 32 lanes.
-template <int SD>
+template <int SD, int CD>
 __device__ __forceinline__ void append_live(const LiveList& live, bool alive, int lane, uint32_t i, int steps, const float* c,
                                             const float* s)
 {
@@ -222,21 +225,23 @@ __device__ __forceinline__ void append_live(const LiveList& live, bool alive, in
     if(alive) {
         const uint32_t j = base + __popc(m & ((1u << lane) - 1u));
         live.idx[j] = i;
-        live.steps[j] = steps;
+        if(live.steps) live.steps[j] = steps;
 #pragma unroll
-        for(int k = 0; k < 4; ++k) live.ctl[(size_t)j * 4 + k] = c[k];
+        for(int k = 0; k < CD; ++k) live.ctl[(size_t)j * CD + k] = c[k];
 #pragma unroll
         for(int k = 0; k < SD; ++k) live.state[(size_t)j * SD + k] = s[k];
     }
 }
 
+// Segments i of one round (pointers offset to the round's first segment; i0 = that segment's index
+// in the batch, which keys its draws).
 template <int M>
 __global__ void __launch_bounds__(256, 4) k_propagate_head(KParams p, Grid g, const float* __restrict__ parents,
                                                         const float* __restrict__ draws, uint32_t stream_id, uint32_t n,
-                                                        float* __restrict__ rows, uint8_t* __restrict__ valid,
+                                                        uint32_t i0, float* __restrict__ rows, uint8_t* __restrict__ valid,
                                                         int32_t* __restrict__ steps_out, LiveList live)
 {
-    constexpr int SD = ModelDims<M>::SD;
+    constexpr int SD = ModelDims<M>::SD, CD = ModelDims<M>::CD;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     bool alive = false;
@@ -251,7 +256,7 @@ __global__ void __launch_bounds__(256, 4) k_propagate_head(KParams p, Grid g, co
             for(int k = 0; k < 5; ++k) u[k] = __ldg(draws + (size_t)i * 5 + k);
             u[5] = 0.0f;
         } else {
-            child_draws(p, stream_id, 0u, i, u);
+            child_draws(p, stream_id, 0u, i0 + i, u);
         }
         steps = draw_controls(p, u, c);
         const auto k = segment_consts<M>(p, c);
@@ -266,7 +271,7 @@ __global__ void __launch_bounds__(256, 4) k_propagate_head(KParams p, Grid g, co
         alive = ok && done < steps;
         if(!alive) write_segment<M>(p, i, s, c, steps, ok, done, rows, valid, steps_out);
     }
-    append_live<SD>(live, alive, lane, i, steps, c, s);
+    append_live<SD, CD>(live, alive, lane, i, steps, c, s);
 }
 
 template <int M>
@@ -274,7 +279,7 @@ __global__ void __launch_bounds__(256, 4) k_propagate_tail(KParams p, Grid g, fl
                                                         uint8_t* __restrict__ valid, int32_t* __restrict__ steps_out,
                                                         LiveList live, int from, int until, LiveList next)
 {
-    constexpr int SD = ModelDims<M>::SD;
+    constexpr int SD = ModelDims<M>::SD, CD = ModelDims<M>::CD;
     const uint32_t count = *live.count;
     if(blockIdx.x * blockDim.x >= count) return;  // whole block past the list: the ballot below needs full warps
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -285,9 +290,9 @@ __global__ void __launch_bounds__(256, 4) k_propagate_tail(KParams p, Grid g, fl
     float s[SD], c[4];
     if(j < count) {
         i = live.idx[j];
-        steps = live.steps[j];
+        steps = live.steps ? live.steps[j] : p.nsteps;
 #pragma unroll
-        for(int k = 0; k < 4; ++k) c[k] = live.ctl[(size_t)j * 4 + k];
+        for(int k = 0; k < 4; ++k) c[k] = k < CD ? live.ctl[(size_t)j * CD + k] : 0.0f;
 #pragma unroll
         for(int k = 0; k < SD; ++k) s[k] = live.state[(size_t)j * SD + k];
         const auto kc = segment_consts<M>(p, c);
@@ -302,18 +307,29 @@ __global__ void __launch_bounds__(256, 4) k_propagate_tail(KParams p, Grid g, fl
         alive = next.count && ok && done < steps;
         if(!alive) write_segment<M>(p, i, s, c, steps, ok, done, rows, valid, steps_out);
     }
-    if(next.count) append_live<SD>(next, alive, lane, i, steps, c, s);
+    if(next.count) append_live<SD, CD>(next, alive, lane, i, steps, c, s);
 }
 
+// The three phases over rounds of kPhaseChunk segments; `counts` (two words, 128 bytes apart) are
+// cleared before every round.
 template <int M>
 void launch_phases(const KParams& p, const Grid& g, const float* parents, const float* draws, uint32_t stream_id, uint32_t n,
                    float* rows, uint8_t* valid, int32_t* steps_out, const LiveList& first, const LiveList& second,
-                   const LiveList& none, uint32_t blocks, cudaStream_t s)
+                   const LiveList& none, void* counts, cudaStream_t s)
 {
-    k_propagate_head<M><<<blocks, 256, 0, s>>>(p, g, parents, draws, stream_id, n, rows, valid, steps_out, first);
-    const int mid = mid_steps(p);
-    k_propagate_tail<M><<<blocks, 256, 0, s>>>(p, g, rows, valid, steps_out, first, kHeadSteps, mid, second);
-    k_propagate_tail<M><<<blocks, 256, 0, s>>>(p, g, rows, valid, steps_out, second, mid, INT_MAX, none);
+    const int SD = p.sd, S = p.S, mid = mid_steps(p);
+    for(uint32_t o = 0; o < n; o += kPhaseChunk) {
+        const uint32_t m = std::min(kPhaseChunk, n - o), blocks = (m + 255) / 256;
+        float* r = rows + (size_t)o * S;
+        uint8_t* v = valid + o;
+        int32_t* st = steps_out ? steps_out + o : nullptr;
+        cudaMemsetAsync(counts, 0, 256, s);
+        k_propagate_head<M><<<blocks, 256, 0, s>>>(p, g, parents + (size_t)o * SD, draws ? draws + (size_t)o * 5 : nullptr,
+                                                   stream_id, m, o, r, v, st, first);
+        k_propagate_tail<M><<<blocks, 256, 0, s>>>(p, g, r, v, st, first, kHeadSteps, mid, second);
+        k_propagate_tail<M><<<blocks, 256, 0, s>>>(p, g, r, v, st, second, mid, INT_MAX, none);
+        count_launch(3);
+    }
 }
 
 __global__ void k_collide_batch(Grid g, const float* __restrict__ bbmin, const float* __restrict__ bbmax, uint32_t n,
@@ -559,12 +575,14 @@ kpax_status kpax_propagate_batch(const kpax_config* cfg, kpax_env* env, const fl
     if(n < kPhasedMin)
         return launch_propagate(p, env->env.view(), d_parents, d_draws, draw_stream, n, d_rows, d_valid, d_steps,
                                 (cudaStream_t)stream);
-    // phases: the two live lists live in the env's scratch, grown on demand (counts at bytes 0 and
-    // 128, then each list's index, step-count, control and state arrays)
+    // phases: the two live lists of a round live in the env's scratch, grown on demand (counts at
+    // bytes 0 and 128, then each list's index, step-count (drawn durations only), control and state
+    // arrays)
     Env& e = env->env;
     auto align = [](size_t b) { return (b + 255) / 256 * 256; };
-    const size_t l_idx = 0, l_steps = align(4ull * n), l_ctl = l_steps + align(4ull * n), l_state = l_ctl + align(16ull * n),
-                 l_bytes = l_state + align(4ull * p.sd * n), bytes = 256 + 2 * l_bytes;
+    const size_t m = std::min(n, kPhaseChunk);
+    const size_t l_idx = 0, l_steps = align(4ull * m), l_ctl = l_steps + (p.fixed_steps ? 0 : align(4ull * m)),
+                 l_state = l_ctl + align(4ull * p.cd * m), l_bytes = l_state + align(4ull * p.sd * m), bytes = 256 + 2 * l_bytes;
     if(bytes > e.live_cap) {
         if(e.d_live) cudaFree(e.d_live), e.d_live = nullptr, e.live_cap = 0;
         KPAX_CUDA(cudaMalloc(&e.d_live, bytes));
@@ -574,30 +592,27 @@ kpax_status kpax_propagate_batch(const kpax_config* cfg, kpax_env* env, const fl
     auto list = [&](int k) {
         char* l = base + 256 + (size_t)k * l_bytes;
         return LiveList{reinterpret_cast<uint32_t*>(base + 128 * k), reinterpret_cast<uint32_t*>(l + l_idx),
-                        reinterpret_cast<int32_t*>(l + l_steps), reinterpret_cast<float*>(l + l_ctl),
+                        p.fixed_steps ? nullptr : reinterpret_cast<int32_t*>(l + l_steps), reinterpret_cast<float*>(l + l_ctl),
                         reinterpret_cast<float*>(l + l_state)};
     };
     const LiveList first = list(0), second = list(1), none{};
     cudaStream_t s = (cudaStream_t)stream;
-    KPAX_CUDA(cudaMemsetAsync(base, 0, 256, s));
     const Grid g = e.view();
-    const uint32_t blocks = (n + 255) / 256;
     switch(p.model) {
         case KPAX_MODEL_DOUBLE_INTEGRATOR:
             launch_phases<KPAX_MODEL_DOUBLE_INTEGRATOR>(p, g, d_parents, d_draws, draw_stream, n, d_rows, d_valid, d_steps, first,
-                                                       second, none, blocks, s);
+                                                       second, none, base, s);
             break;
         case KPAX_MODEL_DUBINS_AIRPLANE:
             launch_phases<KPAX_MODEL_DUBINS_AIRPLANE>(p, g, d_parents, d_draws, draw_stream, n, d_rows, d_valid, d_steps, first,
-                                                     second, none, blocks, s);
+                                                     second, none, base, s);
             break;
         default:
             launch_phases<KPAX_MODEL_QUADROTOR>(p, g, d_parents, d_draws, draw_stream, n, d_rows, d_valid, d_steps, first, second,
-                                               none, blocks, s);
+                                               none, base, s);
             break;
     }
     KPAX_CHECK_LAUNCH();
-    count_launch(3);
     return KPAX_OK;
 }
 

@@ -779,6 +779,8 @@ int ko_plan(const kpax_config* cfg, const float* init, const float* goal, const 
     uint32_t* entry = (uint32_t*)malloc(sizeof(uint32_t) * (budget_max ? budget_max : 1));
     float* child = (float*)malloc(sizeof(float) * S * (budget_max ? budget_max : 1));
     int32_t* child_r1 = (int32_t*)malloc(sizeof(int32_t) * (budget_max ? budget_max : 1));
+    int32_t* child_r2 = (int32_t*)malloc(sizeof(int32_t) * (budget_max ? budget_max : 1));
+    uint8_t* child_ok = (uint8_t*)malloc(budget_max ? budget_max : 1);
     uint8_t* child_next = (uint8_t*)malloc(budget_max ? budget_max : 1);
     ko_env* env = ko_env_create(cfg, obs, n_obs);
     ko_region_table(cfg, table);
@@ -805,16 +807,29 @@ int ko_plan(const kpax_config* cfg, const float* init, const float* goal, const 
         const uint32_t n = E * k;
         take_entries(rep, tree, R, E, entry);
         memcpy(nxt, cur, sizeof(uint32_t) * words);
-        /* propagateFrontier_kernel1 body (KPAX.cu:381-396) with snapshot R2 reads */
+        /* propagateFrontier_kernel1 body (KPAX.cu:381-396) with snapshot R2 reads: the children are
+         * independent (their draws, parents, the R2 snapshot and last iteration's scores are fixed),
+         * so they are propagated in parallel and their counter updates applied in child order */
+#pragma omp parallel for schedule(dynamic, 64)
+        for(long cc = 0; cc < (long)n; ++cc) {
+            const uint32_t c = (uint32_t)cc;
+            float u[6], x0[12];
+            ko_child_draws(cfg->seed, plan_idx, it, c, u);
+            memcpy(x0, rows + (size_t)entry[c / k] * S, sizeof(float) * sd);
+            float* x1 = child + (size_t)c * S;
+            child_ok[c] = (uint8_t)ko_propagate(cfg, env, x0, u, x1, NULL, NULL);
+            child_r1[c] = ko_region_r1(cfg, x1);
+            child_r2[c] = ko_region_r2(cfg, table, x1, child_r1[c]);
+        }
         for(uint32_t c = 0; c < n; ++c) {
             uint32_t p = entry[c / k];
             float u[6], x0[12];
             ko_child_draws(cfg->seed, plan_idx, it, c, u);
             memcpy(x0, rows + (size_t)p * S, sizeof(float) * sd);
             float* x1 = child + (size_t)c * S;
-            int ok = ko_propagate(cfg, env, x0, u, x1, NULL, NULL);
-            int a = ko_region_r1(cfg, x1);
-            int b = ko_region_r2(cfg, table, x1, a);
+            int ok = child_ok[c];
+            int a = child_r1[c];
+            int b = child_r2[c];
             counter[a] += 1;
             child_r1[c] = a;
             child_next[c] = 0;
@@ -899,7 +914,7 @@ int ko_plan(const kpax_config* cfg, const float* init, const float* goal, const 
         if(out->r2_bits) memcpy(out->r2_bits, cur, sizeof(uint32_t) * words);
     }
     free(rows), free(parent), free(cost), free(r1), free(rep), free(counter), free(valid), free(scores);
-    free(cur), free(nxt), free(table), free(entry), free(child), free(child_r1), free(child_next);
+    free(cur), free(nxt), free(table), free(entry), free(child), free(child_r1), free(child_r2), free(child_ok), free(child_next);
     ko_env_destroy(env);
     return found;
 }
