@@ -151,7 +151,7 @@ def cpu_reference_rate(cfg, obs, parents, budget_s: float, per_parent: int = 32,
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
 
-    ref = O.RefLib(cfg.model)
+    ref = O.RefLib(cfg.model, "quad_ref" if args.workload == "quad-ref" else None)
     ref.set_obstacles(obs)
     threads = ref.L.kref_max_threads()
     n1, P = ref.num_r1, ref.r2_per_r1
@@ -398,14 +398,17 @@ def run_reference(args) -> None:
         }
         print(json.dumps(line), flush=True)
         return
-    pre, scene, desc = WORKLOADS[args.workload]
+    if args.workload == "quad-ref":
+        pre, scene, desc = kpax.PRESET_QUAD_REF, quad_trees_scene, QUAD_REF_DESC
+    else:
+        pre, scene, desc = WORKLOADS[args.workload]
     cfg = kpax.preset(pre)
     obs, start, goal = scene()
     parents = frontier_parents(cfg, obs, start, goal)
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
 
-    ref = O.RefLib(cfg.model)
+    ref = O.RefLib(cfg.model, "quad_ref" if args.workload == "quad-ref" else None)
     ref.set_obstacles(obs)
     threads = ref.L.kref_max_threads()
     n1, P = ref.num_r1, ref.r2_per_r1
@@ -525,6 +528,100 @@ def reference_cuda_leg(cfg, obs, start, goal, queries, args) -> dict:
         out["ours_same_config"]["query_set"] = query_outcomes(pl, queries, obs)
     pl.close()
     return out
+
+
+QUAD_REF_DESC = ("12D quadrotor with the reference's own configuration block (h 0.1 s, steps 1 + (int)(u * 10), Zc in "
+                 "[0, 30], torques in [-pi, pi], tree capacity 400000, 300 iterations) on its quadTrees scene (158 boxes) "
+                 "with its drivers' pair (10, 8, 5) -> (80, 95, 90)")
+
+
+def quad_trees_scene():
+    """The reference's quadTrees obstacle file (include/config/obstacles/quadTrees), committed as a
+    fixture, with its drivers' start and goal (comprehensive_benchmark.cu:251-252)."""
+    obs = np.ascontiguousarray(np.load(ROOT / "tests" / "golden" / "quad_quadTrees.npz")["obstacles"], np.float32)
+    start, goal = np.zeros(12, np.float32), np.zeros(12, np.float32)
+    start[:3], goal[:3] = (10.0, 8.0, 5.0), (80.0, 95.0, 90.0)
+    return obs, start, goal
+
+
+def ks_distance(a, b) -> float | None:
+    a, b = np.sort(np.asarray(a, np.float64)), np.sort(np.asarray(b, np.float64))
+    if not a.size or not b.size:
+        return None
+    x = np.union1d(a, b)
+    return float(np.max(np.abs(np.searchsorted(a, x, "right") / a.size - np.searchsorted(b, x, "right") / b.size)))
+
+
+def run_quad_ref(args) -> None:
+    """Whole plans at the reference's own quadrotor configuration: this library through
+    kpax_plan_host (host buffers) beside the reference's CUDA build through KPAX::plan, the same
+    number of plans each: success (goal reached), time to solution, path-cost distributions."""
+    import torch
+
+    ws, rank, local = dist_setup(args.gpus)
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device (no CPU fallback)")
+    torch.cuda.set_device(local)
+    cfg = kpax.preset(kpax.PRESET_QUAD_REF)
+    cfg.seed = cfg.seed + 1000003 * rank
+    obs, start, goal = quad_trees_scene()
+    pl = kpax.KPAX(cfg)
+    for _ in range(max(args.warmup, 1)):
+        pl.plan_host(start, goal, obs)
+    n = args.plans_ref
+    found, tts, costs, valid, secs, iters = 0, [], [], 0, 0.0, []
+    launches0 = kpax.kernel_launches()
+    with Clocks(local) as clk:
+        for _ in range(n):
+            t0 = time.perf_counter()
+            r = pl.plan_host(start, goal, obs)
+            dt = time.perf_counter() - t0
+            secs += dt
+            valid += r.valid_expansions
+            iters.append(r.iters)
+            if r.found:
+                found += 1
+                tts.append(1000 * dt)
+                costs.append(float(r.path_cost))
+    launches = kpax.kernel_launches() - launches0
+    pl.close()
+    ours = {"plans": n, "success_rate": found / n, "tts_ms_p50": float(np.percentile(tts, 50)) if tts else None,
+            "tts_ms_p95": float(np.percentile(tts, 95)) if tts else None,
+            "path_cost_median": float(np.median(costs)) if costs else None,
+            "iterations_median": float(np.median(iters)), "valid_expansions_per_s": valid / secs}
+    ref = None
+    if rank == 0 and not args.no_ref_cuda:
+        sys.path.insert(0, str(ROOT / "oracle" / "refcuda"))
+        import refcuda
+
+        rs = refcuda.summarise(refcuda.run("quad_ref", obs, [[*start[:3], *goal[:3]]], iteration_cap=cfg.max_iter,
+                                           repeats=n, timeout_s=600))
+        if "unavailable" in rs:
+            ref = rs
+        else:
+            t = rs["tts_ms"]
+            ref = {"plans": rs["plans"], "success_rate": rs["success_rate"],
+                   "tts_ms_p50": float(np.percentile(t, 50)) if t else None,
+                   "tts_ms_p95": float(np.percentile(t, 95)) if t else None,
+                   "path_cost_median": float(np.median(rs["path_costs"])) if rs["path_costs"] else None,
+                   "capacity_stops": rs["capacity_stops"], "valid_expansions_per_s": rs["value"],
+                   "kind": "reference CUDA build: KPAX::plan from its own sources, sm_100a; seeds from the wall clock "
+                           "as in the reference (KPAX.cu:90-91)",
+                   "path_cost_ks_vs_ours": ks_distance(costs, rs["path_costs"])}
+    if rank == 0:
+        value = valid / secs
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": n, "warmup": args.warmup,
+                "ms_per_step": 1000 * secs / n, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "fp32", "data": "the reference's quadTrees obstacle file",
+                "config": {"workload": QUAD_REF_DESC, "expansions_per_iter": cfg.expansions_per_iter,
+                           "l2": "whole plans back to back (each plan's data is larger than L2 only late in a plan)",
+                           "parallelism": f"replicas x{ws}"},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": obs.nbytes + 2 * 4 * cfg.sample_dim,
+                        "d2h_bytes_per_step": 128, "plans": n, "success_rate": ours["success_rate"],
+                        "tts_ms_p50": ours["tts_ms_p50"], "tts_ms_p95": ours["tts_ms_p95"]},
+                "plan_outcomes": {"ours": ours, "reference_cuda": ref}, "gpu_launches": launches,
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
 
 
 def run_ours(args) -> None:
@@ -1025,7 +1122,9 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "learned", "segments", "collide"], default="quad")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "learned", "segments", "collide", "quad-ref"],
+                    default="quad")
+    ap.add_argument("--plans-ref", type=int, default=256, help="plans per side of the quad-ref workload")
     ap.add_argument("--seeds", type=int, default=256, help="held-out scenes of the learned workload")
     ap.add_argument("--eps", type=float, default=0.2, help="uniform fraction of the learned proposal")
     ap.add_argument("--proposal", choices=["on", "off"], default="on", help="learned proposal for batched quadrotor queries")
@@ -1050,6 +1149,8 @@ def main() -> None:
         run_segments(args)
     elif args.workload == "collide":
         run_collide(args)
+    elif args.workload == "quad-ref":
+        run_quad_ref(args)
     else:
         run_ours(args)
 

@@ -245,8 +245,10 @@ def plan(cfg, init, goal, obs, plan_idx: int = 0, max_iters: int | None = None, 
 class RefLib:
     """The reference's own routines built for the host (one library per configuration)."""
 
-    def __init__(self, model: int):
-        self.name = REF_NAMES[model]
+    def __init__(self, model: int, name: str | None = None):
+        """name: the configuration's library (default the model's benchmark configuration; "quad_ref"
+        for the reference's own quadrotor block)."""
+        self.name = name or REF_NAMES[model]
         path = ORACLE_DIR / "_ref" / f"libkref_{self.name}.so"
         if not path.exists():
             build()
