@@ -449,6 +449,14 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def pct_all(ms, q: float):
+    """Nearest-rank percentile of plan times with unsolved plans as +inf (None when it is one)."""
+    if not len(ms):
+        return None
+    v = float(np.quantile(np.asarray(ms, np.float64), q / 100.0, method="inverted_cdf"))
+    return v if np.isfinite(v) else None
+
+
 def query_outcomes(pl, queries: np.ndarray, obs: np.ndarray) -> dict:
     """Whole plans of a query set (rows: start xyz, goal xyz) through kpax_plan_host from host
     buffers: success (goal reached), time to solution (host clock of the call), path costs."""
@@ -472,8 +480,7 @@ def query_outcomes(pl, queries: np.ndarray, obs: np.ndarray) -> dict:
     return {"queries": n, "success_rate": found / max(n, 1),
             "tts_ms_p50": float(np.percentile(tts, 50)) if tts else None,
             "tts_ms_p95": float(np.percentile(tts, 95)) if tts else None,
-            "tts_ms_p50_all": float(np.percentile(all_ms, 50)) if n else None,
-            "tts_ms_p95_all": float(np.percentile(all_ms, 95)) if n else None,
+            "tts_ms_p50_all": pct_all(all_ms, 50), "tts_ms_p95_all": pct_all(all_ms, 95),
             "path_cost_median": float(np.median(costs)) if costs else None,
             "valid_expansions_per_s": valid / secs if secs > 0 else None}
 

@@ -169,10 +169,17 @@ def logit_targets(ctrl: np.ndarray, cfg: kpax.Config) -> np.ndarray:
     return y
 
 
+# Start-goal separation bands (m) of a mixed harvest: scene j of the training seeds draws from band
+# j mod 4, so the network sees near goals (whose plans mostly succeed and contribute solution
+# edges) as well as the 25-45 m family it is evaluated on.
+SEP_BANDS = ((6.0, 12.0), (12.0, 20.0), (20.0, 30.0), (25.0, 45.0))
+
+
 def harvest(seeds, pairs_per_env: int, cfg: kpax.Config, net: kpax.MLP | None = None, eps: float = 0.2, seed: int = 0,
-            log=print, ray: bool = False, select: str = "weighted", elite: float = 0.02):
+            log=print, ray: bool = False, select: str = "weighted", elite: float = 0.02, sep_mix: bool = False):
     """Plans every scene of `seeds` (plain sampler, or `net` with epsilon `eps`) and returns the
-    device feature / target tensors and per-scene plan statistics."""
+    device feature / target tensors and per-scene plan statistics.  sep_mix: scene j's start and
+    goal are SEP_BANDS[j % 4] apart instead of the family's 25-45 m."""
     import torch
 
     rng = np.random.default_rng(seed)
@@ -186,7 +193,11 @@ def harvest(seeds, pairs_per_env: int, cfg: kpax.Config, net: kpax.MLP | None = 
     filled = 0
     t0 = time.time()
     for j, sd in enumerate(seeds):
-        obs, start, goal = E.learned_family(int(sd))
+        if sep_mix:
+            lo, hi = SEP_BANDS[j % len(SEP_BANDS)]
+            obs, start, goal = E.learned_family(int(sd), min_sep=lo, max_sep=hi)
+        else:
+            obs, start, goal = E.learned_family(int(sd))
         d_obs = torch.from_numpy(obs).cuda()
         r = planner.plan(start, goal, d_obs.data_ptr(), obs.shape[0])
         rows, parents, _ = planner.export_tree()
@@ -321,6 +332,7 @@ def main(argv=None):
     t.add_argument("--max-iter", type=int, default=0)
     t.add_argument("--select", choices=("weighted", "far", "goal"), default="goal")
     t.add_argument("--ray", action="store_true")
+    t.add_argument("--sep-mix", action="store_true", help="harvest scenes from the four separation bands of SEP_BANDS")
     t.add_argument("--eval-seeds", type=int, default=256)
     t.add_argument("--out", type=Path, default=DEFAULT_WEIGHTS)
     e = sub.add_parser("eval")
@@ -362,14 +374,15 @@ def main(argv=None):
         seeds = [TRAIN_SEED0 + i for i in range(a.envs)]
         net, w = None, None
         meta = {"envs": a.envs, "pairs": a.pairs, "steps": a.steps, "batch": a.batch, "lr": a.lr, "select": a.select,
-                "ray": a.ray, "eps": a.eps, "rounds": []}
+                "ray": a.ray, "eps": a.eps, "sep_mix": bool(a.sep_mix), "rounds": []}
         eval_seeds = [EVAL_SEED0 + i for i in range(a.eval_seeds)]
         if a.eval_seeds:
             meta["plain"] = summarize(evaluate(eval_seeds, cfg, progress=True))
             print(json.dumps({"plain": meta["plain"]}))
         for rnd in range(a.rounds):
             t0 = time.time()
-            X, Y, st = harvest(seeds, a.pairs // a.envs, cfg, net=net, eps=a.eps, seed=rnd, select=a.select, ray=a.ray)
+            X, Y, st = harvest(seeds, a.pairs // a.envs, cfg, net=net, eps=a.eps, seed=rnd, select=a.select, ray=a.ray,
+                               sep_mix=a.sep_mix)
             t_h = time.time() - t0
             net, hist = train(X, Y, a.steps, cfg, a.batch, a.lr, seed=rnd, w0=w)
             w = net.get_params()

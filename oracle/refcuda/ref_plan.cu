@@ -12,9 +12,15 @@
 // Guards (both checked before any device work of the planner runs):
 //  - capacity: MAX_ITER is kref_iteration_bound() (see kref_cuda_common.h), evaluated by the
 //    reference before each iteration.  It sums the frontier's repeat counts R (the quantity
-//    propagateFrontier scans, KPAX.cu:316-321) and ends the plan when R x 32 children would not
-//    fit in the tree, so the branch of KPAX.cu:323-341 never runs and every write of
-//    propagateFrontier_kernel1 / repeatInd / updateFrontier_kernel stays inside its buffer.
+//    propagateFrontier scans, KPAX.cu:316-321) and ends the plan before an iteration whose frontier
+//    has more entries than the tree has free slots.  That is the one case in which the reference
+//    writes past its buffers: propIterations rounds down to 0 and is forced to 1
+//    (KPAX.cu:325-333), so R children are appended into fewer free slots (updateFrontier_kernel,
+//    KPAX.cu:461) and repeatInd fills R entries (Planner.cu:68-80).  With R <= free slots the
+//    branch of KPAX.cu:323-341 runs as designed (propIterations = min(free / R, 32) children per
+//    entry) and stays inside every buffer; its clear of frontier[tid] by thread index
+//    (KPAX.cu:411) reaches index propIterations * R + 31 < MAX_TREE_SIZE once the tree holds 32
+//    nodes, which the guard also requires whenever that branch would run.
 //  - hash grid: a cell's obstacle count keeps growing past its 16 slots (spatialHash.cu:41-48)
 //    and isMotionValidSpatialHash reads `count` slots from the cell's start
 //    (spatialHash.cu:166-173), i.e. into the following cells' slots.  The harness recounts the
@@ -54,10 +60,11 @@ bool g_stopped = false;  // the last evaluation ended the loop
 double g_hook_s = 0.0;
 
 struct HookRec {
-    double t0, t1;     // host clock around the hook
-    uint32_t R;        // frontier repeat total before the next iteration
-    uint32_t tree;     // h_treeSize_
-    long long valid;   // sum of the valid counters so far
+    double t0, t1;       // host clock around the hook
+    uint32_t R;          // frontier repeat total before the next iteration
+    uint32_t tree;       // h_treeSize_
+    long long valid;     // sum of the valid counters so far
+    long long children;  // sum of the sample counters so far (one per child, KPAX.cu:390)
 };
 std::vector<HookRec> g_recs;
 
@@ -75,9 +82,12 @@ int kref_iteration_bound(void)
     const double t0 = now_s();
     const uint32_t R = thrust::reduce(pl.d_activeFrontierRepeatCount_.begin(), pl.d_activeFrontierRepeatCount_.end(), 0u);
     const long long valid = thrust::reduce(pl.graph_.d_validCounterArray_.begin(), pl.graph_.d_validCounterArray_.end(), 0LL);
-    const bool fits = (uint64_t)R * pl.h_activeBlockSize_ <= (uint64_t)(MAX_TREE_SIZE - pl.h_treeSize_);
+    const long long children = thrust::reduce(pl.graph_.d_counterArray_.begin(), pl.graph_.d_counterArray_.end(), 0LL);
+    const uint64_t free_slots = (uint64_t)(MAX_TREE_SIZE - pl.h_treeSize_);
+    const bool full_expansion = (uint64_t)R * pl.h_activeBlockSize_ <= free_slots;  // propagateFrontier_kernel1
+    const bool fits = full_expansion || ((uint64_t)R <= free_slots && pl.h_treeSize_ >= 32);
     const double t1 = now_s();
-    g_recs.push_back({t0, t1, R, pl.h_treeSize_, valid});
+    g_recs.push_back({t0, t1, R, pl.h_treeSize_, valid, children});
     g_hook_s += t1 - t0;
     g_guard_stop = !fits;
     g_stopped = !fits || pl.h_itr_ >= g_cap;
@@ -223,15 +233,16 @@ int main(int argc, char** argv)
                     }
                 }
             }
-            // per iteration: children (R x 32 of the hook before it), valid children, host seconds
+            // per iteration: children and valid children (the reference's counters), host seconds
             std::ostringstream it;
             const size_t nrec = g_recs.size();
             const size_t n_it = g_stopped && nrec ? nrec - 1 : nrec;
             for(size_t i = 0; i < n_it; ++i) {
                 const double te = i + 1 < nrec ? g_recs[i + 1].t0 : t1;
                 const long long ve = i + 1 < nrec ? g_recs[i + 1].valid : valid;
-                it << (i ? "," : "") << "[" << (unsigned long long)g_recs[i].R * planner.h_activeBlockSize_ << ","
-                   << (ve - g_recs[i].valid) << "," << (te - g_recs[i].t1) << "]";
+                const long long ce = i + 1 < nrec ? g_recs[i + 1].children : children;
+                it << (i ? "," : "") << "[" << (ce - g_recs[i].children) << "," << (ve - g_recs[i].valid) << ","
+                   << (te - g_recs[i].t1) << "]";
             }
             js << (first ? "\n  " : ",\n  ") << "{\"start\": [" << q[0] << "," << q[1] << "," << q[2] << "], \"goal\": [" << q[3]
                << "," << q[4] << "," << q[5] << "], \"found\": " << (goal != 0 ? 1 : 0) << ", \"iters\": " << planner.h_itr_
