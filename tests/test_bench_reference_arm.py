@@ -42,3 +42,12 @@ def test_collide_reference_line():
 def test_no_counterpart_lines(workload):
     d = run("--workload", workload)
     assert d["impl"] == "reference" and d["unavailable"]
+
+
+@pytest.mark.skipif(not (ROOT / "oracle" / "_ref" / "libkref_quad_ref.so").exists(), reason="reference routines not built")
+def test_quad_ref_reference_line():
+    """The reference's own quadrotor block (h 0.1 s, up to 10 steps, torques in [-pi, pi]) on its
+    quadTrees scene: the host-compiled reference body of that block."""
+    d = run("--workload", "quad-ref", "--steps", "1", "--warmup", "1")
+    assert d["impl"] == "reference" and d["metric"] == "valid expansions/s" and d["value"] > 0
+    assert "quadTrees" in d["config"]["workload"] and d["config"]["expansions_per_iter"] > 0
