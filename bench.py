@@ -151,7 +151,7 @@ def cpu_reference_rate(cfg, obs, parents, budget_s: float, per_parent: int = 32,
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
 
-    ref = O.RefLib(cfg.model, "quad_ref" if args.workload == "quad-ref" else None)
+    ref = O.RefLib(cfg.model)
     ref.set_obstacles(obs)
     threads = ref.L.kref_max_threads()
     n1, P = ref.num_r1, ref.r2_per_r1
@@ -559,75 +559,97 @@ def ks_distance(a, b) -> float | None:
     return float(np.max(np.abs(np.searchsorted(a, x, "right") / a.size - np.searchsorted(b, x, "right") / b.size)))
 
 
+def ours_plans(cfg, obs, start, goal, n: int, warmup: int) -> dict:
+    """n plans of this library through kpax_plan_host (host buffers), host clock per call."""
+    pl = kpax.KPAX(cfg)
+    for _ in range(max(warmup, 1)):
+        pl.plan_host(start, goal, obs)
+    found, tts, costs, valid, secs, iters = 0, [], [], 0, 0.0, []
+    for _ in range(n):
+        t0 = time.perf_counter()
+        r = pl.plan_host(start, goal, obs)
+        dt = time.perf_counter() - t0
+        secs += dt
+        valid += r.valid_expansions
+        iters.append(r.iters)
+        if r.found:
+            found += 1
+            tts.append(1000 * dt)
+            costs.append(float(r.path_cost))
+    pl.close()
+    return {"plans": n, "success_rate": found / n, "tts_ms_p50": float(np.percentile(tts, 50)) if tts else None,
+            "tts_ms_p95": float(np.percentile(tts, 95)) if tts else None,
+            "path_cost_median": float(np.median(costs)) if costs else None, "iterations_median": float(np.median(iters)),
+            "valid_expansions_per_s": valid / secs, "seconds": secs, "path_costs": costs}
+
+
+def reference_plans(ref_cfg: str, obs, start, goal, n: int, iteration_cap: int) -> dict:
+    """n plans of the reference's CUDA build (KPAX::plan) through oracle/refcuda."""
+    sys.path.insert(0, str(ROOT / "oracle" / "refcuda"))
+    import refcuda
+
+    rs = refcuda.summarise(refcuda.run(ref_cfg, obs, [[*start[:3], *goal[:3]]], iteration_cap=iteration_cap, repeats=n,
+                                       timeout_s=900))
+    if "unavailable" in rs:
+        return rs
+    t = rs["tts_ms"]
+    return {"plans": rs["plans"], "success_rate": rs["success_rate"],
+            "tts_ms_p50": float(np.percentile(t, 50)) if t else None,
+            "tts_ms_p95": float(np.percentile(t, 95)) if t else None,
+            "path_cost_median": float(np.median(rs["path_costs"])) if rs["path_costs"] else None,
+            "capacity_stops": rs["capacity_stops"], "valid_expansions_per_s": rs["value"], "path_costs": rs["path_costs"],
+            "kind": "reference CUDA build: KPAX::plan from its own sources, sm_100a; seeds from the wall clock as in the "
+                    "reference (KPAX.cu:90-91); a plan is ended (unsolved) before an iteration whose frontier has more "
+                    "entries than the tree has free slots, where the reference appends past its buffers (KPAX.cu:325-333)"}
+
+
 def run_quad_ref(args) -> None:
     """Whole plans at the reference's own quadrotor configuration: this library through
     kpax_plan_host (host buffers) beside the reference's CUDA build through KPAX::plan, the same
-    number of plans each: success (goal reached), time to solution, path-cost distributions."""
+    number of plans each, at the configured tree capacity (400000) and at 2^22: success (goal
+    reached), time to solution, path-cost distributions."""
     import torch
 
     ws, rank, local = dist_setup(args.gpus)
     if not torch.cuda.is_available():
         raise SystemExit("bench.py needs a CUDA device (no CPU fallback)")
     torch.cuda.set_device(local)
-    cfg = kpax.preset(kpax.PRESET_QUAD_REF)
-    cfg.seed = cfg.seed + 1000003 * rank
     obs, start, goal = quad_trees_scene()
-    pl = kpax.KPAX(cfg)
-    for _ in range(max(args.warmup, 1)):
-        pl.plan_host(start, goal, obs)
     n = args.plans_ref
-    found, tts, costs, valid, secs, iters = 0, [], [], 0, 0.0, []
+    sides = []
     launches0 = kpax.kernel_launches()
     with Clocks(local) as clk:
-        for _ in range(n):
-            t0 = time.perf_counter()
-            r = pl.plan_host(start, goal, obs)
-            dt = time.perf_counter() - t0
-            secs += dt
-            valid += r.valid_expansions
-            iters.append(r.iters)
-            if r.found:
-                found += 1
-                tts.append(1000 * dt)
-                costs.append(float(r.path_cost))
+        for cap, ref_cfg in ((400000, "quad_ref"), (1 << 22, "quad_ref_4m")):
+            cfg = kpax.preset(kpax.PRESET_QUAD_REF)
+            cfg.seed = cfg.seed + 1000003 * rank
+            cfg.max_tree_size = cap
+            cfg.expansions_per_iter = cap
+            sides.append({"tree_capacity": cap, "ours": ours_plans(cfg, obs, start, goal, n, args.warmup), "cfg": cfg,
+                          "ref_cfg": ref_cfg})
     launches = kpax.kernel_launches() - launches0
-    pl.close()
-    ours = {"plans": n, "success_rate": found / n, "tts_ms_p50": float(np.percentile(tts, 50)) if tts else None,
-            "tts_ms_p95": float(np.percentile(tts, 95)) if tts else None,
-            "path_cost_median": float(np.median(costs)) if costs else None,
-            "iterations_median": float(np.median(iters)), "valid_expansions_per_s": valid / secs}
-    ref = None
-    if rank == 0 and not args.no_ref_cuda:
-        sys.path.insert(0, str(ROOT / "oracle" / "refcuda"))
-        import refcuda
-
-        rs = refcuda.summarise(refcuda.run("quad_ref", obs, [[*start[:3], *goal[:3]]], iteration_cap=cfg.max_iter,
-                                           repeats=n, timeout_s=600))
-        if "unavailable" in rs:
-            ref = rs
-        else:
-            t = rs["tts_ms"]
-            ref = {"plans": rs["plans"], "success_rate": rs["success_rate"],
-                   "tts_ms_p50": float(np.percentile(t, 50)) if t else None,
-                   "tts_ms_p95": float(np.percentile(t, 95)) if t else None,
-                   "path_cost_median": float(np.median(rs["path_costs"])) if rs["path_costs"] else None,
-                   "capacity_stops": rs["capacity_stops"], "valid_expansions_per_s": rs["value"],
-                   "kind": "reference CUDA build: KPAX::plan from its own sources, sm_100a; seeds from the wall clock "
-                           "as in the reference (KPAX.cu:90-91)",
-                   "path_cost_ks_vs_ours": ks_distance(costs, rs["path_costs"])}
+    for sd in sides:
+        ref = None
+        if rank == 0 and not args.no_ref_cuda:
+            ref = reference_plans(sd["ref_cfg"], obs, start, goal, n, sd["cfg"].max_iter)
+            if "path_costs" in ref:
+                ref["path_cost_ks_vs_ours"] = ks_distance(sd["ours"]["path_costs"], ref.pop("path_costs"))
+        sd["reference_cuda"] = ref
+        sd["ours"].pop("path_costs")
+        del sd["cfg"], sd["ref_cfg"]
     if rank == 0:
-        value = valid / secs
+        head = sides[0]["ours"]
+        value = head["valid_expansions_per_s"]
+        cfg = kpax.preset(kpax.PRESET_QUAD_REF)
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": n, "warmup": args.warmup,
-                "ms_per_step": 1000 * secs / n, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "ms_per_step": 1000 * head["seconds"] / n, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "fp32", "data": "the reference's quadTrees obstacle file",
                 "config": {"workload": QUAD_REF_DESC, "expansions_per_iter": cfg.expansions_per_iter,
                            "l2": "whole plans back to back (each plan's data is larger than L2 only late in a plan)",
                            "parallelism": f"replicas x{ws}"},
                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": obs.nbytes + 2 * 4 * cfg.sample_dim,
-                        "d2h_bytes_per_step": 128, "plans": n, "success_rate": ours["success_rate"],
-                        "tts_ms_p50": ours["tts_ms_p50"], "tts_ms_p95": ours["tts_ms_p95"]},
-                "plan_outcomes": {"ours": ours, "reference_cuda": ref}, "gpu_launches": launches,
-                "clocks": clk.summary()}
+                        "d2h_bytes_per_step": 128, "plans": n, "success_rate": head["success_rate"],
+                        "tts_ms_p50": head["tts_ms_p50"], "tts_ms_p95": head["tts_ms_p95"]},
+                "plan_outcomes": sides, "gpu_launches": launches, "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
 
 

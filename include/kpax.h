@@ -229,7 +229,7 @@ kpax_status kpax_env_stats(kpax_env* env, uint32_t* n_cells, uint32_t* n_entries
  *  d_rows:    n x SAMPLE_DIM output rows (state after the last executed step, controls,
  *             duration) exactly as the reference writes x1.
  *  d_valid:   n bytes, 1 = collision free and within bounds.  d_steps (optional): executed steps.
- * Batches of 2^18 segments or more run in rounds of up to 2^19 segments, three phases each, whose
+ * Batches of 2^18 segments or more run in rounds of up to 2^24 segments, three phases each, whose
  * survivor lists use scratch held by `env` (about 2 x 4 x (1 + control_dim + state_dim) bytes per
  * segment of a round, plus 4 per segment for drawn durations; kept for later calls and freed by
  * kpax_env_destroy), so calls that share an env must be issued in order on one stream. */
