@@ -974,6 +974,9 @@ def run_batch(args) -> None:
     torch.cuda.set_device(local)
     queries = E.batch_queries(args.queries, seed=4 + 1000 * rank)
     cfgs = batch_configs(queries)
+    if args.batch_iters:  # solvability study: more iterations per query than the presets' 300
+        for c in cfgs:
+            c.max_iter = args.batch_iters
     tuned_models = {}
     if not args.no_tune:  # per model: the cached parameters of its single-query workload
         import kpax_autotune
@@ -1003,7 +1006,7 @@ def run_batch(args) -> None:
         batch.plan(starts, goals, ptrs, sizes)
     launches0 = kpax.kernel_launches()
     tot_ms, tot_valid, wall, tts, found, n_plans = 0.0, 0, 0.0, [], 0, 0
-    per_model = {m: [0, 0] for m in (1, 2, 3)}
+    per_model = {m: [0, 0, 0] for m in (1, 2, 3)}  # plans, solved, trees filled before the goal
     with Clocks(local) as clk:
         for _ in range(args.steps):
             torch.cuda.synchronize()
@@ -1016,6 +1019,7 @@ def run_batch(args) -> None:
             n_plans += len(res)
             for d, r in zip(queries, res):
                 per_model[d["model"]][0] += 1
+                per_model[d["model"]][2] += int(bool(r["tree_full"]) and not r["found"])
                 if r["found"]:
                     found += 1
                     per_model[d["model"]][1] += 1
@@ -1037,6 +1041,9 @@ def run_batch(args) -> None:
         "success_rate": found / max(n_plans, 1),
         "success_by_model": {{1: "double_integrator", 2: "dubins", 3: "quadrotor"}[m]: v[1] / max(v[0], 1)
                              for m, v in per_model.items()},
+        "tree_filled_unsolved_by_model": {{1: "double_integrator", 2: "dubins", 3: "quadrotor"}[m]: v[2] / max(v[0], 1)
+                                          for m, v in per_model.items()},
+        "iterations_per_query": args.batch_iters or "presets' 300",
         "tts_ms_p50": float(np.percentile(tts, 50)) if tts else None,
         "tts_ms_p95": float(np.percentile(tts, 95)) if tts else None,
         "e2e": {"value": tot_valid / wall, "unit": UNIT, "h2d_bytes_per_step": int(h_obs.numel() * 4),
@@ -1154,6 +1161,7 @@ def main() -> None:
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "learned", "segments", "collide", "quad-ref"],
                     default="quad")
     ap.add_argument("--plans-ref", type=int, default=256, help="plans per side of the quad-ref workload")
+    ap.add_argument("--batch-iters", type=int, default=0, help="iteration cap of every batched query (0 = presets)")
     ap.add_argument("--seeds", type=int, default=256, help="held-out scenes of the learned workload")
     ap.add_argument("--eps", type=float, default=0.2, help="uniform fraction of the learned proposal")
     ap.add_argument("--proposal", choices=["on", "off"], default="on", help="learned proposal for batched quadrotor queries")
