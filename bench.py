@@ -589,7 +589,7 @@ def reference_plans(ref_cfg: str, obs, start, goal, n: int, iteration_cap: int) 
     import refcuda
 
     rs = refcuda.summarise(refcuda.run(ref_cfg, obs, [[*start[:3], *goal[:3]]], iteration_cap=iteration_cap, repeats=n,
-                                       timeout_s=900))
+                                       timeout_s=300))
     if "unavailable" in rs:
         return rs
     t = rs["tts_ms"]
@@ -619,23 +619,25 @@ def run_quad_ref(args) -> None:
     sides = []
     launches0 = kpax.kernel_launches()
     with Clocks(local) as clk:
-        for cap, ref_cfg in ((400000, "quad_ref"), (1 << 22, "quad_ref_4m")):
+        # the 2^22 capacity costs the reference a curand_init of 4M generator states per plan (and larger
+        # iterations): fewer plans there
+        for cap, ref_cfg, n_cap in ((400000, "quad_ref", n), (1 << 22, "quad_ref_4m", min(n, args.plans_ref_big))):
             cfg = kpax.preset(kpax.PRESET_QUAD_REF)
             cfg.seed = cfg.seed + 1000003 * rank
             cfg.max_tree_size = cap
             cfg.expansions_per_iter = cap
-            sides.append({"tree_capacity": cap, "ours": ours_plans(cfg, obs, start, goal, n, args.warmup), "cfg": cfg,
-                          "ref_cfg": ref_cfg})
+            sides.append({"tree_capacity": cap, "ours": ours_plans(cfg, obs, start, goal, n_cap, args.warmup), "cfg": cfg,
+                          "ref_cfg": ref_cfg, "n": n_cap})
     launches = kpax.kernel_launches() - launches0
     for sd in sides:
         ref = None
         if rank == 0 and not args.no_ref_cuda:
-            ref = reference_plans(sd["ref_cfg"], obs, start, goal, n, sd["cfg"].max_iter)
+            ref = reference_plans(sd["ref_cfg"], obs, start, goal, sd["n"], sd["cfg"].max_iter)
             if "path_costs" in ref:
                 ref["path_cost_ks_vs_ours"] = ks_distance(sd["ours"]["path_costs"], ref.pop("path_costs"))
         sd["reference_cuda"] = ref
         sd["ours"].pop("path_costs")
-        del sd["cfg"], sd["ref_cfg"]
+        del sd["cfg"], sd["ref_cfg"], sd["n"]
     if rank == 0:
         head = sides[0]["ours"]
         value = head["valid_expansions_per_s"]
@@ -1161,6 +1163,7 @@ def main() -> None:
     ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "learned", "segments", "collide", "quad-ref"],
                     default="quad")
     ap.add_argument("--plans-ref", type=int, default=256, help="plans per side of the quad-ref workload")
+    ap.add_argument("--plans-ref-big", type=int, default=32, help="plans per side at the 2^22 tree capacity (quad-ref)")
     ap.add_argument("--batch-iters", type=int, default=0, help="iteration cap of every batched query (0 = presets)")
     ap.add_argument("--seeds", type=int, default=256, help="held-out scenes of the learned workload")
     ap.add_argument("--eps", type=float, default=0.2, help="uniform fraction of the learned proposal")
