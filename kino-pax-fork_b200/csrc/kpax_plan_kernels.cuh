@@ -66,7 +66,8 @@ struct alignas(16) Ctl {
     uint32_t tree, tree_old, iter, R, k, E, n, appended;
     uint32_t goal_idx, done, full, error;
     uint32_t plan_idx, max_iters, stop_at_goal, epoch;
-    uint32_t iters_done, path_len, scores_ready, pad0;
+    uint32_t iters_done, path_len, scores_ready;
+    uint32_t stop_req;  // persistent batch stages: the query is to finish at the next iteration's start
     float faccept, goal[3];
     float score_total, pad1[3];
     unsigned long long n_exp, n_valid, n_steps;
@@ -134,6 +135,14 @@ __device__ __forceinline__ void finish_query(Ctl* ctl, uint32_t* active)
         ctl->t_done_ns = globaltimer();
         if(active) atomicSub(active, 1u);
     }
+}
+
+// The persistent batch stages never change `done` inside a stage (their CTAs derive their work
+// from it): a query that is to stop records the request and its time, and k_batch_start applies
+// it before the next iteration's first stage.
+__device__ __forceinline__ void request_finish(Ctl* ctl)
+{
+    if(atomicExch(&ctl->stop_req, 1u) == 0u) ctl->t_done_ns = globaltimer();
 }
 
 // Status word: [epoch:30 | flag:2 | value:32]; flag 1 = block aggregate, 2 = inclusive prefix.
@@ -340,6 +349,48 @@ __device__ __forceinline__ uint32_t scan_tiles(uint32_t* tiles, uint32_t n, uint
     return *s_carry;
 }
 
+// Tile b of the frontier count (kFrontierBS threads): repeats of its kTile nodes resolved, their sum
+// stored in tiles[b].
+__device__ __forceinline__ void count_tile(const QueryDev& sq, uint32_t b, uint32_t tree, uint32_t tree_old, uint32_t iter,
+                                           uint32_t plan, float fa, float total, uint32_t ready, uint32_t* s_warp)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t sum = 0;
+#pragma unroll
+    for(int j = 0; j < kItems; ++j) {
+        const uint32_t i = b * kTile + j * kFrontierBS + threadIdx.x;  // coalesced
+        if(i < tree) sum += resolve_repeat(sq.p, sq.t, sq.rg, i, tree_old, iter, plan, fa, total, ready);
+    }
+#pragma unroll
+    for(int d = 16; d > 0; d >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, d);
+    if(lane == 0) s_warp[warp] = sum;
+    __syncthreads();
+    if(threadIdx.x == 0) {
+        uint32_t acc = 0;
+        for(int w = 0; w < kFrontierBS / 32; ++w) acc += s_warp[w];
+        sq.tiles[b] = acc;
+    }
+    __syncthreads();
+}
+
+// The budget of an iteration (KPAX.cu:323-350) from its frontier's R entries, by one thread:
+// k children per entry and E entries taken, or B == 0 (the tree is full).
+__device__ __forceinline__ void set_budget(const KParams& p, Ctl* ctl, uint64_t R, uint32_t tree, uint32_t& B)
+{
+    B = min(p.budget, p.cap - tree);
+    uint32_t k = p.per_entry, E = 0, n = 0;
+    if(B != 0 && R) {
+        if(R * k > B) {
+            k = (uint32_t)(B / R);
+            if(k == 0) k = 1;
+        }
+        E = (uint32_t)(R < (uint64_t)(B / k) ? R : (uint64_t)(B / k));
+        n = E * k;
+    }
+    ctl->R = (uint32_t)R;
+    ctl->k = k, ctl->E = E, ctl->n = n;
+}
+
 __global__ void __launch_bounds__(kFrontierBS, kFrontierMinBlocks) k_frontier_count(const QueryDev* __restrict__ qs, uint32_t* __restrict__ active)
 {
     __shared__ QueryDev sq;
@@ -348,7 +399,6 @@ __global__ void __launch_bounds__(kFrontierBS, kFrontierMinBlocks) k_frontier_co
     load_query(qs, nullptr, sq);
     const KParams& p = sq.p;
     Ctl* ctl = sq.ctl;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     wait_predecessor();
     release_successor();
     if(__syncthreads_or(ctl->done != 0u)) return;  // one decision for the whole block: barriers follow
@@ -356,24 +406,8 @@ __global__ void __launch_bounds__(kFrontierBS, kFrontierMinBlocks) k_frontier_co
     const uint32_t ready = ctl->scores_ready;
     const float fa = ctl->faccept, total = ctl->score_total;
     const uint32_t ntiles = (tree + kTile - 1) / kTile;
-    for(uint32_t b = blockIdx.x; b < ntiles; b += gridDim.x) {
-        uint32_t sum = 0;
-#pragma unroll
-        for(int j = 0; j < kItems; ++j) {
-            const uint32_t i = b * kTile + j * kFrontierBS + threadIdx.x;  // coalesced
-            if(i < tree) sum += resolve_repeat(p, sq.t, sq.rg, i, tree_old, iter, plan, fa, total, ready);
-        }
-#pragma unroll
-        for(int d = 16; d > 0; d >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, d);
-        if(lane == 0) s_warp[warp] = sum;
-        __syncthreads();
-        if(threadIdx.x == 0) {
-            uint32_t acc = 0;
-            for(int w = 0; w < kFrontierBS / 32; ++w) acc += s_warp[w];
-            sq.tiles[b] = acc;
-        }
-        __syncthreads();
-    }
+    for(uint32_t b = blockIdx.x; b < ntiles; b += gridDim.x)
+        count_tile(sq, b, tree, tree_old, iter, plan, fa, total, ready, s_warp);
     __threadfence();
     __syncthreads();
     if(threadIdx.x == 0) s_last = atomicAdd(sq.farr, 1u) == gridDim.x - 1u;
@@ -383,23 +417,51 @@ __global__ void __launch_bounds__(kFrontierBS, kFrontierMinBlocks) k_frontier_co
     const uint32_t R32 = scan_tiles(sq.tiles, ntiles, s_warp, &s_carry);  // exclusive prefixes; total R
     if(threadIdx.x == 0) {  // the budget of this iteration (KPAX.cu:323-350)
         *sq.farr = 0u;
-        const uint64_t R = R32;
-        const uint32_t B = min(p.budget, p.cap - tree);
-        uint32_t k = p.per_entry, E = 0, n = 0;
+        uint32_t B = 0;
+        set_budget(p, ctl, R32, tree, B);
         if(B == 0) {
             ctl->full = 1u;
             finish_query(ctl, active);
-        } else if(R) {
-            if(R * k > B) {
-                k = (uint32_t)(B / R);
-                if(k == 0) k = 1;
-            }
-            E = (uint32_t)(R < (uint64_t)(B / k) ? R : (uint64_t)(B / k));
-            n = E * k;
         }
-        ctl->R = (uint32_t)R;
-        ctl->k = k, ctl->E = E, ctl->n = n;
     }
+}
+
+// Tile b of the entry list (kFrontierBS threads, kItems consecutive nodes each): node i owns virtual
+// entries [a, a + rep) with a from the tile scan.
+__device__ __forceinline__ void write_tile(const QueryDev& sq, uint32_t b, uint32_t tree, uint64_t R, uint32_t E,
+                                           uint32_t* s_warp)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const TreeDev& t = sq.t;
+    const uint32_t i0 = b * kTile + threadIdx.x * kItems;  // consecutive nodes per thread
+    uint32_t cnt[kItems], sum = 0;
+#pragma unroll
+    for(int j = 0; j < kItems; ++j) {
+        const uint32_t i = i0 + j;
+        cnt[j] = i < tree ? (uint32_t)t.rep[i] : 0u;
+        sum += cnt[j];
+    }
+    uint32_t x = sum;
+#pragma unroll
+    for(int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+        if(lane >= d) x += y;
+    }
+    if(lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    uint32_t wex = 0;
+    for(int w = 0; w < warp; ++w) wex += s_warp[w];
+    uint64_t a = (uint64_t)__ldcg(sq.tiles + b) + wex + x - sum;
+#pragma unroll
+    for(int j = 0; j < kItems; ++j) {
+        if(!cnt[j]) continue;
+        const uint64_t bnd = a + cnt[j];
+        const uint64_t lo = (a * E + R - 1) / R, hi = (bnd * E + R - 1) / R;
+        for(uint64_t e = lo; e < hi; ++e) sq.entries[e] = i0 + j;
+        if(lo < hi) t.rep[i0 + j] = 0;
+        a = bnd;
+    }
+    __syncthreads();
 }
 
 // Node i owns virtual entries [a, a + rep) with a from the tile scan.  Entry j of the E taken is
@@ -410,7 +472,6 @@ __global__ void __launch_bounds__(kFrontierBS) k_frontier_write(const QueryDev* 
     __shared__ QueryDev sq;
     __shared__ uint32_t s_warp[kFrontierBS / 32];
     load_query(qs, nullptr, sq);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     Ctl* ctl = sq.ctl;
     wait_predecessor();
     release_successor();
@@ -419,38 +480,7 @@ __global__ void __launch_bounds__(kFrontierBS) k_frontier_write(const QueryDev* 
     const uint64_t R = ctl->R;
     if(E == 0) return;
     const uint32_t ntiles = (tree + kTile - 1) / kTile;
-    const TreeDev& t = sq.t;
-    for(uint32_t b = blockIdx.x; b < ntiles; b += gridDim.x) {
-        const uint32_t i0 = b * kTile + threadIdx.x * kItems;  // consecutive nodes per thread
-        uint32_t cnt[kItems], sum = 0;
-#pragma unroll
-        for(int j = 0; j < kItems; ++j) {
-            const uint32_t i = i0 + j;
-            cnt[j] = i < tree ? (uint32_t)t.rep[i] : 0u;
-            sum += cnt[j];
-        }
-        uint32_t x = sum;
-#pragma unroll
-        for(int d = 1; d < 32; d <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
-            if(lane >= d) x += y;
-        }
-        if(lane == 31) s_warp[warp] = x;
-        __syncthreads();
-        uint32_t wex = 0;
-        for(int w = 0; w < warp; ++w) wex += s_warp[w];
-        uint64_t a = (uint64_t)sq.tiles[b] + wex + x - sum;
-#pragma unroll
-        for(int j = 0; j < kItems; ++j) {
-            if(!cnt[j]) continue;
-            const uint64_t bnd = a + cnt[j];
-            const uint64_t lo = (a * E + R - 1) / R, hi = (bnd * E + R - 1) / R;
-            for(uint64_t e = lo; e < hi; ++e) sq.entries[e] = i0 + j;
-            if(lo < hi) t.rep[i0 + j] = 0;
-            a = bnd;
-        }
-        __syncthreads();
-    }
+    for(uint32_t b = blockIdx.x; b < ntiles; b += gridDim.x) write_tile(sq, b, tree, R, E, s_warp);
 }
 
 // Shared-memory scratch of the expansion tiles of one block.
@@ -468,7 +498,7 @@ struct ExpandSmem {
 // with an error).
 template <int M, int BS>
 __device__ __forceinline__ bool expand_tiles(QueryDev& sq, uint32_t n, uint32_t k, uint32_t first, uint32_t stride,
-                                             uint32_t* __restrict__ active, ExpandSmem<BS / 32>& sm)
+                                             uint32_t* __restrict__ active, ExpandSmem<BS / 32>& sm, bool defer_finish = false)
 {
     constexpr int SD = ModelDims<M>::SD, CD = ModelDims<M>::CD, S = SD + CD + 1;
     constexpr int NW = BS / 32;
@@ -544,7 +574,8 @@ __device__ __forceinline__ bool expand_tiles(QueryDev& sq, uint32_t n, uint32_t 
                 if(ns) atomicAdd(&ctl->n_steps, ns);
                 if(!ok) {
                     atomicOr(&ctl->error, kErrTimeout);
-                    finish_query(ctl, active);
+                    if(defer_finish) request_finish(ctl);
+                    else finish_query(ctl, active);
                 }
                 if(ok && b == ntile - 1) ctl->appended = excl + acc;
                 sm.excl = excl;
@@ -638,7 +669,8 @@ __device__ __forceinline__ void score_partials(const QueryDev& sq, uint32_t gtid
 
 // Total of the partials by one block (all threads; s_part holds kPartials floats), then the
 // iteration's bookkeeping by thread 0: tree size, fAccept (KPAX.cu:527-528), counters, stop flags.
-__device__ __forceinline__ void score_finish(const QueryDev& sq, float* s_part, uint32_t* __restrict__ active)
+__device__ __forceinline__ void score_finish(const QueryDev& sq, float* s_part, uint32_t* __restrict__ active,
+                                             bool defer_finish = false)
 {
     const KParams& p = sq.p;
     Ctl* ctl = sq.ctl;
@@ -672,7 +704,10 @@ __device__ __forceinline__ void score_finish(const QueryDev& sq, float* s_part, 
         ctl->iters_done = iter;
         ctl->iter = iter + 1u;
         ctl->epoch = vc->epoch + 1u;
-        if((vc->goal_idx != kNone && vc->stop_at_goal) || iter >= vc->max_iters) finish_query(ctl, active);
+        if((vc->goal_idx != kNone && vc->stop_at_goal) || iter >= vc->max_iters) {
+            if(defer_finish) request_finish(ctl);
+            else finish_query(ctl, active);
+        }
     }
 }
 

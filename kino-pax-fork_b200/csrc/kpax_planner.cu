@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "kpax_batch_kernels.cuh"
 #include "kpax_internal.h"
 #include "kpax_plan_kernels.cuh"
 
@@ -90,6 +91,30 @@ void launch_iterate(int bs, uint32_t gx, cudaStream_t s, const QueryDev* dq, uin
     }
 }
 
+// The persistent expansion of a batch's model group at one of its block sizes.
+template <int M>
+void* expand_all_kernel(int bs)
+{
+    switch(bs) {
+        case 128: return (void*)k_expand_all<M, 128>;
+        case 256: return (void*)k_expand_all<M, 256>;
+        case 512: return (void*)k_expand_all<M, 512>;
+        default: return (void*)k_expand_all<M, kExpandBS>;
+    }
+}
+
+template <int M>
+void launch_expand_all(int bs, uint32_t gx, size_t smem, cudaStream_t s, const QueryDev* dq, const Ctl* ctls,
+                       const uint32_t* qidx, uint32_t nq, uint32_t* active)
+{
+    switch(bs) {
+        case 128: launch_chained(k_expand_all<M, 128>, dim3(gx), 128, smem, s, dq, ctls, qidx, nq, active); break;
+        case 256: launch_chained(k_expand_all<M, 256>, dim3(gx), 256, smem, s, dq, ctls, qidx, nq, active); break;
+        case 512: launch_chained(k_expand_all<M, 512>, dim3(gx), 512, smem, s, dq, ctls, qidx, nq, active); break;
+        default: launch_chained(k_expand_all<M, kExpandBS>, dim3(gx), kExpandBS, smem, s, dq, ctls, qidx, nq, active); break;
+    }
+}
+
 struct PlanBatch {
     uint32_t nq = 0;
     std::vector<kpax_config> cfg;
@@ -105,6 +130,8 @@ struct PlanBatch {
     uint32_t expand_gx[3] = {0, 0, 0};
     int expand_bs[3] = {kExpandBS, kExpandBS, kExpandBS};  // block size per model group (its first query's)
     uint32_t gx_front = 1, gx_score = 1;
+    bool persistent = false;  // batch: persistent stage launches over all queries (per-query offsets)
+    uint32_t gx_count_all = 0, gx_write_all = 0, gx_scores_all = 0, gx_expand_all[3] = {0, 0, 0};
     bool fused = false;      // single query without the proposal: one k_iterate launch per iteration
     uint32_t gx_iter = 0;    // its CTAs (all resident), 0 when the kernel cannot be used
     Ctl* d_ctl = nullptr;
@@ -255,6 +282,32 @@ struct PlanBatch {
             const uint32_t resident = (uint32_t)std::max(per_sm, 0) * (uint32_t)sms;
             gx_iter = std::min<uint32_t>(std::min<uint32_t>(expand_gx[m], resident), (uint32_t)kIterMaxCTAs);
         }
+        if(n > 1 && n <= kBatchMaxQueries) {  // persistent stages: grids of resident CTAs
+            int dev = 0, sms = 148;
+            KPAX_CUDA(cudaGetDevice(&dev));
+            KPAX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            auto resident = [&](const void* fn, int bs, size_t smem, uint32_t& gx) -> kpax_status {
+                int per_sm = 0;
+                KPAX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, bs, smem));
+                gx = (uint32_t)std::max(per_sm, 0) * (uint32_t)sms;
+                return KPAX_OK;
+            };
+            const size_t sq = 4 * ((size_t)n + 1);
+            kpax_status st = resident((const void*)k_count_all, kFrontierBS, sq, gx_count_all);
+            if(st == KPAX_OK) st = resident((const void*)k_write_all, kFrontierBS, sq, gx_write_all);
+            if(st == KPAX_OK) st = resident((const void*)k_scores_all, kScoreBS, sq, gx_scores_all);
+            for(int m = 0; m < 3 && st == KPAX_OK; ++m) {
+                if(groups[m].empty()) continue;
+                const size_t sg = 4 * (groups[m].size() + 1);
+                const void* fn = m == 0 ? expand_all_kernel<KPAX_MODEL_DOUBLE_INTEGRATOR>(expand_bs[m])
+                                        : m == 1 ? expand_all_kernel<KPAX_MODEL_DUBINS_AIRPLANE>(expand_bs[m])
+                                                 : expand_all_kernel<KPAX_MODEL_QUADROTOR>(expand_bs[m]);
+                st = resident(fn, expand_bs[m], sg, gx_expand_all[m]);
+            }
+            if(st != KPAX_OK) return st;
+            persistent = gx_count_all && gx_write_all && gx_scores_all && (groups[0].empty() || gx_expand_all[0]) &&
+                         (groups[1].empty() || gx_expand_all[1]) && (groups[2].empty() || gx_expand_all[2]);
+        }
         update_fused();
         // control blocks, counters and arrival flags start at zero; no node is in a frontier
         KPAX_CUDA(cudaMemsetAsync(pool, 0, region_lo, stream));
@@ -334,6 +387,35 @@ struct PlanBatch {
             if(m == 0) launch_iterate<KPAX_MODEL_DOUBLE_INTEGRATOR>(expand_bs[m], gx_iter, stream, dq, d_active);
             else if(m == 1) launch_iterate<KPAX_MODEL_DUBINS_AIRPLANE>(expand_bs[m], gx_iter, stream, dq, d_active);
             else launch_iterate<KPAX_MODEL_QUADROTOR>(expand_bs[m], gx_iter, stream, dq, d_active);
+            if(ev) cudaEventRecord(ev[3], stream);
+            return;
+        }
+        if(persistent) {  // one launch per stage over all queries; model groups one after another
+            const size_t sq = 4 * ((size_t)nq + 1);
+            launch_chained(k_batch_start, dim3((nq + kBatchStartBS - 1) / kBatchStartBS), kBatchStartBS, 0, stream, d_ctl, nq,
+                           d_active);
+            launch_chained(k_count_all, dim3(gx_count_all), kFrontierBS, sq, stream, dq, (const Ctl*)d_ctl, nq);
+            launch_chained(k_write_all, dim3(gx_write_all), kFrontierBS, sq, stream, dq, (const Ctl*)d_ctl, nq);
+            if(ev && split) cudaEventRecord(ev[1], stream);
+            if(n_learned)
+                launch_chained(k_propose, dim3(gx_prop, n_learned), mlp::tc::kThreads, mlp::tc::kSmemBytes, stream, dq,
+                               d_learned);
+            for(int m = 0; m < 3; ++m) {
+                if(groups[m].empty()) continue;
+                const uint32_t g = (uint32_t)groups[m].size();
+                const size_t sg = 4 * ((size_t)g + 1);
+                if(m == 0)
+                    launch_expand_all<KPAX_MODEL_DOUBLE_INTEGRATOR>(expand_bs[m], gx_expand_all[m], sg, stream, dq, d_ctl,
+                                                                    d_groups[m], g, d_active);
+                else if(m == 1)
+                    launch_expand_all<KPAX_MODEL_DUBINS_AIRPLANE>(expand_bs[m], gx_expand_all[m], sg, stream, dq, d_ctl,
+                                                                  d_groups[m], g, d_active);
+                else
+                    launch_expand_all<KPAX_MODEL_QUADROTOR>(expand_bs[m], gx_expand_all[m], sg, stream, dq, d_ctl,
+                                                            d_groups[m], g, d_active);
+            }
+            if(ev && split) cudaEventRecord(ev[2], stream);
+            launch_chained(k_scores_all, dim3(gx_scores_all), kScoreBS, sq, stream, dq, (const Ctl*)d_ctl, nq, d_active);
             if(ev) cudaEventRecord(ev[3], stream);
             return;
         }
@@ -432,6 +514,11 @@ struct PlanBatch {
     uint64_t kernels_per_iteration() const
     {
         if(fused) return 1;
+        if(persistent) {  // start, count, write, (proposal), one expansion per model group, scores
+            uint64_t k = n_learned ? 5 : 4;
+            for(int m = 0; m < 3; ++m) k += groups[m].empty() ? 0 : 1;
+            return k;
+        }
         uint64_t k = n_learned ? 4 : 3;  // two frontier passes, the score pass, the proposal pass
         for(int m = 0; m < 3; ++m) k += groups[m].empty() ? 0 : 1;
         return k;
@@ -565,6 +652,7 @@ struct PlanBatch {
             Ctl& c = h_ctl[q];
             c.max_iters = c.iters_done + n;
             c.stop_at_goal = stop_at_goal;
+            c.stop_req = 0;  // a stop the batch stages requested is decided again
             c.done = (c.full || c.error || (stop_at_goal && c.goal_idx != kNone)) ? 1u : 0u;
             act += c.done ? 0u : 1u;
         }

@@ -77,3 +77,58 @@ def test_second_batch_plan_uses_a_new_random_stream(cuda):
     assert (second.tree_size, second.iters, second.valid_expansions) == (r2[0]["tree_size"], r2[0]["iters"],
                                                                           r2[0]["valid_expansions"])
     batch.close()
+
+
+def test_persistent_stages_over_many_uneven_queries(cuda):
+    """24 queries of uneven size in one batch (the stages run as persistent launches over all
+    queries' work, with per-query offsets): trees from 2^10 to 2^16 nodes, some filling before
+    their goal, some reaching it in a few iterations, some planning with no obstacles.  Every query
+    must give its single plan."""
+    import torch
+
+    rng = np.random.default_rng(5)
+    dobs, ds, dg = E.dubins_scene()
+    qobs, qs_, qg = E.quad_scene(n_total=300)
+    obs0, s0, _ = E.di_scene()
+    qs = []
+    for i in range(24):
+        kind = i % 3
+        if kind == 0:
+            c = kpax.preset(kpax.PRESET_DI)
+            c.max_tree_size = int(2 ** rng.integers(10, 15))
+            c.expansions_per_iter = min(c.max_tree_size, 1 << 11)
+            c.max_iter, c.seed = 25, 100 + i
+            c.v_min, c.v_max = -5.0, 5.0
+            for k in range(3):
+                c.ctrl_min[k], c.ctrl_max[k] = -4.0, 4.0
+            goal = np.array([rng.uniform(20, 60), rng.uniform(20, 60), rng.uniform(20, 60), 0, 0, 0], np.float32)
+            qs.append((c, obs0 if i % 2 else np.zeros((0, 6), np.float32), s0, goal))
+        elif kind == 1:
+            c = kpax.preset(kpax.PRESET_DUBINS)
+            c.max_tree_size = int(2 ** rng.integers(12, 17))
+            c.expansions_per_iter = min(c.max_tree_size, 1 << 12)
+            c.max_iter, c.seed = 10, 200 + i
+            qs.append((c, dobs, ds, dg))
+        else:
+            c = kpax.preset(kpax.PRESET_QUAD)
+            c.max_tree_size = int(2 ** rng.integers(12, 17))
+            c.expansions_per_iter = min(c.max_tree_size, 1 << 12)
+            c.max_iter, c.seed = 8, 300 + i
+            qs.append((c, qobs, qs_, qg))
+    d_obs = [torch.from_numpy(np.ascontiguousarray(o, np.float32)).cuda() if o.size else None for _, o, _, _ in qs]
+    ptrs = [d.data_ptr() if d is not None else 0 for d in d_obs]
+    batch = kpax.Batch([c for c, _, _, _ in qs])
+    res, stats = batch.plan([s for _, _, s, _ in qs], [g for _, _, _, g in qs], ptrs, [o.shape[0] for _, o, _, _ in qs])
+    full = found = 0
+    for q, (cfg, obs, s, g) in enumerate(qs):
+        pl = kpax.KPAX(cfg)
+        r = pl.plan(s, g, ptrs[q], obs.shape[0])
+        single = {f: getattr(r, f) for f in ("found", "goal_idx", "path_len", "tree_size", "iters", "tree_full",
+                                              "expansions", "valid_expansions", "path_cost")}
+        assert {f: res[q][f] for f in single} == single, (q, single, {f: res[q][f] for f in single})
+        full += int(r.tree_full)
+        found += int(r.found)
+        pl.close()
+    assert full >= 1 and found >= 1, (full, found)  # both early exits are exercised
+    assert stats["found"] == found
+    batch.close()
