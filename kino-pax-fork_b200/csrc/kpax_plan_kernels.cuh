@@ -744,7 +744,7 @@ __global__ void __launch_bounds__(kScoreBS) k_scores(const QueryDev* __restrict_
 // arithmetic, same partial sums), so plans are bit-identical to the per-stage path.
 
 constexpr int kIterMaxCTAs = 1024;  // CTAs of a k_iterate launch
-constexpr int kIterBatch = 16;      // nodes per thread whose loads are issued together
+constexpr int kIterBatch = 8;       // nodes per thread whose loads are issued together
 
 __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p)
 {
