@@ -200,6 +200,44 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_expand_al
     }
 }
 
+// Expansion of all queries of every model in one launch (their models share the block size BS):
+// the same units as k_expand_all over qidx, which lists the quadrotor queries first, then Dubins,
+// then the double integrator, so the costliest tiles are taken first and the cheap ones fill the
+// launch's tail.  Each unit runs the expansion of its query's model.
+template <int BS>
+__global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_expand_mixed(const QueryDev* __restrict__ qs,
+                                                                                  const Ctl* __restrict__ ctls,
+                                                                                  const uint32_t* __restrict__ qidx,
+                                                                                  uint32_t nq, uint32_t* __restrict__ active)
+{
+    extern __shared__ uint32_t s_off[];
+    __shared__ QueryDev sq;
+    __shared__ ExpandSmem<BS / 32> sm;
+    __shared__ uint32_t s_warp[BS / 32];
+    wait_predecessor();
+    const uint32_t total = query_offsets<BS / 32>(nq, s_off, s_warp, [&](uint32_t i) {
+        const Ctl& c = ctls[qidx[i]];
+        return (c.done || c.full) ? 0u : (c.n ? (c.n + BS - 1) / BS : 1u);
+    });
+    uint32_t cur = kNone, n = 0, k = 0;
+    int model = 0;
+    for(uint32_t g = blockIdx.x; g < total; g += gridDim.x) {
+        const uint32_t i = find_query(s_off, nq, g);
+        if(i != cur) {
+            load_query_at(qs, qidx[i], sq);
+            n = sq.ctl->n, k = sq.ctl->k, model = sq.p.model;
+            cur = i;
+        }
+        const uint32_t t = g - s_off[i];
+        bool ok;
+        if(model == KPAX_MODEL_QUADROTOR) ok = expand_tiles<KPAX_MODEL_QUADROTOR, BS>(sq, n, k, t, 0x80000000u, active, sm, true);
+        else if(model == KPAX_MODEL_DUBINS_AIRPLANE)
+            ok = expand_tiles<KPAX_MODEL_DUBINS_AIRPLANE, BS>(sq, n, k, t, 0x80000000u, active, sm, true);
+        else ok = expand_tiles<KPAX_MODEL_DOUBLE_INTEGRATOR, BS>(sq, n, k, t, 0x80000000u, active, sm, true);
+        if(!ok) return;
+    }
+}
+
 constexpr int kScoreUnitWarps = kScoreBS / 32;  // partial sums per score unit
 
 // Region scores of all queries: a unit is kScoreUnitWarps consecutive partial sums of one query (and

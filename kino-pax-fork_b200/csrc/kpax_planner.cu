@@ -115,6 +115,27 @@ void launch_expand_all(int bs, uint32_t gx, size_t smem, cudaStream_t s, const Q
     }
 }
 
+void* expand_mixed_kernel(int bs)
+{
+    switch(bs) {
+        case 128: return (void*)k_expand_mixed<128>;
+        case 256: return (void*)k_expand_mixed<256>;
+        case 512: return (void*)k_expand_mixed<512>;
+        default: return (void*)k_expand_mixed<kExpandBS>;
+    }
+}
+
+void launch_expand_mixed(int bs, uint32_t gx, size_t smem, cudaStream_t s, const QueryDev* dq, const Ctl* ctls,
+                         const uint32_t* qidx, uint32_t nq, uint32_t* active)
+{
+    switch(bs) {
+        case 128: launch_chained(k_expand_mixed<128>, dim3(gx), 128, smem, s, dq, ctls, qidx, nq, active); break;
+        case 256: launch_chained(k_expand_mixed<256>, dim3(gx), 256, smem, s, dq, ctls, qidx, nq, active); break;
+        case 512: launch_chained(k_expand_mixed<512>, dim3(gx), 512, smem, s, dq, ctls, qidx, nq, active); break;
+        default: launch_chained(k_expand_mixed<kExpandBS>, dim3(gx), kExpandBS, smem, s, dq, ctls, qidx, nq, active); break;
+    }
+}
+
 struct PlanBatch {
     uint32_t nq = 0;
     std::vector<kpax_config> cfg;
@@ -132,6 +153,10 @@ struct PlanBatch {
     uint32_t gx_front = 1, gx_score = 1;
     bool persistent = false;  // batch: persistent stage launches over all queries (per-query offsets)
     uint32_t gx_count_all = 0, gx_write_all = 0, gx_scores_all = 0, gx_expand_all[3] = {0, 0, 0};
+    // every model group at one block size: one mixed-model expansion over all queries, quadrotor first
+    int mixed_bs = 0;
+    uint32_t gx_mixed = 0;
+    uint32_t* d_mixed = nullptr;
     bool fused = false;      // single query without the proposal: one k_iterate launch per iteration
     uint32_t gx_iter = 0;    // its CTAs (all resident), 0 when the kernel cannot be used
     Ctl* d_ctl = nullptr;
@@ -280,7 +305,9 @@ struct PlanBatch {
                               : m == 1 ? iterate_kernel<KPAX_MODEL_DUBINS_AIRPLANE>(bs) : iterate_kernel<KPAX_MODEL_QUADROTOR>(bs);
             KPAX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, bs, 0));
             const uint32_t resident = (uint32_t)std::max(per_sm, 0) * (uint32_t)sms;
-            gx_iter = std::min<uint32_t>(std::min<uint32_t>(expand_gx[m], resident), (uint32_t)kIterMaxCTAs);
+            // every resident CTA: the frontier and score phases use them all, the expansion as many as
+            // it has tiles (a small budget's iteration leaves the rest idle in that phase)
+            gx_iter = std::min<uint32_t>(resident, (uint32_t)kIterMaxCTAs);
         }
         if(n > 1 && n <= kBatchMaxQueries) {  // persistent stages: grids of resident CTAs
             int dev = 0, sms = 148;
@@ -307,6 +334,24 @@ struct PlanBatch {
             if(st != KPAX_OK) return st;
             persistent = gx_count_all && gx_write_all && gx_scores_all && (groups[0].empty() || gx_expand_all[0]) &&
                          (groups[1].empty() || gx_expand_all[1]) && (groups[2].empty() || gx_expand_all[2]);
+            int bs0 = 0, ngroups = 0;
+            bool same_bs = true;
+            for(int m = 0; m < 3; ++m) {
+                if(groups[m].empty()) continue;
+                ++ngroups;
+                if(!bs0) bs0 = expand_bs[m];
+                same_bs = same_bs && expand_bs[m] == bs0;
+            }
+            if(persistent && ngroups > 1 && same_bs) {
+                std::vector<uint32_t> order;
+                for(int m = 2; m >= 0; --m) order.insert(order.end(), groups[m].begin(), groups[m].end());
+                KPAX_CUDA(cudaMalloc(&d_mixed, sizeof(uint32_t) * order.size()));
+                KPAX_CUDA(cudaMemcpyAsync(d_mixed, order.data(), sizeof(uint32_t) * order.size(), cudaMemcpyHostToDevice,
+                                          stream));
+                uint32_t gx = 0;
+                if((st = resident(expand_mixed_kernel(bs0), bs0, 4 * ((size_t)n + 1), gx)) != KPAX_OK) return st;
+                if(gx) mixed_bs = bs0, gx_mixed = gx;
+            }
         }
         update_fused();
         // control blocks, counters and arrival flags start at zero; no node is in a frontier
@@ -325,7 +370,7 @@ struct PlanBatch {
         for(Env& e : env) e.release();
         for(int m = 0; m < 3; ++m)
             if(d_groups[m]) cudaFree(d_groups[m]);
-        void* dev[] = {pool, dq, d_ctl, d_active, d_ig, d_path, d_flush, d_img, d_learn, d_learned};
+        void* dev[] = {pool, dq, d_ctl, d_active, d_ig, d_path, d_flush, d_img, d_learn, d_learned, d_mixed};
         for(void* p : dev)
             if(p) cudaFree(p);
         void* host[] = {h_ctl, h_active, h_ig, h_path};
@@ -400,7 +445,7 @@ struct PlanBatch {
             if(n_learned)
                 launch_chained(k_propose, dim3(gx_prop, n_learned), mlp::tc::kThreads, mlp::tc::kSmemBytes, stream, dq,
                                d_learned);
-            for(int m = 0; m < 3; ++m) {
+            for(int m = 0; m < 3 && !mixed_bs; ++m) {
                 if(groups[m].empty()) continue;
                 const uint32_t g = (uint32_t)groups[m].size();
                 const size_t sg = 4 * ((size_t)g + 1);
@@ -414,6 +459,7 @@ struct PlanBatch {
                     launch_expand_all<KPAX_MODEL_QUADROTOR>(expand_bs[m], gx_expand_all[m], sg, stream, dq, d_ctl,
                                                             d_groups[m], g, d_active);
             }
+            if(mixed_bs) launch_expand_mixed(mixed_bs, gx_mixed, sq, stream, dq, d_ctl, d_mixed, nq, d_active);
             if(ev && split) cudaEventRecord(ev[2], stream);
             launch_chained(k_scores_all, dim3(gx_scores_all), kScoreBS, sq, stream, dq, (const Ctl*)d_ctl, nq, d_active);
             if(ev) cudaEventRecord(ev[3], stream);
@@ -514,8 +560,9 @@ struct PlanBatch {
     uint64_t kernels_per_iteration() const
     {
         if(fused) return 1;
-        if(persistent) {  // start, count, write, (proposal), one expansion per model group, scores
+        if(persistent) {  // start, count, write, (proposal), the expansion(s), scores
             uint64_t k = n_learned ? 5 : 4;
+            if(mixed_bs) return k + 1;
             for(int m = 0; m < 3; ++m) k += groups[m].empty() ? 0 : 1;
             return k;
         }
