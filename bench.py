@@ -50,8 +50,9 @@ FLOP_PER_STEP = {kpax.MODEL_DOUBLE_INTEGRATOR: 18, kpax.MODEL_DUBINS_AIRPLANE: 5
 # L2 flushed before the iteration) in an ncu capture of the default workload; none for the others
 EXPAND_DRAM_BYTES = {kpax.MODEL_QUADROTOR: 1535744 + 0}
 # the same sum over the three phase kernels of one 2^20-segment Dubins batch (L2 flushed before the
-# step), per segment: scaled by the segment count, as the traffic grows with it
-PHASED_DRAM_BYTES_PER_SEGMENT = (118480128 + 29827072) / (1 << 20)
+# step, no cache flush between the kernels), per segment: scaled by the segment count, as the
+# traffic grows with it
+PHASED_DRAM_BYTES_PER_SEGMENT = (30508800 + 103499264) / (1 << 20)
 WORKLOADS = {
     "quad": (kpax.PRESET_QUAD, E.quad_scene, "12D quadrotor, building scene (1000 AABBs incl. windowed wall), "
              "2^16 expansions/iteration, 25 RK4 steps of 0.02 s"),
