@@ -2,6 +2,7 @@
 // capture of the iteration kernels (kpax_plan_kernels.cuh), and the C ABI for single plans
 // (KPAX::plan, KPAX.cu:51-115) and batches of independent queries.
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -157,6 +158,11 @@ struct PlanBatch {
     int mixed_bs = 0;
     uint32_t gx_mixed = 0;
     uint32_t* d_mixed = nullptr;
+    // the batch's expansion: 0 one block per child tile of every query, model groups on concurrent
+    // streams (the default: a model keeps its own occupancy); 1 persistent per model group, one
+    // after another; 2 one persistent launch for every model (KPAX_BATCH_EXPAND selects 1 or 2 for
+    // measurements)
+    int expand_mode = 0;
     bool fused = false;      // single query without the proposal: one k_iterate launch per iteration
     uint32_t gx_iter = 0;    // its CTAs (all resident), 0 when the kernel cannot be used
     Ctl* d_ctl = nullptr;
@@ -342,6 +348,7 @@ struct PlanBatch {
                 if(!bs0) bs0 = expand_bs[m];
                 same_bs = same_bs && expand_bs[m] == bs0;
             }
+            if(const char* e = getenv("KPAX_BATCH_EXPAND")) expand_mode = atoi(e) == 1 ? 1 : atoi(e) == 2 ? 2 : 0;
             if(persistent && ngroups > 1 && same_bs) {
                 std::vector<uint32_t> order;
                 for(int m = 2; m >= 0; --m) order.insert(order.end(), groups[m].begin(), groups[m].end());
@@ -445,21 +452,43 @@ struct PlanBatch {
             if(n_learned)
                 launch_chained(k_propose, dim3(gx_prop, n_learned), mlp::tc::kThreads, mlp::tc::kSmemBytes, stream, dq,
                                d_learned);
-            for(int m = 0; m < 3 && !mixed_bs; ++m) {
-                if(groups[m].empty()) continue;
-                const uint32_t g = (uint32_t)groups[m].size();
-                const size_t sg = 4 * ((size_t)g + 1);
-                if(m == 0)
-                    launch_expand_all<KPAX_MODEL_DOUBLE_INTEGRATOR>(expand_bs[m], gx_expand_all[m], sg, stream, dq, d_ctl,
-                                                                    d_groups[m], g, d_active);
-                else if(m == 1)
-                    launch_expand_all<KPAX_MODEL_DUBINS_AIRPLANE>(expand_bs[m], gx_expand_all[m], sg, stream, dq, d_ctl,
-                                                                  d_groups[m], g, d_active);
-                else
-                    launch_expand_all<KPAX_MODEL_QUADROTOR>(expand_bs[m], gx_expand_all[m], sg, stream, dq, d_ctl,
-                                                            d_groups[m], g, d_active);
+            if(expand_mode == 0) {  // per model group: one block per child tile of every query, groups concurrent
+                int used[3], nused = 0;
+                for(int m = 0; m < 3; ++m)
+                    if(!groups[m].empty()) used[nused++] = m;
+                if(nused > 1) cudaEventRecord(ev_fork, stream);
+                for(int u = 0; u < nused; ++u) {
+                    const int m = used[u];
+                    cudaStream_t s = stream;
+                    if(u < nused - 1) {
+                        s = side[u];
+                        cudaStreamWaitEvent(s, ev_fork, 0);
+                    }
+                    const dim3 grid(expand_gx[m], (uint32_t)groups[m].size());
+                    if(m == 0) launch_expand<KPAX_MODEL_DOUBLE_INTEGRATOR>(expand_bs[m], grid, s, dq, d_groups[m], d_active);
+                    else if(m == 1) launch_expand<KPAX_MODEL_DUBINS_AIRPLANE>(expand_bs[m], grid, s, dq, d_groups[m], d_active);
+                    else launch_expand<KPAX_MODEL_QUADROTOR>(expand_bs[m], grid, s, dq, d_groups[m], d_active);
+                    if(u < nused - 1) cudaEventRecord(ev_join[u], s);
+                }
+                for(int u = 0; u + 1 < nused; ++u) cudaStreamWaitEvent(stream, ev_join[u], 0);
+            } else if(expand_mode == 2 && mixed_bs) {
+                launch_expand_mixed(mixed_bs, gx_mixed, sq, stream, dq, d_ctl, d_mixed, nq, d_active);
+            } else {
+                for(int m = 0; m < 3; ++m) {
+                    if(groups[m].empty()) continue;
+                    const uint32_t g = (uint32_t)groups[m].size();
+                    const size_t sg = 4 * ((size_t)g + 1);
+                    if(m == 0)
+                        launch_expand_all<KPAX_MODEL_DOUBLE_INTEGRATOR>(expand_bs[m], gx_expand_all[m], sg, stream, dq, d_ctl,
+                                                                        d_groups[m], g, d_active);
+                    else if(m == 1)
+                        launch_expand_all<KPAX_MODEL_DUBINS_AIRPLANE>(expand_bs[m], gx_expand_all[m], sg, stream, dq, d_ctl,
+                                                                      d_groups[m], g, d_active);
+                    else
+                        launch_expand_all<KPAX_MODEL_QUADROTOR>(expand_bs[m], gx_expand_all[m], sg, stream, dq, d_ctl,
+                                                                d_groups[m], g, d_active);
+                }
             }
-            if(mixed_bs) launch_expand_mixed(mixed_bs, gx_mixed, sq, stream, dq, d_ctl, d_mixed, nq, d_active);
             if(ev && split) cudaEventRecord(ev[2], stream);
             launch_chained(k_scores_all, dim3(gx_scores_all), kScoreBS, sq, stream, dq, (const Ctl*)d_ctl, nq, d_active);
             if(ev) cudaEventRecord(ev[3], stream);
@@ -562,7 +591,7 @@ struct PlanBatch {
         if(fused) return 1;
         if(persistent) {  // start, count, write, (proposal), the expansion(s), scores
             uint64_t k = n_learned ? 5 : 4;
-            if(mixed_bs) return k + 1;
+            if(expand_mode == 2 && mixed_bs) return k + 1;
             for(int m = 0; m < 3; ++m) k += groups[m].empty() ? 0 : 1;
             return k;
         }
