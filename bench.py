@@ -722,22 +722,31 @@ def run_ours(args) -> None:
     seg_par = torch.from_numpy(E.sample_states(cfg.model, seg_n, 17)).cuda()
     seg_rows = torch.empty((seg_n, cfg.sample_dim), device="cuda")
     seg_valid = torch.empty(seg_n, dtype=torch.uint8, device="cuda")
-    seg_env = kpax.Env(cfg, d_obs.data_ptr(), obs.shape[0])
     flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device="cuda")
-    fl_seg = []
-    with torch.cuda.stream(stream):
-        for i in range(8):
-            flush.fill_(i & 0xFF)
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            kpax.propagate_batch(cfg, seg_env, seg_par.data_ptr(), None, 900 + i, seg_n, seg_rows.data_ptr(),
-                                 seg_valid.data_ptr(), stream=stream.cuda_stream)
-            b.record(stream)
-            torch.cuda.synchronize()
-            fl_seg.append(a.elapsed_time(b))
+
+    def segment_floor(env) -> float:
+        ts = []
+        with torch.cuda.stream(stream):
+            for i in range(8):
+                flush.fill_(i & 0xFF)
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                kpax.propagate_batch(cfg, env, seg_par.data_ptr(), None, 900 + i, seg_n, seg_rows.data_ptr(),
+                                     seg_valid.data_ptr(), stream=stream.cuda_stream)
+                b.record(stream)
+                torch.cuda.synchronize()
+                ts.append(a.elapsed_time(b))
+        return float(np.median(ts[3:]))
+
+    seg_env = kpax.Env(cfg, d_obs.data_ptr(), obs.shape[0])
+    chain_floor_ms = segment_floor(seg_env)
+    seg_env.close()
+    # the same chain with no obstacles (every segment runs its steps; the grid queries find empty
+    # cells): the share of the floor the obstacle tests take
+    seg_env = kpax.Env(cfg, d_obs.data_ptr(), 0)
+    chain_floor_empty_ms = segment_floor(seg_env)
     seg_env.close()
     del flush
-    chain_floor_ms = float(np.median(fl_seg[3:]))
     # the per-kernel breakdown from as many iterations with events between the kernels, on a new
     # plan grown the same way (the tree stays below its capacity)
     pl.begin(start, goal, d_obs.data_ptr(), obs.shape[0])
@@ -767,7 +776,8 @@ def run_ours(args) -> None:
                 "floor_note": "the propagation kernel on 4096 independent segments of the same model and scene (one warp "
                               "per SM): the dependency chain of one full-length segment, which bounds the expansion "
                               "kernel from below whatever its FP32 rate",
-                "floor_frac": chain_floor_ms / (1000 * t_exp / args.steps)}
+                "floor_frac": chain_floor_ms / (1000 * t_exp / args.steps),
+                "latency_floor_no_obstacles_ms": chain_floor_empty_ms}
 
     # end to end: whole plans from host buffers through the C ABI
     e2e_v, e2e_t, tts, found = 0, 0.0, [], 0

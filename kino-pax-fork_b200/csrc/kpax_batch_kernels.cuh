@@ -3,9 +3,10 @@
 //
 // A stage's work comes in units (node tiles of the frontier passes, child tiles of the expansion,
 // groups of region partials of the score pass).  Every CTA computes the per-query unit counts and
-// their exclusive offsets in shared memory, then takes the global units b, b + G, b + 2G, ... and
-// finds each unit's query by binary search in the offsets, loading that query's descriptor when
-// the query changes.  A query's last unit to finish (per-query arrival counter) closes the query's
+// their exclusive offsets in shared memory, then takes its units — a contiguous share in the
+// frontier and score passes, units b, b + G, b + 2G, ... in the expansion (whose look-back must
+// only wait on lower units already taken) — finds each unit's query by binary search in the
+// offsets, and loads that query's descriptor when the query changes.  A query's last unit to finish (per-query arrival counter) closes the query's
 // stage: the tile scan and budget of the count pass, the score total and bookkeeping of the score
 // pass.  Each unit runs the per-tile code of the single-query kernels (count_tile, write_tile,
 // expand_tiles, score_partials, score_finish), so a query planned in a batch gives its single plan
@@ -74,6 +75,15 @@ __device__ __forceinline__ uint32_t find_query(const uint32_t* s_off, uint32_t n
     return lo;
 }
 
+// Contiguous share [lo, hi) of `total` units for this CTA: consecutive units mostly belong to the
+// same query, so a CTA loads few descriptors (stages without waits between CTAs only).
+__device__ __forceinline__ void unit_range(uint32_t total, uint32_t& lo, uint32_t& hi)
+{
+    const uint32_t per = (total + gridDim.x - 1) / gridDim.x;
+    lo = min(total, blockIdx.x * per);
+    hi = min(total, lo + per);
+}
+
 // Copies query q's descriptor into shared memory (all threads; the previous one is no longer read).
 __device__ __forceinline__ void load_query_at(const QueryDev* __restrict__ qs, uint32_t q, QueryDev& sq)
 {
@@ -115,7 +125,9 @@ __global__ void __launch_bounds__(kFrontierBS) k_count_all(const QueryDev* __res
     });
     uint32_t cur = kNone, tree = 0, tree_old = 0, iter = 0, plan = 0, ready = 0, ntiles = 0;
     float fa = 0.0f, ftotal = 0.0f;
-    for(uint32_t g = blockIdx.x; g < total; g += gridDim.x) {
+    uint32_t g0, g1;
+    unit_range(total, g0, g1);
+    for(uint32_t g = g0; g < g1; ++g) {
         const uint32_t q = find_query(s_off, nq, g);
         if(q != cur) {
             load_query_at(qs, q, sq);
@@ -158,7 +170,9 @@ __global__ void __launch_bounds__(kFrontierBS) k_write_all(const QueryDev* __res
     });
     uint32_t cur = kNone, tree = 0, E = 0;
     uint64_t R = 0;
-    for(uint32_t g = blockIdx.x; g < total; g += gridDim.x) {
+    uint32_t g0, g1;
+    unit_range(total, g0, g1);
+    for(uint32_t g = g0; g < g1; ++g) {
         const uint32_t q = find_query(s_off, nq, g);
         if(q != cur) {
             load_query_at(qs, q, sq);
@@ -260,7 +274,9 @@ __global__ void __launch_bounds__(kScoreBS) k_scores_all(const QueryDev* __restr
     });
     uint32_t cur = kNone, units = 0;
     const int tid = threadIdx.x;
-    for(uint32_t g = blockIdx.x; g < total; g += gridDim.x) {
+    uint32_t g0, g1;
+    unit_range(total, g0, g1);
+    for(uint32_t g = g0; g < g1; ++g) {
         const uint32_t q = find_query(s_off, nq, g);
         if(q != cur) {
             load_query_at(qs, q, sq);

@@ -158,11 +158,12 @@ struct PlanBatch {
     int mixed_bs = 0;
     uint32_t gx_mixed = 0;
     uint32_t* d_mixed = nullptr;
-    // the batch's expansion: 0 one block per child tile of every query, model groups on concurrent
-    // streams (the default: a model keeps its own occupancy); 1 persistent per model group, one
-    // after another; 2 one persistent launch for every model (KPAX_BATCH_EXPAND selects 1 or 2 for
-    // measurements)
-    int expand_mode = 0;
+    // the batch's expansion: 1 (default) one persistent launch per model group over its queries'
+    // tiles, groups one after another, each at its model's own occupancy; 2 one persistent launch
+    // for every model (the quadrotor's register budget for all); 0 one block per child tile of every
+    // query, model groups on concurrent streams.  KPAX_BATCH_EXPAND=0|2 selects the alternatives
+    // for measurements; the plans are the same.
+    int expand_mode = 1;
     bool fused = false;      // single query without the proposal: one k_iterate launch per iteration
     uint32_t gx_iter = 0;    // its CTAs (all resident), 0 when the kernel cannot be used
     Ctl* d_ctl = nullptr;
@@ -348,7 +349,7 @@ struct PlanBatch {
                 if(!bs0) bs0 = expand_bs[m];
                 same_bs = same_bs && expand_bs[m] == bs0;
             }
-            if(const char* e = getenv("KPAX_BATCH_EXPAND")) expand_mode = atoi(e) == 1 ? 1 : atoi(e) == 2 ? 2 : 0;
+            if(const char* e = getenv("KPAX_BATCH_EXPAND")) expand_mode = atoi(e) == 0 ? 0 : atoi(e) == 2 ? 2 : 1;
             if(persistent && ngroups > 1 && same_bs) {
                 std::vector<uint32_t> order;
                 for(int m = 2; m >= 0; --m) order.insert(order.end(), groups[m].begin(), groups[m].end());
