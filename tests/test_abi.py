@@ -60,7 +60,8 @@ def test_preset_values_follow_benchmark_configs():
     "field,value",
     [("model", 7), ("state_dim", 5), ("max_tree_size", 1), ("step_size", 0.0), ("w_max", -1.0), ("c_r1_length", 40),
      ("hash_cell_size", 0.0), ("children_per_entry", 0), ("expansions_per_iter", 0), ("c_dim", 9), ("block_size", 33),
-     ("block_size", 384), ("samples_per_thread", 9), ("samples_per_thread", -1)],
+     ("block_size", 384), ("samples_per_thread", 9), ("samples_per_thread", -1), ("iteration_kernels", 2),
+     ("iteration_kernels", -1)],
 )
 def test_invalid_configs_are_rejected_with_a_message(field, value):
     cfg = kpax.preset(kpax.PRESET_QUAD)
@@ -170,3 +171,17 @@ def test_null_arguments_are_rejected_without_a_gpu():
     assert lib.kpax_test_wait_timeout(16, None, None) == kpax.EINVAL
     assert lib.kpax_test_wait_timeout((1 << 22) + 1, ctypes.byref(status), None) == kpax.EINVAL
     assert lib.kpax_last_error()
+
+
+def test_fp32_peak_checks_its_arguments_without_a_gpu():
+    lib = kpax.load()
+    t, ms = ctypes.c_double(), ctypes.c_double()
+    assert lib.kpax_fp32_peak(8, ctypes.byref(t), ctypes.byref(ms), None) == kpax.EINVAL  # fewer than 16 FMAs
+    assert lib.kpax_fp32_peak(1 << 16, None, None, None) == kpax.EINVAL
+    assert b"iters" in lib.kpax_last_error()
+
+
+def test_config_default_runs_the_fused_iteration():
+    """iteration_kernels = 0 (a single persistent launch per iteration) is every preset's default."""
+    for which in (kpax.PRESET_DI, kpax.PRESET_DUBINS, kpax.PRESET_QUAD, kpax.PRESET_QUAD_REF):
+        assert kpax.preset(which).iteration_kernels == 0
