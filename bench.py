@@ -14,12 +14,14 @@ the reference's own counter (sum of d_validCounterArray_, src/planners/KPAX.cu:3
          host (oracle/_ref, OpenMP over all cores) on a bounded sample of the same children.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload quad|dubins|di|segments|collide|learned|batch]
+                  [--workload quad|dubins|di|segments|collide|learned|batch|quad-ref|expansion-scan]
 
 Other workloads: dubins / di (the same iteration on the other models), segments (2^22 independent
 Dubins segments through kpax_propagate_batch), collide (2^22 swept-box queries through
 kpax_collide_batch), learned (learned-vs-plain A/B on 256 held-out scenes, tensor-core pass and
-training rates), batch (1024 mixed queries in one batched plan).
+training rates), batch (1024 mixed queries in one batched plan), quad-ref (the reference's own
+quadrotor block on its quadTrees scene, beside the reference's CUDA build), expansion-scan (the
+fused iteration's phase times against the children per iteration, building and empty scenes).
 The reference arm has no counterpart for learned and batch and says so.
 """
 from __future__ import annotations
@@ -1165,13 +1167,48 @@ def run_learned(args) -> None:
         print(json.dumps(line), flush=True)
 
 
+def run_expansion_scan(args) -> None:
+    """Phase times of the fused quadrotor iteration against the children per iteration, in the building
+    scene and with no obstacles, at the default expansion block (the pair layout: two warps per 32
+    children) and at 128-child blocks (one thread per child).  With 448 children per block the
+    expansion's CTAs each hold the same load whatever the budget (only their number changes), so a
+    flat expansion time says that the per-SM chain, not anything shared between SMs, sets it; the
+    empty scene bounds what any staging of the obstacle lists could save."""
+    torch.cuda.set_device(0)
+    obs, start, goal = E.quad_scene()
+    scan = []
+    for scene, o in (("building", obs), ("empty", np.zeros((0, 6), np.float32))):
+        d_obs = torch.from_numpy(o).cuda() if o.size else torch.zeros(6, device="cuda")
+        for bs in (448, 128):
+            for budget in (148 * 32, 148 * 32 * 4, 1 << 15, 1 << 16):
+                cfg = kpax.preset(kpax.PRESET_QUAD)
+                cfg.hash_cell_size, cfg.block_size, cfg.expansions_per_iter = 2.5, bs, budget
+                pl = kpax.KPAX(cfg)
+                pl.begin(start, goal, d_obs.data_ptr(), o.shape[0])
+                pl.iterate_timed(8, 0)
+                pl.iterate_timed(max(args.warmup, 3), FLUSH_BYTES)
+                times, tot = pl.iterate_timed(args.steps, FLUSH_BYTES, split=True)
+                scan.append({"scene": scene, "block_children": bs, "budget": budget,
+                             "iteration_ms": float(times[:, 0].mean()), "frontier_ms": float(times[:, 1].mean()),
+                             "expansion_ms": float(times[:, 2].mean()), "scores_ms": float(times[:, 3].mean()),
+                             "children_per_iter": tot["children"] / args.steps,
+                             "steps_per_child": tot["steps"] / max(tot["children"], 1)})
+                pl.close()
+    print(json.dumps({"metric": "expansion phase time", "unit": "ms", "higher_is_better": False, "n_gpus": 1,
+                      "steps": args.steps, "warmup": args.warmup, "data": "synthetic",
+                      "config": {"workload": "fused quadrotor iteration, budget scan: " + WORKLOADS["quad"][2],
+                                 "l2": "flushed before each timed iteration"},
+                      "scan": scan}), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "learned", "segments", "collide", "quad-ref"],
+    ap.add_argument("--workload", choices=sorted(WORKLOADS) + ["batch", "learned", "segments", "collide", "quad-ref",
+                                                               "expansion-scan"],
                     default="quad")
     ap.add_argument("--plans-ref", type=int, default=256, help="plans per side of the quad-ref workload")
     ap.add_argument("--plans-ref-big", type=int, default=32, help="plans per side at the 2^22 tree capacity (quad-ref)")
@@ -1202,6 +1239,8 @@ def main() -> None:
         run_collide(args)
     elif args.workload == "quad-ref":
         run_quad_ref(args)
+    elif args.workload == "expansion-scan":
+        run_expansion_scan(args)
     else:
         run_ours(args)
 

@@ -299,5 +299,87 @@ __global__ void __launch_bounds__(kScoreBS) k_scores_all(const QueryDev* __restr
     }
 }
 
+// The proposal pass of a batch as one persistent launch: the entries of every learned query,
+// concatenated tile by tile, are spread over all CTAs (CTA b takes tiles b, b + gridDim.x, ...),
+// so the pass is balanced however the entries are spread over the queries.  off[j] is the first
+// tile of learned query j (k_propose_tiles), off[nl] the number of tiles.
+struct BatchEntrySrc {
+    static constexpr bool kDebug = false;
+    const QueryDev* qs;
+    const uint32_t* qidx;
+    const uint32_t* off;
+    uint32_t nl;
+    uint32_t j, row0, E;  // cursor: learned query, first row of the tile, the query's entries
+    const QueryDev* q;
+    __device__ uint32_t tiles() const { return off[nl]; }
+    __device__ void seek(uint32_t tile)
+    {
+        while(off[j + 1] <= tile) ++j;  // tile < off[nl], so j stays below nl
+        q = qs + qidx[j];
+        row0 = (tile - off[j]) * mlp::tc::kRows;
+        E = q->ctl->E;
+    }
+    __device__ uint32_t rows() const { return min((uint32_t)mlp::tc::kRows, E - row0); }
+    __device__ float* records() const { return q->mix + (size_t)row0 * mlp::kMixFloats; }
+    __device__ void row_features(uint32_t r, float x[mlp::kInPad]) const { entry_features(*q, row0 + r, x); }
+    __device__ void dump_h(int, uint32_t, uint32_t, const uint4*) const {}
+    __device__ void dump_out(uint32_t, uint32_t, float) const {}
+};
+
+// Tile offsets of the batch proposal pass (one CTA of kPropTilesBS threads, nl <= kBatchMaxQueries): off[j] = tiles of
+// the learned queries before j, off[nl] = all; a query that has finished, or takes no entries
+// this iteration, has none.
+constexpr int kPropTilesBS = 1024;
+__global__ void __launch_bounds__(kPropTilesBS) k_propose_tiles(const QueryDev* __restrict__ qs, const uint32_t* __restrict__ qidx,
+                                                                uint32_t nl, uint32_t* __restrict__ off)
+{
+    constexpr int kPer = (kBatchMaxQueries + kPropTilesBS - 1) / kPropTilesBS;
+    __shared__ uint32_t s_warp[kPropTilesBS / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    wait_predecessor();
+    release_successor();
+    uint32_t v[kPer], sum = 0;
+#pragma unroll
+    for(int i = 0; i < kPer; ++i) {
+        const uint32_t j = (uint32_t)tid * kPer + i;
+        v[i] = 0u;
+        if(j < nl) {
+            const QueryDev& q = qs[qidx[j]];
+            const Ctl* ctl = q.ctl;
+            v[i] = (ctl->done || !q.mix) ? 0u : (ctl->E + mlp::tc::kRows - 1) / mlp::tc::kRows;
+        }
+        sum += v[i];
+    }
+    uint32_t x = sum;
+#pragma unroll
+    for(int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+        if(lane >= d) x += y;
+    }
+    if(lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    uint32_t acc = x - sum;
+    for(int w = 0; w < warp; ++w) acc += s_warp[w];
+#pragma unroll
+    for(int i = 0; i < kPer; ++i) {
+        const uint32_t j = (uint32_t)tid * kPer + i;
+        if(j < nl) off[j] = acc;
+        acc += v[i];
+        if(j + 1 == nl) off[nl] = acc;
+    }
+}
+
+__global__ void __launch_bounds__(mlp::tc::kThreads, 1) k_propose_all(const QueryDev* __restrict__ qs, const uint32_t* __restrict__ qidx,
+                                                                       uint32_t nl, const uint32_t* __restrict__ off, uint32_t* __restrict__ err)
+{
+    extern __shared__ __align__(1024) uint8_t smem[];
+    wait_predecessor();
+    release_successor();
+    BatchEntrySrc src{qs, qidx, off, nl, 0u, 0u, 0u, nullptr};
+    const bool ok = mlp::tc::forward(src, qs[qidx[0]].mlp_img, smem, err);
+    if(!ok && threadIdx.x == 0)  // a wait gave up: the learned queries stop at this iteration's scores
+        for(uint32_t j = 0; j < nl; ++j) atomicOr(&qs[qidx[j]].ctl->error, mlp::tc::kErrWait);
+}
+
 }  // namespace plan
 }  // namespace kpax

@@ -6,8 +6,9 @@
 //    fused; they are bit-identical to the oracle for identical inputs;
 //  - the double-integrator step is written the same way, so DI segments are bit-identical;
 //  - Dubins and quadrotor RK4 use a branch-free sine/cosine (sincos_fast, within a few ulp of
-//    CUDA's sincosf), tan as sin times the reciprocal cosine, the PTX approximate square root
-//    and reciprocal, and let the compiler fuse multiply-adds; they match the oracle within the
+//    CUDA's sincosf), tan as sin times the reciprocal cosine and the PTX approximate square root
+//    and reciprocal; Dubins lets the compiler fuse multiply-adds, the quadrotor's right-hand side
+//    and stage sums spell out every fused multiply-add; they match the oracle within the
 //    propagation tolerance.
 #pragma once
 #include <stdint.h>
@@ -424,81 +425,139 @@ __device__ __forceinline__ bool step_dubins(const StepParams& p, const Grid& g, 
     return finite_all(s, 6) && step_free(g, p0, s);
 }
 
-// Quadrotor right-hand side, statePropagator.cu:325-370, evaluated at x0 + delta*k.
-// Model constants NU 10e-3, MU 2e-6, IX 1, IY 1, IZ 2, GRAVITY -9.81, MASS 1 (config.h:300-308).
-// trig0: (sin, cos) of the three Euler angles of x0.  kFirst evaluates the first RK4 stage, at
-// x0 + 1 * 0: the state is x0 + 0 (which only turns -0 into +0) and the angle-sum shift by 0
-// reduces to sin + 0 and cos, so the stage skips the shift and gives the same bits.
-template <bool kFirst = false>
-__device__ __forceinline__ void quad_rhs(float* xd, const float* x0, const float* k, float delta, const float* c,
-                                         const float* trig0)  // xd may alias k
+// Quadrotor right-hand side, statePropagator.cu:325-370, in its two halves: the kinematics
+// (position and Euler-angle rates, xd[0..5]) read the attitude's sines and cosines and the body
+// velocities and rates; the dynamics (velocity and rate derivatives, xd[6..11]) read sin/cos of
+// roll and pitch, the velocities, rates and controls.  Model constants NU 10e-3, MU 2e-6, IX 1,
+// IY 1, IZ 2, GRAVITY -9.81, MASS 1 (config.h:300-308).  Every operation is written out (explicit
+// roundings and fused multiply-adds), so the result does not depend on how the compiler contracts
+// the expressions where the step is inlined.
+struct QuadTrig {
+    float sf, cf, st, ct, sp, cp;  // sin / cos of roll, pitch, yaw
+};
+struct QuadRates {
+    float u, v, w, p, q, r;  // body velocities and rates
+};
+
+__device__ __forceinline__ void quad_kin(float* xd, const QuadTrig& t, const QuadRates& b)
 {
-    const float NU = 10e-3f, MU = 2e-6f, G = -9.81f;
-    float u, v, w, pp, q, r, sf, cf, st, ct, sp, cp;
-    if constexpr(kFirst) {
-        u = x0[6] + 0.0f, v = x0[7] + 0.0f, w = x0[8] + 0.0f;
-        pp = x0[9] + 0.0f, q = x0[10] + 0.0f, r = x0[11] + 0.0f;
-        sf = trig0[0] + 0.0f, cf = trig0[1], st = trig0[2] + 0.0f, ct = trig0[3], sp = trig0[4] + 0.0f, cp = trig0[5];
-    } else {
-        u = x0[6] + delta * k[6], v = x0[7] + delta * k[7], w = x0[8] + delta * k[8];
-        pp = x0[9] + delta * k[9], q = x0[10] + delta * k[10], r = x0[11] + delta * k[11];
-        const float d0 = delta * k[3], d1 = delta * k[4], d2 = delta * k[5];
-        if(fmaxf(fabsf(d0), fmaxf(fabsf(d1), fabsf(d2))) <= kShiftMax) {
-            sincos_shift(trig0[0], trig0[1], d0, &sf, &cf);
-            sincos_shift(trig0[2], trig0[3], d1, &st, &ct);
-            sincos_shift(trig0[4], trig0[5], d2, &sp, &cp);
-        } else {  // large attitude increments or non-finite values: evaluate at the rounded angles
-            sincos_checked(x0[3] + d0, &sf, &cf);
-            sincos_checked(x0[4] + d1, &st, &ct);
-            sincos_checked(x0[5] + d2, &sp, &cp);
-        }
-    }
-    const float sec = rcp_approx(ct);  // tan(theta) = sin * sec, 1/cos(theta) = sec
-    xd[0] = ct * cp * u + (sf * st * cp - cf * sp) * v + (cf * st * cp + sf * sp) * w;
-    xd[1] = ct * sp * u + (sf * st * sp + cf * cp) * v + (cf * st * sp - sf * cp) * w;
-    xd[2] = -st * u + sf * ct * v + cf * ct * w;
-    const float qr = q * sf + r * cf;
-    xd[3] = pp + qr * (st * sec);
-    xd[4] = q * cf - r * sf;
-    xd[5] = qr * sec;
-    const float XYZ = -NU * sqrt_approx(u * u + v * v + w * w);
-    xd[6] = (r * v - q * w) - G * st + XYZ * u;
-    xd[7] = (pp * w - r * u) + G * ct * sf + XYZ * v;
-    xd[8] = (q * u - pp * v) + G * ct * cf + XYZ * w + c[0];
-    const float LMN = -MU * sqrt_approx(pp * pp + q * q + r * r);
-    xd[9] = -(q * r) + LMN * pp + c[1];          // (IY - IZ)/IX = -1, 1/IX = 1
-    xd[10] = (pp * r) + LMN * q + c[2];          // (IZ - IX)/IY = 1,  1/IY = 1
-    xd[11] = 0.0f * (pp * q) + 0.5f * (LMN * r) + 0.5f * c[3];  // (IX - IY)/IZ = 0, 1/IZ = 0.5
+    const float sec = rcp_approx(t.ct);  // tan(theta) = sin * sec, 1/cos(theta) = sec
+    const float sfst = __fmul_rn(t.sf, t.st), cfst = __fmul_rn(t.cf, t.st);
+    const float r01 = __fmaf_rn(sfst, t.cp, -__fmul_rn(t.cf, t.sp)), r02 = __fmaf_rn(cfst, t.cp, __fmul_rn(t.sf, t.sp));
+    const float r11 = __fmaf_rn(sfst, t.sp, __fmul_rn(t.cf, t.cp)), r12 = __fmaf_rn(cfst, t.sp, -__fmul_rn(t.sf, t.cp));
+    xd[0] = __fmaf_rn(r02, b.w, __fmaf_rn(r01, b.v, __fmul_rn(__fmul_rn(t.ct, t.cp), b.u)));
+    xd[1] = __fmaf_rn(r12, b.w, __fmaf_rn(r11, b.v, __fmul_rn(__fmul_rn(t.ct, t.sp), b.u)));
+    xd[2] = __fmaf_rn(__fmul_rn(t.cf, t.ct), b.w, __fmaf_rn(__fmul_rn(t.sf, t.ct), b.v, -__fmul_rn(t.st, b.u)));
+    const float qr = __fmaf_rn(b.q, t.sf, __fmul_rn(b.r, t.cf));
+    xd[3] = __fmaf_rn(qr, __fmul_rn(t.st, sec), b.p);
+    xd[4] = __fmaf_rn(b.q, t.cf, -__fmul_rn(b.r, t.sf));
+    xd[5] = __fmul_rn(qr, sec);
 }
 
-// Quadrotor RK4, statePropagatorSpatialHash.cu:234-308.  The four stages run as a loop over one
-// copy of the right-hand side (k is updated in place: each stage reads the previous stage's k
-// before writing its own); the stage sum keeps the reference's order ((k1 + 2k2) + 2k3) + k4.
-// One step from s in place; false when the step fails a check (velocity box, workspace, finite,
-// collision).
+__device__ __forceinline__ void quad_dyn(float* xd, float sf, float cf, float st, float ct, const QuadRates& b, const float* c)
+{
+    const float NU = 10e-3f, MU = 2e-6f, G = -9.81f;
+    const float XYZ = __fmul_rn(-NU, sqrt_approx(__fmaf_rn(b.w, b.w, __fmaf_rn(b.v, b.v, __fmul_rn(b.u, b.u)))));
+    const float gct = __fmul_rn(G, ct);
+    xd[0] = __fmaf_rn(XYZ, b.u, __fmaf_rn(-G, st, __fmaf_rn(b.r, b.v, -__fmul_rn(b.q, b.w))));
+    xd[1] = __fmaf_rn(XYZ, b.v, __fmaf_rn(gct, sf, __fmaf_rn(b.p, b.w, -__fmul_rn(b.r, b.u))));
+    xd[2] = __fadd_rn(__fmaf_rn(XYZ, b.w, __fmaf_rn(gct, cf, __fmaf_rn(b.q, b.u, -__fmul_rn(b.p, b.v)))), c[0]);
+    const float LMN = __fmul_rn(-MU, sqrt_approx(__fmaf_rn(b.r, b.r, __fmaf_rn(b.q, b.q, __fmul_rn(b.p, b.p)))));
+    xd[3] = __fadd_rn(__fmaf_rn(LMN, b.p, -__fmul_rn(b.q, b.r)), c[1]);  // (IY - IZ)/IX = -1, 1/IX = 1
+    xd[4] = __fadd_rn(__fmaf_rn(LMN, b.q, __fmul_rn(b.p, b.r)), c[2]);   // (IZ - IX)/IY = 1,  1/IY = 1
+    // (IX - IY)/IZ = 0 (the product still carries a non-finite rate), 1/IZ = 0.5
+    xd[5] = __fmaf_rn(0.5f, c[3], __fmaf_rn(0.5f, __fmul_rn(LMN, b.r), __fmul_rn(0.0f, __fmul_rn(b.p, b.q))));
+}
+
+// The first RK4 stage is evaluated at x0 + 1 * 0: the state is x0 + 0 (which only turns -0 into
+// +0) and the angle-sum shift by 0 reduces to sin + 0 and cos.  trig0: (sin, cos) of the three
+// Euler angles of x0.
+__device__ __forceinline__ QuadTrig quad_first_trig(const float* trig0)
+{
+    return {__fadd_rn(trig0[0], 0.0f), trig0[1], __fadd_rn(trig0[2], 0.0f), trig0[3], __fadd_rn(trig0[4], 0.0f), trig0[5]};
+}
+
+__device__ __forceinline__ QuadRates quad_first_rates(const float* v0)
+{
+    return {__fadd_rn(v0[0], 0.0f), __fadd_rn(v0[1], 0.0f), __fadd_rn(v0[2], 0.0f),
+            __fadd_rn(v0[3], 0.0f), __fadd_rn(v0[4], 0.0f), __fadd_rn(v0[5], 0.0f)};
+}
+
+// The attitude at a0 + delta * ka (later stages): sin and cos by the angle-sum shift of trig0;
+// large attitude increments or non-finite values are evaluated at the rounded angles.
+__device__ __forceinline__ QuadTrig quad_stage_trig(const float* a0, const float* trig0, const float* ka, float delta)
+{
+    QuadTrig t;
+    const float d0 = __fmul_rn(delta, ka[0]), d1 = __fmul_rn(delta, ka[1]), d2 = __fmul_rn(delta, ka[2]);
+    if(fmaxf(fabsf(d0), fmaxf(fabsf(d1), fabsf(d2))) <= kShiftMax) {
+        sincos_shift(trig0[0], trig0[1], d0, &t.sf, &t.cf);
+        sincos_shift(trig0[2], trig0[3], d1, &t.st, &t.ct);
+        sincos_shift(trig0[4], trig0[5], d2, &t.sp, &t.cp);
+    } else {
+        sincos_checked(__fadd_rn(a0[0], d0), &t.sf, &t.cf);
+        sincos_checked(__fadd_rn(a0[1], d1), &t.st, &t.ct);
+        sincos_checked(__fadd_rn(a0[2], d2), &t.sp, &t.cp);
+    }
+    return t;
+}
+
+__device__ __forceinline__ QuadRates quad_stage_rates(const float* v0, const float* kv, float delta)
+{
+    return {__fmaf_rn(delta, kv[0], v0[0]), __fmaf_rn(delta, kv[1], v0[1]), __fmaf_rn(delta, kv[2], v0[2]),
+            __fmaf_rn(delta, kv[3], v0[3]), __fmaf_rn(delta, kv[4], v0[4]), __fmaf_rn(delta, kv[5], v0[5])};
+}
+
+__device__ __forceinline__ void quad_trig0(const float* a0, float* trig0)
+{
+    sincos_checked(a0[0], &trig0[0], &trig0[1]);
+    sincos_checked(a0[1], &trig0[2], &trig0[3]);
+    sincos_checked(a0[2], &trig0[4], &trig0[5]);
+}
+
+// The per-step checks of each half, in the reference's order (velocity box; workspace; then the
+// finite check and the swept box's collision query).
+__device__ __forceinline__ bool quad_dyn_ok(const StepParams& p, const float* v)
+{
+    return !(v[0] < p.vmin || v[0] > p.vmax || v[1] < p.vmin || v[1] > p.vmax || v[2] < p.vmin || v[2] > p.vmax) &&
+           finite_all(v, 6);
+}
+
+__device__ __forceinline__ bool quad_kin_ok(const StepParams& p, const Grid& g, const float* p0, const float* x)
+{
+    if(x[0] < p.ws_lo || x[0] > p.ws_hi || x[1] < p.ws_lo || x[1] > p.ws_hi || x[2] < p.ws_lo || x[2] > p.ws_hi) return false;
+    return finite_all(x, 6) && step_free(g, p0, x);
+}
+
+// Quadrotor RK4, statePropagatorSpatialHash.cu:234-308: four stages, the stage sum in the
+// reference's order ((k1 + 2k2) + 2k3) + k4.  One step from s in place; false when the step fails
+// a check (velocity box, workspace, finite, collision).
 __device__ __forceinline__ bool step_quad(const StepParams& p, const Grid& g, float* s, const float* c)
 {
     const float h = p.h, hh = p.hh, h6 = p.h6;
     const float p0[3] = {s[0], s[1], s[2]};
     float k[12], acc[12], trig0[6];
-    sincos_checked(s[3], &trig0[0], &trig0[1]);
-    sincos_checked(s[4], &trig0[2], &trig0[3]);
-    sincos_checked(s[5], &trig0[4], &trig0[5]);
-    quad_rhs<true>(k, s, nullptr, 1.0f, c, trig0);
+    quad_trig0(s + 3, trig0);
+    {
+        const QuadTrig t = quad_first_trig(trig0);
+        const QuadRates b = quad_first_rates(s + 6);
+        quad_kin(k, t, b);
+        quad_dyn(k + 6, t.sf, t.cf, t.st, t.ct, b, c);
+    }
 #pragma unroll
     for(int j = 0; j < 12; ++j) acc[j] = k[j];
 #pragma unroll 1
     for(int stage = 1; stage < 4; ++stage) {
         const float delta = stage == 3 ? h : hh, w = stage == 3 ? 1.0f : 2.0f;
-        quad_rhs(k, s, k, delta, c, trig0);
+        const QuadTrig t = quad_stage_trig(s + 3, trig0, k + 3, delta);
+        const QuadRates b = quad_stage_rates(s + 6, k + 6, delta);
+        quad_kin(k, t, b);
+        quad_dyn(k + 6, t.sf, t.cf, t.st, t.ct, b, c);
 #pragma unroll
-        for(int j = 0; j < 12; ++j) acc[j] = acc[j] + w * k[j];
+        for(int j = 0; j < 12; ++j) acc[j] = __fmaf_rn(w, k[j], acc[j]);
     }
 #pragma unroll
-    for(int j = 0; j < 12; ++j) s[j] += h6 * acc[j];
-    if(s[6] < p.vmin || s[6] > p.vmax || s[7] < p.vmin || s[7] > p.vmax || s[8] < p.vmin || s[8] > p.vmax) return false;
-    if(s[0] < p.ws_lo || s[0] > p.ws_hi || s[1] < p.ws_lo || s[1] > p.ws_hi || s[2] < p.ws_lo || s[2] > p.ws_hi) return false;
-    return finite_all(s, 12) && step_free(g, p0, s);
+    for(int j = 0; j < 12; ++j) s[j] = __fmaf_rn(h6, acc[j], s[j]);
+    return quad_dyn_ok(p, s + 6) && quad_kin_ok(p, g, p0, s);
 }
 
 // Per-segment constants of a model's step (the double integrator's acceleration terms, the Dubins

@@ -258,32 +258,37 @@ struct ArraySrc {
     float* out;
     uint16_t* h1;
     uint16_t* h2;
-    __device__ uint32_t count() const { return n; }
-    __device__ float* records() const { return mix; }
-    __device__ void row_features(uint32_t row, float x[kInPad]) const
+    uint32_t row0;  // first row of the current tile
+    __device__ uint32_t tiles() const { return (n + tc::kRows - 1) / tc::kRows; }
+    __device__ void seek(uint32_t tile) { row0 = tile * tc::kRows; }
+    __device__ uint32_t rows() const { return min((uint32_t)tc::kRows, n - row0); }
+    __device__ float* records() const { return mix + (size_t)row0 * kMixFloats; }
+    __device__ void row_features(uint32_t r, float x[kInPad]) const
     {
+        const uint32_t row = row0 + r;
         float s[12], g[3];
         for(int d = 0; d < 12; ++d) s[d] = states[(size_t)row * stride + d];
         for(int d = 0; d < 3; ++d) g[d] = goals[(size_t)row * 3 + d];
         features(p, occ, s, g, x);
     }
-    __device__ void dump_h(int layer, uint32_t row, uint32_t col0, const uint4 bits[2]) const
+    __device__ void dump_h(int layer, uint32_t r, uint32_t col0, const uint4 bits[2]) const
     {
         uint16_t* dst = layer == 1 ? h1 : h2;
         if(!dst) return;
-        uint4* d = reinterpret_cast<uint4*>(dst + (size_t)row * kH + col0);
+        uint4* d = reinterpret_cast<uint4*>(dst + (size_t)(row0 + r) * kH + col0);
         d[0] = bits[0], d[1] = bits[1];
     }
-    __device__ void dump_out(uint32_t row, uint32_t col, float v) const
+    __device__ void dump_out(uint32_t r, uint32_t col, float v) const
     {
-        if(out) out[(size_t)row * kOutPad + col] = v;
+        if(out) out[(size_t)(row0 + r) * kOutPad + col] = v;
     }
 };
 
-__global__ void __launch_bounds__(tc::kThreads, 1) k_forward_tc(ArraySrc src, const uint8_t* __restrict__ img, uint32_t* err)
+__global__ void __launch_bounds__(tc::kThreads, 1) k_forward_tc(const ArraySrc src, const uint8_t* __restrict__ img, uint32_t* err)
 {
     extern __shared__ __align__(1024) uint8_t smem[];
-    tc::forward(src, img, smem, err);
+    ArraySrc s = src;  // per-thread cursor
+    tc::forward(s, img, smem, err);
 }
 
 // One warp per R1 workspace cell: the cell is blocked when at least half of the 4x4x4 lattice

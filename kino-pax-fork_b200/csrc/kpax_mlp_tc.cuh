@@ -283,16 +283,20 @@ __device__ __forceinline__ void store_row16(uint8_t* base, uint32_t r, uint32_t 
     if(packed) packed[0] = lo, packed[1] = hi;
 }
 
-// Source of rows: `uint32_t count()`, `void row_features(uint32_t row, float x[64])`,
-// `float* records()` (count() records of kMixFloats floats), and for debug dumps `kDebug` with
-// `dump_h(layer, row, col0, const uint4 bits[2])` (16 BF16 values) and `dump_out(row, col, v)`.
+// Source of rows, a tile of kRows rows at a time (each thread keeps its own copy):
+// `uint32_t tiles()` (tiles in all), `void seek(uint32_t tile)` (a thread visits its tiles in
+// increasing order), and for the current tile `uint32_t rows()` (1..kRows valid rows),
+// `void row_features(uint32_t r, float x[64])` (row r of the tile), `float* records()` (the
+// tile's rows() records of kMixFloats floats); for debug dumps `kDebug` with
+// `dump_h(layer, r, col0, const uint4 bits[2])` (16 BF16 values) and `dump_out(r, col, v)`.
+// CTA b takes tiles b, b + gridDim.x, ...
+// Returns false in every thread of a CTA whose pipeline gave up a wait (err has kErrWait set).
 template <class Src>
-__device__ void forward(Src& src, const uint8_t* __restrict__ img, uint8_t* smem_raw, uint32_t* __restrict__ err)
+__device__ bool forward(Src& src, const uint8_t* __restrict__ img, uint8_t* smem_raw, uint32_t* __restrict__ err)
 {
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const uint32_t n = src.count();
-    const uint32_t ntiles = (n + kRows - 1) / kRows;
-    if(blockIdx.x >= ntiles) return;
+    const uint32_t ntiles = src.tiles();
+    if(blockIdx.x >= ntiles) return true;
     const uint32_t my_tiles = (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x;
     const uint32_t raw = (uint32_t)__cvta_generic_to_shared(smem_raw);
     const uint32_t pad = ((raw + 1023u) & ~1023u) - raw;
@@ -400,10 +404,11 @@ __device__ void forward(Src& src, const uint8_t* __restrict__ img, uint8_t* smem
                 fail();
                 break;
             }
+            src.seek(tile);
+            const uint32_t nr = src.rows();
             for(uint32_t r = ft; r < (uint32_t)kRows; r += kFeatThreads) {
-                const uint32_t row = tile * kRows + r;
                 float x[kInPad];
-                if(row < n) src.row_features(row, x);
+                if(r < nr) src.row_features(r, x);
                 else
 #pragma unroll
                     for(int c = 0; c < kInPad; ++c) x[c] = 0.0f;
@@ -419,7 +424,8 @@ __device__ void forward(Src& src, const uint8_t* __restrict__ img, uint8_t* smem
         const uint32_t t_lane = tmem + ((32u * q) << 16);
         float* stg = reinterpret_cast<float*>(sm + kSmH);
         for(uint32_t i = 0; i < my_tiles; ++i) {
-            const uint32_t tile = blockIdx.x + i * gridDim.x, row = tile * kRows + r;
+            src.seek(blockIdx.x + i * gridDim.x);
+            const uint32_t nr = src.rows();
             // hidden layers: D (columns d_col..) -> SiLU -> H slab cg; arrive `ready`
             auto hidden = [&](int layer, int bar_d, uint32_t d_col, const float* b, int bar_ready) -> bool {
                 const bool ok = mbar_wait(bar(bar_d), i & 1u);
@@ -442,7 +448,7 @@ __device__ void forward(Src& src, const uint8_t* __restrict__ img, uint8_t* smem
                         uint4 bits[2];
                         store_row16(sm + kSmH, r, col0, v[cc], bits);
                         if constexpr(Src::kDebug) {
-                            if(row < n) src.dump_h(layer, row, col0, bits);
+                            if(r < nr) src.dump_h(layer, r, col0, bits);
                         }
                     }
                 }
@@ -469,14 +475,13 @@ __device__ void forward(Src& src, const uint8_t* __restrict__ img, uint8_t* smem
 #pragma unroll
             for(int c = 0; c < kCols; ++c) rec[c] = o[c] + b3[c];
             if constexpr(Src::kDebug) {
-                if(row < n)
-                    for(int c = 0; c < kCols; ++c) src.dump_out(row, cg * (uint32_t)kCols + (uint32_t)c, o[c] + b3[c]);
+                if(r < nr)
+                    for(int c = 0; c < kCols; ++c) src.dump_out(r, cg * (uint32_t)kCols + (uint32_t)c, o[c] + b3[c]);
             }
             epi_sync();
             // coalesced copy of the tile's records (contiguous rows) to global memory
-            const uint32_t valid = min((uint32_t)kRows, n - tile * kRows);
-            float* dst = src.records() + (size_t)tile * kRows * kMixFloats;
-            for(uint32_t f = tid - 128u; f < valid * (uint32_t)kMixFloats; f += (uint32_t)kEpiThreads)
+            float* dst = src.records();
+            for(uint32_t f = tid - 128u; f < nr * (uint32_t)kMixFloats; f += (uint32_t)kEpiThreads)
                 dst[f] = stg[(f / kMixFloats) * kRecStride + f % kMixFloats];
             epi_sync();  // staging read before the next tile's epilogue rewrites H
         }
@@ -485,6 +490,7 @@ __device__ void forward(Src& src, const uint8_t* __restrict__ img, uint8_t* smem
     __syncthreads();
     fence_after();
     if(warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u) : "memory");
+    return *s_err == 0u;
 }
 
 }  // namespace tc

@@ -810,6 +810,7 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_iterate(c
     __shared__ uint32_t s_flag, s_last;
     __shared__ uint32_t s_warp[NW], s_warp2[NW];
     __shared__ float s_part[kPartials];
+    __shared__ unsigned long long s_t[3];  // phase start times (thread 0)
     load_query(qs, nullptr, sq);
     const KParams& p = sq.p;
     const TreeDev& t = sq.t;
@@ -819,7 +820,7 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_iterate(c
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     wait_predecessor();
     if(__syncthreads_or(ctl->done != 0u)) return;  // one decision for the whole grid: barriers follow
-    const unsigned long long t0 = globaltimer();
+    if(tid == 0) s_t[0] = globaltimer();
     const uint32_t tree = ctl->tree, tree_old = ctl->tree_old, iter = ctl->iter, plan = ctl->plan_idx;
     const uint32_t ready = ctl->scores_ready;
     const float fa = ctl->faccept, total = ctl->score_total;
@@ -925,7 +926,7 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_iterate(c
         if(tid == 0) atomicOr(&ctl->error, kErrTimeout), finish_query(ctl, active);
         return;
     }
-    const unsigned long long t2 = globaltimer();
+    if(tid == 0) s_t[1] = globaltimer();
 
     // ---- expansion (k_expand); a CTA whose look-back wait gave up has finished the query with an
     // error and still takes part in the barrier
@@ -934,7 +935,7 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_iterate(c
         if(tid == 0) atomicOr(&ctl->error, kErrTimeout), finish_query(ctl, active);
         return;
     }
-    const unsigned long long t3 = globaltimer();
+    if(tid == 0) s_t[2] = globaltimer();
 
     // ---- region scores (k_scores); the last CTA to finish adds the partials and closes the iteration
     score_partials(sq, cb * BS + tid, G * BS, (int)(cb * NW) + warp, (int)(G * NW));
@@ -948,27 +949,31 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_iterate(c
     score_finish(sq, s_part, active);
     if(tid == 0) {
         const unsigned long long t4 = globaltimer();
-        ctl->t_front_ns += t2 - t0;
-        ctl->t_expand_ns += t3 - t2;
-        ctl->t_score_ns += t4 - t3;
+        ctl->t_front_ns += s_t[1] - s_t[0];
+        ctl->t_expand_ns += s_t[2] - s_t[1];
+        ctl->t_score_ns += t4 - s_t[2];
     }
 }
 
-// Re-activation of the last iteration without a scan (makes exported frontier flags final).
+// Features of frontier entry `row` of query q: the entry's node and the query's goal.
+__device__ __forceinline__ void entry_features(const QueryDev& q, uint32_t row, float x[mlp::kInPad])
+{
+    float s[12];
+    load_state<12>(q.t, q.entries[row], s);
+    const float g[3] = {q.ctl->goal[0], q.ctl->goal[1], q.ctl->goal[2]};
+    mlp::features(q.p, q.occ, s, g, x);
+}
+
 // Rows of the proposal pass: the frontier entries of the iteration (k_frontier_write).
 struct EntrySrc {
     static constexpr bool kDebug = false;
     const QueryDev* q;
-    uint32_t E;
-    __device__ uint32_t count() const { return E; }
-    __device__ float* records() const { return q->mix; }
-    __device__ void row_features(uint32_t row, float x[mlp::kInPad]) const
-    {
-        float s[12];
-        load_state<12>(q->t, q->entries[row], s);
-        const float g[3] = {q->ctl->goal[0], q->ctl->goal[1], q->ctl->goal[2]};
-        mlp::features(q->p, q->occ, s, g, x);
-    }
+    uint32_t E, row0;
+    __device__ uint32_t tiles() const { return (E + mlp::tc::kRows - 1) / mlp::tc::kRows; }
+    __device__ void seek(uint32_t tile) { row0 = tile * mlp::tc::kRows; }
+    __device__ uint32_t rows() const { return min((uint32_t)mlp::tc::kRows, E - row0); }
+    __device__ float* records() const { return q->mix + (size_t)row0 * mlp::kMixFloats; }
+    __device__ void row_features(uint32_t r, float x[mlp::kInPad]) const { entry_features(*q, row0 + r, x); }
     __device__ void dump_h(int, uint32_t, uint32_t, const uint4*) const {}
     __device__ void dump_out(uint32_t, uint32_t, float) const {}
 };
@@ -984,7 +989,7 @@ __global__ void __launch_bounds__(mlp::tc::kThreads, 1) k_propose(const QueryDev
     wait_predecessor();
     release_successor();
     if(sq.ctl->done || !sq.mix) return;
-    EntrySrc src{&sq, sq.ctl->E};
+    EntrySrc src{&sq, sq.ctl->E, 0u};
     mlp::tc::forward(src, sq.mlp_img, smem, &sq.ctl->error);
 }
 

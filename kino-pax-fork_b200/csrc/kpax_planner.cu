@@ -194,6 +194,10 @@ struct PlanBatch {
     char* d_learn = nullptr;         // mixture records and occupancy bits of the learned queries
     uint32_t* d_learned = nullptr;   // indices of the learned queries
     uint32_t n_learned = 0, gx_prop = 1;
+    // more than one learned query: one persistent proposal launch over all of their entries,
+    // after k_propose_tiles has laid their tiles out (d_prop_off: nl + 1 offsets, an error word)
+    uint32_t* d_prop_off = nullptr;
+    uint32_t gx_prop_all = 0;
 
     kpax_status init(const kpax_config* cfgs, uint32_t n)
     {
@@ -378,7 +382,7 @@ struct PlanBatch {
         for(Env& e : env) e.release();
         for(int m = 0; m < 3; ++m)
             if(d_groups[m]) cudaFree(d_groups[m]);
-        void* dev[] = {pool, dq, d_ctl, d_active, d_ig, d_path, d_flush, d_img, d_learn, d_learned, d_mixed};
+        void* dev[] = {pool, dq, d_ctl, d_active, d_ig, d_path, d_flush, d_img, d_learn, d_learned, d_mixed, d_prop_off};
         for(void* p : dev)
             if(p) cudaFree(p);
         void* host[] = {h_ctl, h_active, h_ig, h_path};
@@ -450,9 +454,7 @@ struct PlanBatch {
             launch_chained(k_count_all, dim3(gx_count_all), kFrontierBS, sq, stream, dq, (const Ctl*)d_ctl, nq);
             launch_chained(k_write_all, dim3(gx_write_all), kFrontierBS, sq, stream, dq, (const Ctl*)d_ctl, nq);
             if(ev && split) cudaEventRecord(ev[1], stream);
-            if(n_learned)
-                launch_chained(k_propose, dim3(gx_prop, n_learned), mlp::tc::kThreads, mlp::tc::kSmemBytes, stream, dq,
-                               d_learned);
+            if(n_learned) launch_proposal(stream);
             if(expand_mode == 0) {  // per model group: one block per child tile of every query, groups concurrent
                 int used[3], nused = 0;
                 for(int m = 0; m < 3; ++m)
@@ -510,8 +512,7 @@ struct PlanBatch {
                 cudaStreamWaitEvent(s, ev_fork, 0);
             }
             const dim3 grid(expand_gx[m], (uint32_t)groups[m].size());
-            if(m == 2 && n_learned)
-                launch_chained(k_propose, dim3(gx_prop, n_learned), mlp::tc::kThreads, mlp::tc::kSmemBytes, s, dq, d_learned);
+            if(m == 2 && n_learned) launch_proposal(s);
             if(m == 0) launch_expand<KPAX_MODEL_DOUBLE_INTEGRATOR>(expand_bs[m], grid, s, dq, d_groups[m], d_active);
             else if(m == 1) launch_expand<KPAX_MODEL_DUBINS_AIRPLANE>(expand_bs[m], grid, s, dq, d_groups[m], d_active);
             else launch_expand<KPAX_MODEL_QUADROTOR>(expand_bs[m], grid, s, dq, d_groups[m], d_active);
@@ -521,6 +522,19 @@ struct PlanBatch {
         if(ev && split) cudaEventRecord(ev[2], stream);
         launch_chained(k_scores, dim3(gx_score, nq), kScoreBS, 0, stream, dq, d_active);
         if(ev) cudaEventRecord(ev[3], stream);
+    }
+
+    // The learned proposal pass: one grid row per learned query, or (more than one) one launch
+    // whose CTAs share all their entry tiles.
+    void launch_proposal(cudaStream_t s)
+    {
+        if(d_prop_off) {
+            launch_chained(k_propose_tiles, dim3(1), kPropTilesBS, 0, s, dq, d_learned, n_learned, d_prop_off);
+            launch_chained(k_propose_all, dim3(gx_prop_all), mlp::tc::kThreads, mlp::tc::kSmemBytes, s, dq, d_learned, n_learned,
+                           d_prop_off, d_prop_off + n_learned + 1);
+        } else {
+            launch_chained(k_propose, dim3(gx_prop, n_learned), mlp::tc::kThreads, mlp::tc::kSmemBytes, s, dq, d_learned);
+        }
     }
 
     // Learned proposal for the quadrotor queries with enable[q] != 0 (all when enable is null);
@@ -540,10 +554,10 @@ struct PlanBatch {
         KPAX_CUDA(cudaStreamSynchronize(stream));
         if(graph) cudaGraphExecDestroy(graph), graph = nullptr;
         graph_key.clear();
-        for(void* p : {(void*)d_img, (void*)d_learn, (void*)d_learned})
+        for(void* p : {(void*)d_img, (void*)d_learn, (void*)d_learned, (void*)d_prop_off})
             if(p) cudaFree(p);
-        d_img = nullptr, d_learn = nullptr, d_learned = nullptr;
-        n_learned = 0;
+        d_img = nullptr, d_learn = nullptr, d_learned = nullptr, d_prop_off = nullptr;
+        n_learned = 0, gx_prop_all = 0;
         for(QueryDev& d : hq) d.mlp_img = nullptr, d.mix = nullptr, d.occ = nullptr, d.prop_eps = 1.0f;
         if(!sel.empty()) {
             KPAX_CUDA(cudaMalloc(&d_img, mlp::kImgBytes));
@@ -574,6 +588,14 @@ struct PlanBatch {
             KPAX_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
             gx_prop = std::max<uint32_t>(1, std::min<uint32_t>(max_tiles, (2u * (uint32_t)sms + n_learned - 1) / n_learned));
             KPAX_CUDA(cudaFuncSetAttribute(k_propose, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp::tc::kSmemBytes));
+            if(n_learned > 1 && n_learned <= kBatchMaxQueries) {
+                KPAX_CUDA(cudaFuncSetAttribute(k_propose_all, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp::tc::kSmemBytes));
+                int per_sm = 0;
+                KPAX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_propose_all, mlp::tc::kThreads, mlp::tc::kSmemBytes));
+                KPAX_CUDA(cudaMalloc(&d_prop_off, sizeof(uint32_t) * (n_learned + 2)));
+                KPAX_CUDA(cudaMemsetAsync(d_prop_off, 0, sizeof(uint32_t) * (n_learned + 2), stream));
+                gx_prop_all = (uint32_t)std::max(1, per_sm) * (uint32_t)sms;
+            }
             if(begun)  // a plan in progress: occupancy of the current environments
                 for(uint32_t q : sel) {
                     kpax_status st = launch_occupancy(prm[q], env[q].view(), const_cast<uint32_t*>(hq[q].occ), stream);
@@ -591,12 +613,12 @@ struct PlanBatch {
     {
         if(fused) return 1;
         if(persistent) {  // start, count, write, (proposal), the expansion(s), scores
-            uint64_t k = n_learned ? 5 : 4;
+            uint64_t k = n_learned ? (d_prop_off ? 6 : 5) : 4;
             if(expand_mode == 2 && mixed_bs) return k + 1;
             for(int m = 0; m < 3; ++m) k += groups[m].empty() ? 0 : 1;
             return k;
         }
-        uint64_t k = n_learned ? 4 : 3;  // two frontier passes, the score pass, the proposal pass
+        uint64_t k = n_learned ? (d_prop_off ? 5 : 4) : 3;  // two frontier passes, the score pass, the proposal pass(es)
         for(int m = 0; m < 3; ++m) k += groups[m].empty() ? 0 : 1;
         return k;
     }

@@ -132,3 +132,35 @@ def test_persistent_stages_over_many_uneven_queries(cuda):
     assert full >= 1 and found >= 1, (full, found)  # both early exits are exercised
     assert stats["found"] == found
     batch.close()
+
+
+def test_learned_proposal_in_a_batch_matches_single_plans(cuda):
+    """With the learned proposal on, a batch runs one proposal launch over the entries of all its
+    quadrotor queries (tiles shared by every CTA); each query's records, and so its plan, equal
+    those of the query planned alone."""
+    import torch
+
+    import kpax_learn as L
+
+    net = L.load_network(L.DEFAULT_WEIGHTS)
+    qobs, s, g = E.quad_scene(n_total=300)
+    qs = []
+    for i, (budget, cap, iters) in enumerate(((1 << 13, 1 << 16, 8), (1 << 11, 1 << 15, 10), (1 << 12, 1 << 16, 6))):
+        c = kpax.preset(kpax.PRESET_QUAD)
+        c.max_tree_size, c.expansions_per_iter, c.max_iter, c.seed = cap, budget, iters, 21 + i
+        qs.append((c, qobs if i != 1 else np.zeros((0, 6), np.float32), s, g))
+    qs.append(_queries()[0])  # a double integrator query beside them
+    d_obs = [torch.from_numpy(np.ascontiguousarray(o, np.float32)).cuda() if o.size else None for _, o, _, _ in qs]
+    ptrs = [d.data_ptr() if d is not None else 0 for d in d_obs]
+    batch = kpax.Batch([c for c, _, _, _ in qs])
+    batch.set_proposal(net, 0.3)
+    res, _ = batch.plan([s for _, _, s, _ in qs], [g for _, _, _, g in qs], ptrs, [o.shape[0] for _, o, _, _ in qs])
+    for q, (cfg, obs, s_, g_) in enumerate(qs):
+        pl = kpax.KPAX(cfg)
+        if cfg.model == kpax.MODEL_QUADROTOR:
+            pl.set_proposal(net, 0.3)
+        r = pl.plan(s_, g_, ptrs[q], obs.shape[0])
+        single = {f: getattr(r, f) for f in ("found", "goal_idx", "tree_size", "iters", "expansions", "valid_expansions")}
+        assert {f: res[q][f] for f in single} == single, (q, single, res[q])
+        pl.close()
+    batch.close()
