@@ -51,6 +51,9 @@ FLOP_PER_STEP = {kpax.MODEL_DOUBLE_INTEGRATOR: 18, kpax.MODEL_DUBINS_AIRPLANE: 5
 # dram__bytes_read.sum + dram__bytes_write.sum of one steady-state k_expand launch (2^16 children,
 # L2 flushed before the iteration) in an ncu capture of the default workload; none for the others
 EXPAND_DRAM_BYTES = {kpax.MODEL_QUADROTOR: 1535744 + 0}
+# the same sum for the one-pass kernel (kpax_propagate_batch_noalloc) on 2^20 Dubins segments, L2
+# flushed before the step, per segment
+ONE_PASS_DRAM_BYTES_PER_SEGMENT = (25186304 + 48397824) / (1 << 20)
 # the same sum over the three phase kernels of one 2^20-segment Dubins batch (L2 flushed before the
 # step, no cache flush between the kernels), per segment: scaled by the segment count, as the
 # traffic grows with it
@@ -890,8 +893,12 @@ def run_segments(args) -> None:
     stream = torch.cuda.current_stream()
 
     def launch(i):
-        kpax.propagate_batch(cfg, env, d_par.data_ptr(), None, i, n, rows.data_ptr(), valid.data_ptr(), steps.data_ptr(),
-                             stream=stream.cuda_stream)
+        if args.one_pass:  # the allocation-free entry: one pass over every segment at any batch size
+            kpax.propagate_batch_noalloc(cfg, d_obs.data_ptr(), obs.shape[0], d_par.data_ptr(), None, i, n, rows.data_ptr(),
+                                         valid.data_ptr(), steps.data_ptr(), stream=stream.cuda_stream)
+        else:
+            kpax.propagate_batch(cfg, env, d_par.data_ptr(), None, i, n, rows.data_ptr(), valid.data_ptr(), steps.data_ptr(),
+                                 stream=stream.cuda_stream)
 
     for i in range(max(args.warmup, 3)):
         launch(1000 + i)
@@ -910,6 +917,7 @@ def run_segments(args) -> None:
             n_valid += valid.sum(dtype=torch.int64)  # device-side tallies, outside the events
             n_steps += steps.sum(dtype=torch.int64)
         torch.cuda.synchronize()
+        fp32_peak = max(kpax.fp32_peak(1 << 16)[0] for _ in range(3))  # the same GPU and clocks
     if dist:
         dist.barrier()
     launches = kpax.kernel_launches() - launches0
@@ -920,18 +928,25 @@ def run_segments(args) -> None:
 
     peaks = load_peaks()
     sm_mhz = peaks.get("sm_max_mhz", 1965.0)
-    fp32_peak = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
+    phased = n >= 1 << 18 and not args.one_pass
     achieved = n_steps * FLOP_PER_STEP[cfg.model] / t_s / 1e12
     roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                "traffic": int(PHASED_DRAM_BYTES_PER_SEGMENT * n) if n >= 1 << 18 else None,
-                "traffic_note": "DRAM bytes read + written per step by the three phase kernels, from an ncu capture of "
-                                "2^20 segments scaled to the segment count (summary under profiles/); "
-                                "the algorithmic bytes are 69 per segment (parent 24, row 40, verdict 1, steps 4), the rest "
-                                "is the survivors' round trips and partial-sector fills of rows written out of order",
-                "kernel": "k_propagate_head + 2 x k_propagate_tail<Dubins> (phased batch)" if n >= 1 << 18
+                "traffic": int(PHASED_DRAM_BYTES_PER_SEGMENT * n) if phased
+                           else int(ONE_PASS_DRAM_BYTES_PER_SEGMENT * n) if args.one_pass else None,
+                "traffic_note": ("DRAM bytes read + written per step by the three phase kernels, from an ncu capture of "
+                                 "2^20 segments scaled to the segment count (summary under profiles/); "
+                                 "the algorithmic bytes are 69 per segment (parent 24, row 40, verdict 1, steps 4), the "
+                                 "rest is the survivors' round trips and partial-sector fills of rows written out of order")
+                                if phased else
+                                ("DRAM bytes read + written per step by the one-pass kernel, from an ncu capture of 2^20 "
+                                 "segments scaled to the segment count (summary under profiles/): 70.2 B per segment "
+                                 "against 69 algorithmic"),
+                "kernel": "k_propagate_head + 2 x k_propagate_tail<Dubins> (phased batch)" if phased
                           else "k_propagate_batch<Dubins>",
-                "peak_note": "nominal FP32: 148 SM x 128 lanes x 2 FLOP x clocks.max.sm (no measured FP32 peak in "
-                             "MEASURED_PEAKS.json); plus 12 transcendental per step on the MUFU pipe",
+                "peak_note": "measured: kpax_fp32_peak (FMA chains, CUDA events) on this GPU inside the clock-sampling "
+                             "window; MEASURED_PEAKS.json has no FP32 figure; plus 12 transcendental per step on the MUFU "
+                             "pipe",
+                "nominal_peak": 148 * 128 * 2 * sm_mhz * 1e6 / 1e12,
                 "work": f"{n_steps} RK4 steps x {FLOP_PER_STEP[cfg.model]} FLOP over {args.steps} launches",
                 "ms_per_launch": 1000 * t_s / args.steps, "rk4_steps_per_s": n_steps / t_s}
 
@@ -971,6 +986,7 @@ def run_segments(args) -> None:
             "dtype": "fp32", "data": "synthetic",
             "config": {"workload": SEGMENTS_DESC if n == 1 << 22 else SEGMENTS_DESC.replace("2^22", f"2^{args.segments_log2}"),
                        "segments_per_step": n, "valid_fraction": n_valid / (n * args.steps),
+                       "entry": "kpax_propagate_batch_noalloc (one pass)" if args.one_pass else "kpax_propagate_batch",
                        "l2": "flushed before each timed step (256 MiB write, outside the events)",
                        "parallelism": f"replicas x{ws}"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk.summary(),
@@ -1003,6 +1019,9 @@ def run_batch(args) -> None:
             if best:
                 tuned_models[m] = best
         cfgs = [kpax_autotune.apply(c, tuned_models[c.model]) if c.model in tuned_models else c for c in cfgs]
+    if args.batch_block:  # children per expansion tile of every query (a launch-shape study)
+        for c in cfgs:
+            c.block_size = args.batch_block
     sizes = [d["obstacles"].shape[0] for d in queries]
     offs = np.concatenate([[0], np.cumsum(sizes)])
     h_obs = torch.from_numpy(np.concatenate([d["obstacles"] for d in queries])).pin_memory()
@@ -1051,6 +1070,7 @@ def run_batch(args) -> None:
                                "stage for all queries", "l2": "each step is a whole batch plan (~GB working set)",
                    "learned_proposal": f"quadrotor queries, epsilon {args.eps}" if net is not None else "off",
                    "launch": {str(m): v for m, v in tuned_models.items()} or "defaults",
+                   "expansion_block": args.batch_block or "as launch",
                    "parallelism": f"replicas x{ws}"},
         "plans_per_s": n_plans / (tot_ms / 1000.0),
         "success_rate": found / max(n_plans, 1),
@@ -1174,6 +1194,8 @@ def run_expansion_scan(args) -> None:
     expansion's CTAs each hold the same load whatever the budget (only their number changes), so a
     flat expansion time says that the per-SM chain, not anything shared between SMs, sets it; the
     empty scene bounds what any staging of the obstacle lists could save."""
+    import torch
+
     torch.cuda.set_device(0)
     obs, start, goal = E.quad_scene()
     scan = []
@@ -1213,6 +1235,8 @@ def main() -> None:
     ap.add_argument("--plans-ref", type=int, default=256, help="plans per side of the quad-ref workload")
     ap.add_argument("--plans-ref-big", type=int, default=32, help="plans per side at the 2^22 tree capacity (quad-ref)")
     ap.add_argument("--batch-iters", type=int, default=0, help="iteration cap of every batched query (0 = presets)")
+    ap.add_argument("--batch-block", type=int, default=0, choices=[0, 128, 256, 448, 512],
+                    help="children per expansion tile of every batched query (0 = tuned / presets)")
     ap.add_argument("--seeds", type=int, default=256, help="held-out scenes of the learned workload")
     ap.add_argument("--eps", type=float, default=0.2, help="uniform fraction of the learned proposal")
     ap.add_argument("--proposal", choices=["on", "off"], default="on", help="learned proposal for batched quadrotor queries")
@@ -1225,6 +1249,8 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="ignore the autotuner's cached launch parameters")
     ap.add_argument("--segments-log2", type=int, default=22, help="segments per step of the segments workload (log2)")
+    ap.add_argument("--one-pass", action="store_true",
+                    help="segments workload through the allocation-free entry (one pass at any size, no phases)")
     ap.add_argument("--boxes-log2", type=int, default=22, help="box queries per step of the collide workload (log2)")
     args = ap.parse_args()
     if args.impl == "reference":

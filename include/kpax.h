@@ -248,9 +248,8 @@ kpax_status kpax_propagate_batch(const kpax_config* cfg, kpax_env* env, const fl
  * them one after another on one stream.  A call with obstacles blocks the calling thread once: it
  * waits for `stream` to finish counting the grid entries and reads the count back to the host, to
  * check it against the limit.  Set-up: the first call on a device looks up the array's device
- * address (cudaGetSymbolAddress) and keeps it for the life of the process, so make that first call
- * before any stream capture begins, and do not call the entry on a device again after a
- * cudaDeviceReset of it.  Batches of any size run the one-pass propagation kernel (no phase
+ * address (cudaGetSymbolAddress) and keeps it for the life of the process; do not call the entry
+ * on a device again after a cudaDeviceReset of it.  Batches of any size run the one-pass propagation kernel (no phase
  * scratch).  Arguments as kpax_propagate_batch, with the obstacles (n_obs x 6 device floats) in
  * place of an environment. */
 kpax_status kpax_propagate_batch_noalloc(const kpax_config* cfg, const float* d_obstacles,

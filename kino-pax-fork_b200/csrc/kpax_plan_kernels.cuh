@@ -92,7 +92,7 @@ struct alignas(16) QueryDev {
     unsigned long long* lb;  // look-back status of k_expand, one per block
     float* partials;      // kPartials partial score sums
     uint32_t* sarr;       // arrival counter of k_scores
-    uint32_t* bar;        // grid barrier of k_iterate: arrivals, generation
+    uint32_t* bar;        // grid barrier of k_iterate: arrivals (one word used)
     uint32_t* ctas;       // per-CTA repeat sums of k_iterate's frontier phase
     float* path;
     const float* init_goal;  // init row then goal row, S floats each
@@ -753,30 +753,27 @@ __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* p)
     return v;
 }
 
-// Grid-wide barrier of a launch whose CTAs are all resident: bar[0] counts arrivals, bar[1] is the
-// generation.  The last CTA to arrive resets the count and advances the generation; the others poll
-// the generation they read before arriving.  Bounded: returns false after spin_limit polls.
+// Grid-wide barrier of a launch whose CTAs are all resident.  bar[0] counts arrivals over the
+// launch's barriers without being reset in between: the CTA whose arrival returns `old` waits
+// until the count reaches the next multiple of nblocks above it, so the last CTA to arrive passes
+// at once and the others need one poll that sees its arrival (the last CTA of the launch resets
+// the count once every CTA is past the last barrier).  Bounded: returns false after spin_limit
+// polls.
 __device__ __forceinline__ bool grid_barrier(uint32_t* bar, uint32_t nblocks, uint32_t* s_flag,
                                              uint32_t spin_limit = kSpinLimit)
 {
     __syncthreads();
     if(threadIdx.x == 0) {
-        const uint32_t gen = ld_acquire(bar + 1);
-        __threadfence();
+        __threadfence();  // the block's writes before its arrival
+        const uint32_t target = (atomicAdd(bar, 1u) / nblocks + 1u) * nblocks;
         bool ok = true;
-        if(atomicAdd(bar, 1u) == nblocks - 1u) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            uint32_t spins = 0;
-            while(ld_acquire(bar + 1) == gen) {
-                if(++spins > spin_limit) {
-                    ok = false;
-                    break;
-                }
-                if(spins > 16) __nanosleep(32);
+        uint32_t spins = 0;
+        while(ld_acquire(bar) < target) {
+            if(++spins > spin_limit) {
+                ok = false;
+                break;
             }
+            if(spins > 16) __nanosleep(32);
         }
         __threadfence();
         *s_flag = ok ? 1u : 0u;
@@ -800,8 +797,12 @@ __device__ __forceinline__ uint32_t block_sum(uint32_t v, uint32_t* s_warp)
     return t;
 }
 
+// ctl_line: the query's control block, whose line thread 0 prefetches into L2 while the block
+// copies its descriptor (L2 is where the predecessor's writes land, so the prefetch cannot serve a
+// stale copy; the fields are read after the predecessor completes).
 template <int M, int BS>
 __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_iterate(const QueryDev* __restrict__ qs,
+                                                                             const Ctl* ctl_line,
                                                                              uint32_t* __restrict__ active)
 {
     constexpr int NW = BS / 32;
@@ -811,6 +812,7 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_iterate(c
     __shared__ uint32_t s_warp[NW], s_warp2[NW];
     __shared__ float s_part[kPartials];
     __shared__ unsigned long long s_t[3];  // phase start times (thread 0)
+    if(threadIdx.x == 0) asm volatile("prefetch.global.L2 [%0];" ::"l"(ctl_line));
     load_query(qs, nullptr, sq);
     const KParams& p = sq.p;
     const TreeDev& t = sq.t;
@@ -945,7 +947,7 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_iterate(c
     __syncthreads();
     if(!s_last) return;
     __threadfence();
-    if(tid == 0) *sq.sarr = 0u;
+    if(tid == 0) *sq.sarr = 0u, sq.bar[0] = 0u;  // every CTA is past the last grid barrier
     score_finish(sq, s_part, active);
     if(tid == 0) {
         const unsigned long long t4 = globaltimer();

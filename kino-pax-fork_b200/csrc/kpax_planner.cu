@@ -82,13 +82,13 @@ void* iterate_kernel(int bs)
 }
 
 template <int M>
-void launch_iterate(int bs, uint32_t gx, cudaStream_t s, const QueryDev* dq, uint32_t* active)
+void launch_iterate(int bs, uint32_t gx, cudaStream_t s, const QueryDev* dq, const Ctl* ctl, uint32_t* active)
 {
     switch(bs) {
-        case 128: launch_chained(k_iterate<M, 128>, dim3(gx), 128, 0, s, dq, active); break;
-        case 256: launch_chained(k_iterate<M, 256>, dim3(gx), 256, 0, s, dq, active); break;
-        case 512: launch_chained(k_iterate<M, 512>, dim3(gx), 512, 0, s, dq, active); break;
-        default: launch_chained(k_iterate<M, kExpandBS>, dim3(gx), kExpandBS, 0, s, dq, active); break;
+        case 128: launch_chained(k_iterate<M, 128>, dim3(gx), 128, 0, s, dq, ctl, active); break;
+        case 256: launch_chained(k_iterate<M, 256>, dim3(gx), 256, 0, s, dq, ctl, active); break;
+        case 512: launch_chained(k_iterate<M, 512>, dim3(gx), 512, 0, s, dq, ctl, active); break;
+        default: launch_chained(k_iterate<M, kExpandBS>, dim3(gx), kExpandBS, 0, s, dq, ctl, active); break;
     }
 }
 
@@ -441,9 +441,10 @@ struct PlanBatch {
         if(ev) cudaEventRecord(ev[0], stream);
         if(fused) {  // one launch: its phase times come from the device clock (Ctl::t_*_ns)
             const int m = prm[0].model - 1;
-            if(m == 0) launch_iterate<KPAX_MODEL_DOUBLE_INTEGRATOR>(expand_bs[m], gx_iter, stream, dq, d_active);
-            else if(m == 1) launch_iterate<KPAX_MODEL_DUBINS_AIRPLANE>(expand_bs[m], gx_iter, stream, dq, d_active);
-            else launch_iterate<KPAX_MODEL_QUADROTOR>(expand_bs[m], gx_iter, stream, dq, d_active);
+            const Ctl* c0 = d_ctl;  // the single query's control block
+            if(m == 0) launch_iterate<KPAX_MODEL_DOUBLE_INTEGRATOR>(expand_bs[m], gx_iter, stream, dq, c0, d_active);
+            else if(m == 1) launch_iterate<KPAX_MODEL_DUBINS_AIRPLANE>(expand_bs[m], gx_iter, stream, dq, c0, d_active);
+            else launch_iterate<KPAX_MODEL_QUADROTOR>(expand_bs[m], gx_iter, stream, dq, c0, d_active);
             if(ev) cudaEventRecord(ev[3], stream);
             return;
         }
