@@ -688,8 +688,9 @@ def run_ours(args) -> None:
     pl = kpax.KPAX(cfg)
     stream = torch.cuda.ExternalStream(pl.stream)
     pl.begin(start, goal, d_obs.data_ptr(), obs.shape[0])
-    pl.iterate_timed(8, 0)  # grow the frontier until every iteration uses the full budget
-    pl.iterate_timed(max(args.warmup, 3), FLUSH_BYTES)
+    _, grow0 = pl.iterate_timed(8, 0)  # grow the frontier until every iteration uses the full budget
+    _, grow1 = pl.iterate_timed(max(args.warmup, 3), FLUSH_BYTES)
+    tree0 = 1 + grow0["appended"] + grow1["appended"]  # nodes when the timed iterations start
     launches0 = kpax.kernel_launches()
     if dist:
         dist.barrier()
@@ -837,7 +838,9 @@ def run_ours(args) -> None:
                        "launch": {"block_size": cfg.block_size or 448, "samples_per_thread": cfg.samples_per_thread or 1,
                                   "hash_cell_size": cfg.hash_cell_size,
                                   "source": "autotuner cache" if tuning else "defaults"},
-                       "children_per_step": tot["children"] // args.steps, "l2": "flushed before each timed iteration "
+                       "children_per_step": tot["children"] // args.steps,
+                       "tree_nodes": [tree0, tree0 + tot["appended"]],  # at the first and after the last timed iteration
+                       "l2": "flushed before each timed iteration "
                        "(256 MiB write, outside the events)", "parallelism": f"replicas x{ws}"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks,
             "reference_cuda": ref_cuda,

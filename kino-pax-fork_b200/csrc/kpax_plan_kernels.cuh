@@ -283,14 +283,12 @@ __global__ void k_begin(const QueryDev* __restrict__ qs, uint32_t plan_base, uin
     *sq.sarr = 0u, *sq.farr = 0u;
 }
 
+// Node i's repeat count after the iteration's start: r0 its stored byte, reg its region.
 __device__ __forceinline__ uint32_t resolve_repeat(const KParams& p, const TreeDev& t, const RegDev& rg, uint32_t i,
-                                                   uint32_t tree_old, uint32_t iter, uint32_t plan, float fa, float total,
-                                                   uint32_t ready)
+                                                   uint32_t r0, int32_t reg, uint32_t tree_old, uint32_t iter,
+                                                   uint32_t plan, float fa, float total, uint32_t ready)
 {
-    // the node's byte and region id are loaded together, then the region's score and valid count:
-    // two dependent loads per node whichever case applies
-    const uint32_t r0 = t.rep[i];
-    const int32_t reg = t.r1[i];
+    // the region's score and valid count: loaded whichever case applies
     const float raw = rg.score[reg];
     const int32_t nvalid = rg.valid[reg];
     uint32_t r = r0;
@@ -354,12 +352,32 @@ __device__ __forceinline__ uint32_t scan_tiles(uint32_t* tiles, uint32_t n, uint
 __device__ __forceinline__ void count_tile(const QueryDev& sq, uint32_t b, uint32_t tree, uint32_t tree_old, uint32_t iter,
                                            uint32_t plan, float fa, float total, uint32_t ready, uint32_t* s_warp)
 {
+    static_assert(kItems == 4, "a thread's nodes are one 4-byte word of repeat bytes");
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const TreeDev& t = sq.t;
+    // four consecutive nodes per thread: their bytes and region ids in one load each when the
+    // four lie inside the tree and the arrays are aligned for it (the planner's are 256-byte
+    // aligned; kpax_frontier_compact's repeat bytes are the caller's)
+    const uint32_t i0 = b * kTile + 4u * threadIdx.x;
+    const bool vec = ((reinterpret_cast<uintptr_t>(t.rep) & 3u) | (reinterpret_cast<uintptr_t>(t.r1) & 15u)) == 0u;
+    uint32_t r0[4] = {0u, 0u, 0u, 0u};
+    int32_t reg[4] = {0, 0, 0, 0};
+    if(vec && i0 + 3u < tree) {
+        const uint32_t w = *reinterpret_cast<const uint32_t*>(t.rep + i0);
+        const int4 g4 = *reinterpret_cast<const int4*>(t.r1 + i0);
+        r0[0] = w & 0xFFu, r0[1] = (w >> 8) & 0xFFu, r0[2] = (w >> 16) & 0xFFu, r0[3] = w >> 24;
+        reg[0] = g4.x, reg[1] = g4.y, reg[2] = g4.z, reg[3] = g4.w;
+    } else {
+#pragma unroll
+        for(int j = 0; j < 4; ++j)
+            if(i0 + j < tree) r0[j] = t.rep[i0 + j], reg[j] = t.r1[i0 + j];
+    }
     uint32_t sum = 0;
 #pragma unroll
-    for(int j = 0; j < kItems; ++j) {
-        const uint32_t i = b * kTile + j * kFrontierBS + threadIdx.x;  // coalesced
-        if(i < tree) sum += resolve_repeat(sq.p, sq.t, sq.rg, i, tree_old, iter, plan, fa, total, ready);
+    for(int j = 0; j < 4; ++j) {
+        const uint32_t i = i0 + j;
+        if(i < tree)
+            sum += resolve_repeat(sq.p, t, sq.rg, i, r0[j], reg[j], tree_old, iter, plan, fa, total, ready);
     }
 #pragma unroll
     for(int d = 16; d > 0; d >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, d);

@@ -82,8 +82,8 @@ def test_second_batch_plan_uses_a_new_random_stream(cuda):
 def test_persistent_stages_over_many_uneven_queries(cuda):
     """24 queries of uneven size in one batch (the stages run as persistent launches over all
     queries' work, with per-query offsets): trees from 2^10 to 2^16 nodes, some filling before
-    their goal, some reaching it in a few iterations, some planning with no obstacles.  Every query
-    must give its single plan."""
+    their goal, some reaching it in a few iterations (at least the fast double integrator added last),
+    some planning with no obstacles.  Every query must give its single plan."""
     import torch
 
     rng = np.random.default_rng(5)
@@ -115,6 +115,7 @@ def test_persistent_stages_over_many_uneven_queries(cuda):
             c.expansions_per_iter = min(c.max_tree_size, 1 << 12)
             c.max_iter, c.seed = 8, 300 + i
             qs.append((c, qobs, qs_, qg))
+    qs.append(_queries()[0])  # the fast double integrator that reaches its goal in a few iterations
     d_obs = [torch.from_numpy(np.ascontiguousarray(o, np.float32)).cuda() if o.size else None for _, o, _, _ in qs]
     ptrs = [d.data_ptr() if d is not None else 0 for d in d_obs]
     batch = kpax.Batch([c for c, _, _, _ in qs])

@@ -272,6 +272,28 @@ def test_frontier_compaction_bit_exact(cuda, n, density):
         assert st["E"] == budget or st["E"] == R or st["E"] * st["k"] <= budget
 
 
+def test_frontier_compaction_of_unaligned_repeat_bytes(cuda):
+    """The count pass reads four repeat bytes at a time only from 4-byte aligned arrays: repeat
+    bytes that start one byte into a buffer give the oracle's result too."""
+    import torch
+
+    cfg = kpax.preset(kpax.PRESET_QUAD)
+    n = 70001
+    rng = np.random.default_rng(11)
+    rep = np.where(rng.random(n) < 0.3, rng.integers(1, 16, n), 0).astype(np.uint8)
+    rep[rng.random(n) < 0.02] = 255
+    buf = torch.zeros(n + 1, dtype=torch.uint8, device="cuda")
+    buf[1:] = torch.from_numpy(rep).cuda()
+    for budget in (1 << 12, 1 << 16):
+        buf[1:] = torch.from_numpy(rep).cuda()
+        d_ent = torch.full((budget,), -1, dtype=torch.int32, device="cuda")
+        st = kpax.frontier_compact(cfg, buf.data_ptr() + 1, n, budget, d_ent.data_ptr())
+        o_rep, o_ent, o_st = O.frontier_compact(cfg, rep, budget)
+        assert st == o_st, (budget, st, o_st)
+        assert np.array_equal(d_ent[: st["E"]].cpu().numpy().view(np.uint32), o_ent), budget
+        assert np.array_equal(buf.cpu().numpy()[1:], o_rep), budget
+
+
 def test_bounded_wait_gives_up_and_context_stays_usable(cuda):
     """A device-side wait that nothing ends (the expansion's look-back wait on a tile that never
     publishes) gives up after its poll limit: the kernel stores a timeout status and returns, the
