@@ -1023,7 +1023,8 @@ def run_batch(args) -> None:
                 tuned_models[m] = best
         cfgs = [kpax_autotune.apply(c, tuned_models[c.model]) if c.model in tuned_models else c for c in cfgs]
     # children per expansion tile of every query: a batch expands millions of children per
-    # iteration, where 16-warp CTAs hide latency better than the 14 warps the single-query tuning picks
+    # iteration, where the batch expansion's 256-child tiles at four or five CTAs per SM hide more
+    # latency than the single 14-warp CTA the single-query tuning picks
     if args.batch_block:
         for c in cfgs:
             c.block_size = args.batch_block
@@ -1240,9 +1241,9 @@ def main() -> None:
     ap.add_argument("--plans-ref", type=int, default=256, help="plans per side of the quad-ref workload")
     ap.add_argument("--plans-ref-big", type=int, default=32, help="plans per side at the 2^22 tree capacity (quad-ref)")
     ap.add_argument("--batch-iters", type=int, default=0, help="iteration cap of every batched query (0 = presets)")
-    ap.add_argument("--batch-block", type=int, default=512, choices=[0, 128, 256, 448, 512],
+    ap.add_argument("--batch-block", type=int, default=256, choices=[0, 128, 256, 448, 512],
                     help="children per expansion tile of every batched query (0 = the single-query tuning / "
-                         "presets; 512 measured fastest for batches, 128/256/448/512: 647/668/629/677 M/s)")
+                         "presets; 256 measured fastest for batches: four or five CTAs per SM)")
     ap.add_argument("--seeds", type=int, default=256, help="held-out scenes of the learned workload")
     ap.add_argument("--eps", type=float, default=0.2, help="uniform fraction of the learned proposal")
     ap.add_argument("--proposal", choices=["on", "off"], default="on", help="learned proposal for batched quadrotor queries")

@@ -187,8 +187,17 @@ __global__ void __launch_bounds__(kFrontierBS) k_write_all(const QueryDev* __res
 // query without children, which publishes its empty append).  Look-back waits only on lower tiles
 // of the same query, which lower global units hold: every CTA must be resident (the host sizes the
 // grid by occupancy), and the successor is released only at completion.
+// CTAs per SM the batch expansion is compiled for.  A batch has children for every SM many times
+// over, so its expansion is bound by how many warps each SM interleaves: 256-child tiles run four
+// (quadrotor, 64 registers a thread) or five (the 6-state models, 48) CTAs per SM, whatever that
+// spills.  1024 mixed queries on a B200: 790 M valid expansions/s, against 785 at four CTAs for
+// every model, 757 at three, 683 at one 512-child CTA (16 warps) and 629 at one 448-child CTA.
+// Other tile sizes keep the single-query bound.
 template <int M, int BS>
-__global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_expand_all(const QueryDev* __restrict__ qs,
+constexpr int kExpandAllMinBlocks = BS == 256 ? (M == KPAX_MODEL_QUADROTOR ? 4 : 5) : (512 / BS > 0 ? 512 / BS : 1);
+
+template <int M, int BS>
+__global__ void __launch_bounds__(BS, (kExpandAllMinBlocks<M, BS>)) k_expand_all(const QueryDev* __restrict__ qs,
                                                                                 const Ctl* __restrict__ ctls,
                                                                                 const uint32_t* __restrict__ qidx,
                                                                                 uint32_t nq, uint32_t* __restrict__ active)

@@ -7,9 +7,9 @@
 //  - the double-integrator step is written the same way, so DI segments are bit-identical;
 //  - Dubins and quadrotor RK4 use a branch-free sine/cosine (sincos_fast, within a few ulp of
 //    CUDA's sincosf), tan as sin times the reciprocal cosine and the PTX approximate square root
-//    and reciprocal; Dubins lets the compiler fuse multiply-adds, the quadrotor's right-hand side
-//    and stage sums spell out every fused multiply-add; they match the oracle within the
-//    propagation tolerance.
+//    and reciprocal, and spell out every rounding and fused multiply-add (so a step gives the same
+//    bits in every kernel it is inlined into); they match the oracle within the propagation
+//    tolerance.
 #pragma once
 #include <stdint.h>
 
@@ -388,8 +388,8 @@ struct DubinsShifts {
 __device__ __forceinline__ DubinsShifts dubins_shifts(const KParams& p, const float* c)
 {
     const float h = p.h, hh = p.hh, yr = c[1], pr = c[2];
-    return {fmaxf(fabsf(h * pr), fabsf(h * yr)) <= kShiftMax, shift_coef(hh * pr), shift_coef(hh * yr), shift_coef(h * pr),
-            shift_coef(h * yr)};
+    return {fmaxf(fabsf(__fmul_rn(h, pr)), fabsf(__fmul_rn(h, yr))) <= kShiftMax, shift_coef(__fmul_rn(hh, pr)),
+            shift_coef(__fmul_rn(hh, yr)), shift_coef(__fmul_rn(h, pr)), shift_coef(__fmul_rn(h, yr))};
 }
 
 __device__ __forceinline__ bool step_dubins(const StepParams& p, const Grid& g, float* s, const float* c, const DubinsShifts& k)
@@ -407,19 +407,22 @@ __device__ __forceinline__ bool step_dubins(const StepParams& p, const Grid& g, 
         sincos_apply(sp0, cp0, k.p2, &sp2, &cp2);
         sincos_apply(sy0, cy0, k.y2, &sy2, &cy2);
     } else {
-        sincos_checked(pitch + hh * pr, &sp1, &cp1);
-        sincos_checked(yaw + hh * yr, &sy1, &cy1);
-        sincos_checked(pitch + h * pr, &sp2, &cp2);
-        sincos_checked(yaw + h * yr, &sy2, &cy2);
+        sincos_checked(__fmaf_rn(hh, pr, pitch), &sp1, &cp1);
+        sincos_checked(__fmaf_rn(hh, yr, yaw), &sy1, &cy1);
+        sincos_checked(__fmaf_rn(h, pr, pitch), &sp2, &cp2);
+        sincos_checked(__fmaf_rn(h, yr, yaw), &sy2, &cy2);
     }
-    const float vm = v + hh * a, ve = v + h * a;
-    const float mx = vm * cp1 * cy1, my = vm * cp1 * sy1, mz = vm * sp1;
-    s[0] += h6 * (v * cp0 * cy0 + 2.0f * (mx + mx) + ve * cp2 * cy2);
-    s[1] += h6 * (v * cp0 * sy0 + 2.0f * (my + my) + ve * cp2 * sy2);
-    s[2] += h6 * (v * sp0 + 2.0f * (mz + mz) + ve * sp2);
-    s[3] = yaw + h * yr;
-    s[4] = pitch + h * pr;
-    s[5] = v + h6 * (a + 2.0f * (a + a) + a);
+    // every rounding written out (as the quadrotor's): the same bits wherever the step is inlined
+    const float vm = __fmaf_rn(hh, a, v), ve = __fmaf_rn(h, a, v);
+    const float vmc = __fmul_rn(vm, cp1), vc0 = __fmul_rn(v, cp0), vc2 = __fmul_rn(ve, cp2);
+    const float mx = __fmul_rn(vmc, cy1), my = __fmul_rn(vmc, sy1), mz = __fmul_rn(vm, sp1);
+    // (k1 + 2 (k2 + k3)) + k4 with k2 = k3 (the reference's stage sum; 2 x is exact)
+    s[0] = __fmaf_rn(h6, __fmaf_rn(vc2, cy2, __fmaf_rn(2.0f, __fadd_rn(mx, mx), __fmul_rn(vc0, cy0))), s[0]);
+    s[1] = __fmaf_rn(h6, __fmaf_rn(vc2, sy2, __fmaf_rn(2.0f, __fadd_rn(my, my), __fmul_rn(vc0, sy0))), s[1]);
+    s[2] = __fmaf_rn(h6, __fmaf_rn(ve, sp2, __fmaf_rn(2.0f, __fadd_rn(mz, mz), __fmul_rn(v, sp0))), s[2]);
+    s[3] = __fmaf_rn(h, yr, yaw);
+    s[4] = __fmaf_rn(h, pr, pitch);
+    s[5] = __fmaf_rn(h6, __fadd_rn(__fmaf_rn(2.0f, __fadd_rn(a, a), a), a), v);
     if(s[5] < p.vmin || s[5] > p.vmax || s[4] < p.pitch_lo || s[4] > p.pitch_hi) return false;
     if(s[0] < p.ws_lo || s[0] > p.ws_hi || s[1] < p.ws_lo || s[1] > p.ws_hi || s[2] < p.ws_lo || s[2] > p.ws_hi) return false;
     return finite_all(s, 6) && step_free(g, p0, s);

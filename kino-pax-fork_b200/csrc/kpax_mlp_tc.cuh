@@ -100,8 +100,9 @@ __device__ __forceinline__ void mixture_draws(const KParams& p, const float* __r
     const float* c = rec + k * kCompStride;
 #pragma unroll
     for(int d = 0; d < kDim; ++d) {
-        const float sg = expf(kSigMid + kSigHalf * tanhf(__ldg(c + 1 + kDim + d) * (1.0f / kSigHalf)));
-        const float z = __ldg(c + 1 + d) + sg * n[d];
+        // fused multiply-adds written out: the same draws in every kernel this is inlined into
+        const float sg = expf(__fmaf_rn(kSigHalf, tanhf(__fmul_rn(__ldg(c + 1 + kDim + d), 1.0f / kSigHalf)), kSigMid));
+        const float z = __fmaf_rn(sg, n[d], __ldg(c + 1 + d));
         const float v = 1.0f / (1.0f + expf(-z));
         u[d] = fminf(fmaxf(v, 5.9604645e-8f), 1.0f);
     }

@@ -79,11 +79,13 @@ def test_second_batch_plan_uses_a_new_random_stream(cuda):
     batch.close()
 
 
-def test_persistent_stages_over_many_uneven_queries(cuda):
+@pytest.mark.parametrize("block", [0, 256])
+def test_persistent_stages_over_many_uneven_queries(cuda, block):
     """24 queries of uneven size in one batch (the stages run as persistent launches over all
     queries' work, with per-query offsets): trees from 2^10 to 2^16 nodes, some filling before
     their goal, some reaching it in a few iterations (at least the fast double integrator added last),
-    some planning with no obstacles.  Every query must give its single plan."""
+    some planning with no obstacles.  Every query must give its single plan, at the default
+    expansion tiles and at the 256-child tiles the batch expansion runs at four or five CTAs per SM."""
     import torch
 
     rng = np.random.default_rng(5)
@@ -116,6 +118,9 @@ def test_persistent_stages_over_many_uneven_queries(cuda):
             c.max_iter, c.seed = 8, 300 + i
             qs.append((c, qobs, qs_, qg))
     qs.append(_queries()[0])  # the fast double integrator that reaches its goal in a few iterations
+    if block:  # the batch expansion's 256-child tiles (four or five CTAs per SM)
+        for c, _, _, _ in qs:
+            c.block_size = block
     d_obs = [torch.from_numpy(np.ascontiguousarray(o, np.float32)).cuda() if o.size else None for _, o, _, _ in qs]
     ptrs = [d.data_ptr() if d is not None else 0 for d in d_obs]
     batch = kpax.Batch([c for c, _, _, _ in qs])
@@ -165,3 +170,32 @@ def test_learned_proposal_in_a_batch_matches_single_plans(cuda):
         assert {f: res[q][f] for f in single} == single, (q, single, res[q])
         pl.close()
     batch.close()
+
+
+def test_plans_do_not_depend_on_the_tile_size(cuda):
+    """Every model's step spells out its roundings, so a query's plan is the same whichever
+    kernel expands it: batches at 448- and 256-child tiles (one and four or five CTAs per SM) and
+    single plans at 128-child tiles give the same trees."""
+    import torch
+
+    qs = _queries()
+    d_obs = [torch.from_numpy(np.ascontiguousarray(o, np.float32)).cuda() if o.size else None for _, o, _, _ in qs]
+    ptrs = [d.data_ptr() if d is not None else 0 for d in d_obs]
+    fields = ("found", "goal_idx", "tree_size", "iters", "expansions", "valid_expansions", "path_cost")
+    out = []
+    for block in (448, 256):
+        cfgs = []
+        for c, _, _, _ in qs:
+            c.block_size = block
+            cfgs.append(c)
+        batch = kpax.Batch(cfgs)
+        res, _ = batch.plan([s for _, _, s, _ in qs], [g for _, _, _, g in qs], ptrs, [o.shape[0] for _, o, _, _ in qs])
+        out.append([{f: r[f] for f in fields} for r in res])
+        batch.close()
+    assert out[0] == out[1]
+    for q, (cfg, obs, s, g) in enumerate(qs):
+        cfg.block_size = 128
+        pl = kpax.KPAX(cfg)
+        r = pl.plan(s, g, ptrs[q], obs.shape[0])
+        assert {f: getattr(r, f) for f in fields} == out[0][q], q
+        pl.close()
