@@ -818,7 +818,12 @@ __device__ __forceinline__ uint32_t block_sum(uint32_t v, uint32_t* s_warp)
 // ctl_line: the query's control block, whose line thread 0 prefetches into L2 while the block
 // copies its descriptor (L2 is where the predecessor's writes land, so the prefetch cannot serve a
 // stale copy; the fields are read after the predecessor completes).
-template <int M, int BS>
+// The whole iteration in one launch (kIterWhole), or split around the learned proposal pass:
+// kIterFront (frontier count, budget, entry list) and kIterBack (expansion, scores), with
+// k_propose launched between them.
+constexpr int kIterWhole = 0, kIterFront = 1, kIterBack = 2;
+
+template <int M, int BS, int PART = kIterWhole>
 __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_iterate(const QueryDev* __restrict__ qs,
                                                                              const Ctl* ctl_line,
                                                                              uint32_t* __restrict__ active)
@@ -841,110 +846,120 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_iterate(c
     wait_predecessor();
     if(__syncthreads_or(ctl->done != 0u)) return;  // one decision for the whole grid: barriers follow
     if(tid == 0) s_t[0] = globaltimer();
-    const uint32_t tree = ctl->tree, tree_old = ctl->tree_old, iter = ctl->iter, plan = ctl->plan_idx;
-    const uint32_t ready = ctl->scores_ready;
-    const float fa = ctl->faccept, total = ctl->score_total;
+    uint32_t k = 0, n = 0;  // children per entry and children of this iteration
+    if constexpr(PART != kIterBack) {
+        const uint32_t tree = ctl->tree, tree_old = ctl->tree_old, iter = ctl->iter, plan = ctl->plan_idx;
+        const uint32_t ready = ctl->scores_ready;
+        const float fa = ctl->faccept, total = ctl->score_total;
 
-    // ---- frontier count (k_frontier_count): re-activation of the previous iteration
-    // (KPAX.cu:505-517) and repeats of its new nodes (476-479) over this thread's contiguous nodes
-    const uint32_t per_cta = (tree + G - 1) / G, per_thr = (per_cta + BS - 1) / BS;
-    const uint32_t c_lo = min(tree, cb * per_cta), c_hi = min(tree, c_lo + per_cta);
-    const uint32_t lo = min(c_hi, c_lo + (uint32_t)tid * per_thr), hi = min(c_hi, lo + per_thr);
-    uint32_t sum = 0;
-    for(uint32_t i0 = lo; i0 < hi; i0 += kIterBatch) {
-        uint32_t r0[kIterBatch];
-        int32_t reg[kIterBatch], nv[kIterBatch];
-        float raw[kIterBatch];
-#pragma unroll
-        for(int j = 0; j < kIterBatch; ++j) {  // each node's byte and region id, then its region's
-            const uint32_t i = i0 + j;         // score and valid count: two rounds of loads per batch
-            r0[j] = i < hi ? (uint32_t)t.rep[i] : 0u;
-            reg[j] = i < hi ? t.r1[i] : 0;
-        }
-#pragma unroll
-        for(int j = 0; j < kIterBatch; ++j) raw[j] = rg.score[reg[j]], nv[j] = rg.valid[reg[j]];
-#pragma unroll
-        for(int j = 0; j < kIterBatch; ++j) {
-            const uint32_t i = i0 + j;
-            if(i >= hi) continue;
-            uint32_t r = r0[j];
-            if(r == 0u) {
-                if(i < tree_old) {
-                    const float sc = region_score(raw[j], total, ready, p.eps);
-                    if(reactivate_draw(p, plan, iter - 1u, i) <= __fadd_rn(sc, fa)) r = 1u;
-                }
-            } else if(r == kPending) {
-                r = nv[j] < p.sparse_thr ? p.sparse_repeat : 1u;
+        // ---- frontier count (k_frontier_count): re-activation of the previous iteration
+        // (KPAX.cu:505-517) and repeats of its new nodes (476-479) over this thread's contiguous nodes
+        const uint32_t per_cta = (tree + G - 1) / G, per_thr = (per_cta + BS - 1) / BS;
+        const uint32_t c_lo = min(tree, cb * per_cta), c_hi = min(tree, c_lo + per_cta);
+        const uint32_t lo = min(c_hi, c_lo + (uint32_t)tid * per_thr), hi = min(c_hi, lo + per_thr);
+        uint32_t sum = 0;
+        for(uint32_t i0 = lo; i0 < hi; i0 += kIterBatch) {
+            uint32_t r0[kIterBatch];
+            int32_t reg[kIterBatch], nv[kIterBatch];
+            float raw[kIterBatch];
+    #pragma unroll
+            for(int j = 0; j < kIterBatch; ++j) {  // each node's byte and region id, then its region's
+                const uint32_t i = i0 + j;         // score and valid count: two rounds of loads per batch
+                r0[j] = i < hi ? (uint32_t)t.rep[i] : 0u;
+                reg[j] = i < hi ? t.r1[i] : 0;
             }
-            if(r != r0[j]) t.rep[i] = (uint8_t)r;
-            sum += r;
+    #pragma unroll
+            for(int j = 0; j < kIterBatch; ++j) raw[j] = rg.score[reg[j]], nv[j] = rg.valid[reg[j]];
+    #pragma unroll
+            for(int j = 0; j < kIterBatch; ++j) {
+                const uint32_t i = i0 + j;
+                if(i >= hi) continue;
+                uint32_t r = r0[j];
+                if(r == 0u) {
+                    if(i < tree_old) {
+                        const float sc = region_score(raw[j], total, ready, p.eps);
+                        if(reactivate_draw(p, plan, iter - 1u, i) <= __fadd_rn(sc, fa)) r = 1u;
+                    }
+                } else if(r == kPending) {
+                    r = nv[j] < p.sparse_thr ? p.sparse_repeat : 1u;
+                }
+                if(r != r0[j]) t.rep[i] = (uint8_t)r;
+                sum += r;
+            }
         }
-    }
-    // this thread's exclusive prefix inside the CTA, and the CTA's sum
-    uint32_t x = sum;
-#pragma unroll
-    for(int d = 1; d < 32; d <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
-        if(lane >= d) x += y;
-    }
-    if(lane == 31) s_warp[warp] = x;
-    __syncthreads();
-    uint32_t wex = 0, cta_sum = 0;
-    for(int w = 0; w < NW; ++w) {
-        wex += w < warp ? s_warp[w] : 0u;
-        cta_sum += s_warp[w];
-    }
-    const uint32_t thr_excl = wex + x - sum;
-    if(tid == 0) sq.ctas[cb] = cta_sum;
-    if(!grid_barrier(sq.bar, G, &s_flag)) {
-        if(tid == 0) atomicOr(&ctl->error, kErrTimeout), finish_query(ctl, active);
-        return;
-    }
-    release_successor();  // every CTA is resident now
+        // this thread's exclusive prefix inside the CTA, and the CTA's sum
+        uint32_t x = sum;
+    #pragma unroll
+        for(int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, d);
+            if(lane >= d) x += y;
+        }
+        if(lane == 31) s_warp[warp] = x;
+        __syncthreads();
+        uint32_t wex = 0, cta_sum = 0;
+        for(int w = 0; w < NW; ++w) {
+            wex += w < warp ? s_warp[w] : 0u;
+            cta_sum += s_warp[w];
+        }
+        const uint32_t thr_excl = wex + x - sum;
+        if(tid == 0) sq.ctas[cb] = cta_sum;
+        if(!grid_barrier(sq.bar, G, &s_flag)) {
+            if(tid == 0) atomicOr(&ctl->error, kErrTimeout), finish_query(ctl, active);
+            return;
+        }
+        release_successor();  // every CTA is resident now
 
-    // ---- budget (KPAX.cu:323-350) from the CTA sums, then the entry list (k_frontier_write)
-    uint32_t tot = 0, pre = 0;
-    for(uint32_t j = tid; j < G; j += BS) {
-        const uint32_t v = __ldcg(sq.ctas + j);
-        tot += v;
-        pre += j < cb ? v : 0u;
-    }
-    const uint64_t R = block_sum<NW>(tot, s_warp);
-    const uint32_t a_cta = block_sum<NW>(pre, s_warp2);
-    const uint32_t B = min(p.budget, p.cap - tree);
-    uint32_t k = p.per_entry, E = 0, n = 0;
-    if(B != 0 && R) {
-        if(R * k > B) {
-            k = (uint32_t)(B / R);
-            if(k == 0) k = 1;
+        // ---- budget (KPAX.cu:323-350) from the CTA sums, then the entry list (k_frontier_write)
+        uint32_t tot = 0, pre = 0;
+        for(uint32_t j = tid; j < G; j += BS) {
+            const uint32_t v = __ldcg(sq.ctas + j);
+            tot += v;
+            pre += j < cb ? v : 0u;
         }
-        E = (uint32_t)(R < (uint64_t)(B / k) ? R : (uint64_t)(B / k));
-        n = E * k;
-    }
-    if(cb == 0 && tid == 0) {
-        ctl->R = (uint32_t)R;
-        ctl->k = k, ctl->E = E, ctl->n = n;
-        if(B == 0) {
-            ctl->full = 1u;
-            finish_query(ctl, active);
+        const uint64_t R = block_sum<NW>(tot, s_warp);
+        const uint32_t a_cta = block_sum<NW>(pre, s_warp2);
+        const uint32_t B = min(p.budget, p.cap - tree);
+        k = p.per_entry;
+        uint32_t E = 0;
+        if(B != 0 && R) {
+            if(R * k > B) {
+                k = (uint32_t)(B / R);
+                if(k == 0) k = 1;
+            }
+            E = (uint32_t)(R < (uint64_t)(B / k) ? R : (uint64_t)(B / k));
+            n = E * k;
         }
-    }
-    if(B == 0) return;  // every CTA decides alike
-    if(E) {
-        uint64_t a = (uint64_t)a_cta + thr_excl;  // node i owns virtual entries [a, a + rep)
-        for(uint32_t i = lo; i < hi; ++i) {
-            const uint32_t cnt = t.rep[i];
-            if(!cnt) continue;
-            const uint64_t bnd = a + cnt;
-            const uint64_t elo = (a * E + R - 1) / R, ehi = (bnd * E + R - 1) / R;
-            for(uint64_t e = elo; e < ehi; ++e) sq.entries[e] = i;
-            if(elo < ehi) t.rep[i] = 0;
-            a = bnd;
+        if(cb == 0 && tid == 0) {
+            ctl->R = (uint32_t)R;
+            ctl->k = k, ctl->E = E, ctl->n = n;
+            if(B == 0) {
+                ctl->full = 1u;
+                finish_query(ctl, active);
+            }
         }
-    }
-    if(!grid_barrier(sq.bar, G, &s_flag)) {
-        if(tid == 0) atomicOr(&ctl->error, kErrTimeout), finish_query(ctl, active);
-        return;
+        if(B == 0) return;  // every CTA decides alike
+        if(E) {
+            uint64_t a = (uint64_t)a_cta + thr_excl;  // node i owns virtual entries [a, a + rep)
+            for(uint32_t i = lo; i < hi; ++i) {
+                const uint32_t cnt = t.rep[i];
+                if(!cnt) continue;
+                const uint64_t bnd = a + cnt;
+                const uint64_t elo = (a * E + R - 1) / R, ehi = (bnd * E + R - 1) / R;
+                for(uint64_t e = elo; e < ehi; ++e) sq.entries[e] = i;
+                if(elo < ehi) t.rep[i] = 0;
+                a = bnd;
+            }
+        }
+        if constexpr(PART == kIterFront) {  // the proposal pass and kIterBack follow
+            if(cb == 0 && tid == 0) ctl->t_front_ns += globaltimer() - s_t[0];
+            return;
+        }
+        if(!grid_barrier(sq.bar, G, &s_flag)) {
+            if(tid == 0) atomicOr(&ctl->error, kErrTimeout), finish_query(ctl, active);
+            return;
+        }
+    } else {
+        k = ctl->k, n = ctl->n;  // the budget and entry list of the front launch
     }
     if(tid == 0) s_t[1] = globaltimer();
 
@@ -955,6 +970,7 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_iterate(c
         if(tid == 0) atomicOr(&ctl->error, kErrTimeout), finish_query(ctl, active);
         return;
     }
+    if constexpr(PART == kIterBack) release_successor();  // every CTA is resident now
     if(tid == 0) s_t[2] = globaltimer();
 
     // ---- region scores (k_scores); the last CTA to finish adds the partials and closes the iteration
@@ -969,7 +985,7 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_iterate(c
     score_finish(sq, s_part, active);
     if(tid == 0) {
         const unsigned long long t4 = globaltimer();
-        ctl->t_front_ns += s_t[1] - s_t[0];
+        if constexpr(PART == kIterWhole) ctl->t_front_ns += s_t[1] - s_t[0];
         ctl->t_expand_ns += s_t[2] - s_t[1];
         ctl->t_score_ns += t4 - s_t[2];
     }

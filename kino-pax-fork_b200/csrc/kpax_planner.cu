@@ -69,26 +69,27 @@ void launch_expand(int bs, dim3 grid, cudaStream_t s, const QueryDev* dq, const 
     }
 }
 
-// The fused iteration kernel at one of its block sizes.
-template <int M>
+// The fused iteration kernel (or one of its two parts around the proposal pass) at one of its
+// block sizes.
+template <int M, int PART = kIterWhole>
 void* iterate_kernel(int bs)
 {
     switch(bs) {
-        case 128: return (void*)k_iterate<M, 128>;
-        case 256: return (void*)k_iterate<M, 256>;
-        case 512: return (void*)k_iterate<M, 512>;
-        default: return (void*)k_iterate<M, kExpandBS>;
+        case 128: return (void*)k_iterate<M, 128, PART>;
+        case 256: return (void*)k_iterate<M, 256, PART>;
+        case 512: return (void*)k_iterate<M, 512, PART>;
+        default: return (void*)k_iterate<M, kExpandBS, PART>;
     }
 }
 
-template <int M>
+template <int M, int PART = kIterWhole>
 void launch_iterate(int bs, uint32_t gx, cudaStream_t s, const QueryDev* dq, const Ctl* ctl, uint32_t* active)
 {
     switch(bs) {
-        case 128: launch_chained(k_iterate<M, 128>, dim3(gx), 128, 0, s, dq, ctl, active); break;
-        case 256: launch_chained(k_iterate<M, 256>, dim3(gx), 256, 0, s, dq, ctl, active); break;
-        case 512: launch_chained(k_iterate<M, 512>, dim3(gx), 512, 0, s, dq, ctl, active); break;
-        default: launch_chained(k_iterate<M, kExpandBS>, dim3(gx), kExpandBS, 0, s, dq, ctl, active); break;
+        case 128: launch_chained(k_iterate<M, 128, PART>, dim3(gx), 128, 0, s, dq, ctl, active); break;
+        case 256: launch_chained(k_iterate<M, 256, PART>, dim3(gx), 256, 0, s, dq, ctl, active); break;
+        case 512: launch_chained(k_iterate<M, 512, PART>, dim3(gx), 512, 0, s, dq, ctl, active); break;
+        default: launch_chained(k_iterate<M, kExpandBS, PART>, dim3(gx), kExpandBS, 0, s, dq, ctl, active); break;
     }
 }
 
@@ -165,6 +166,8 @@ struct PlanBatch {
     // for measurements; the plans are the same.
     int expand_mode = 1;
     bool fused = false;      // single query without the proposal: one k_iterate launch per iteration
+    bool fused_split = false;  // single quadrotor query with the proposal: front, proposal pass, back
+    uint32_t gx_split = 0;     // CTAs of the front and back launches (all resident), 0 if unusable
     uint32_t gx_iter = 0;    // its CTAs (all resident), 0 when the kernel cannot be used
     Ctl* d_ctl = nullptr;
     Ctl* h_ctl = nullptr;
@@ -319,6 +322,15 @@ struct PlanBatch {
             // every resident CTA: the frontier and score phases use them all, the expansion as many as
             // it has tiles (a small budget's iteration leaves the rest idle in that phase)
             gx_iter = std::min<uint32_t>(resident, (uint32_t)kIterMaxCTAs);
+            if(m == 2) {  // the two parts around the proposal pass: the smaller occupancy of the two
+                int front = 0, back = 0;
+                KPAX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                    &front, iterate_kernel<KPAX_MODEL_QUADROTOR, kIterFront>(bs), bs, 0));
+                KPAX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                    &back, iterate_kernel<KPAX_MODEL_QUADROTOR, kIterBack>(bs), bs, 0));
+                gx_split = std::min<uint32_t>((uint32_t)std::max(std::min(front, back), 0) * (uint32_t)sms,
+                                              (uint32_t)kIterMaxCTAs);
+            }
         }
         if(n > 1 && n <= kBatchMaxQueries) {  // persistent stages: grids of resident CTAs
             int dev = 0, sms = 148;
@@ -373,7 +385,11 @@ struct PlanBatch {
         return KPAX_OK;
     }
 
-    void update_fused() { fused = nq == 1 && gx_iter > 0 && cfg[0].iteration_kernels == 0 && n_learned == 0; }
+    void update_fused()
+    {
+        fused = nq == 1 && gx_iter > 0 && cfg[0].iteration_kernels == 0 && n_learned == 0;
+        fused_split = nq == 1 && gx_split > 0 && cfg[0].iteration_kernels == 0 && n_learned == 1;
+    }
 
     void release()
     {
@@ -439,6 +455,13 @@ struct PlanBatch {
     void launch_iteration(cudaEvent_t* ev = nullptr, bool split = true)
     {
         if(ev) cudaEventRecord(ev[0], stream);
+        if(fused_split) {  // front launch, proposal pass, back launch; phase times from the device clock
+            launch_iterate<KPAX_MODEL_QUADROTOR, kIterFront>(expand_bs[2], gx_split, stream, dq, d_ctl, d_active);
+            launch_proposal(stream);
+            launch_iterate<KPAX_MODEL_QUADROTOR, kIterBack>(expand_bs[2], gx_split, stream, dq, d_ctl, d_active);
+            if(ev) cudaEventRecord(ev[3], stream);
+            return;
+        }
         if(fused) {  // one launch: its phase times come from the device clock (Ctl::t_*_ns)
             const int m = prm[0].model - 1;
             const Ctl* c0 = d_ctl;  // the single query's control block
@@ -613,6 +636,7 @@ struct PlanBatch {
     uint64_t kernels_per_iteration() const
     {
         if(fused) return 1;
+        if(fused_split) return 3;
         if(persistent) {  // start, count, write, (proposal), the expansion(s), scores
             uint64_t k = n_learned ? (d_prop_off ? 6 : 5) : 4;
             if(expand_mode == 2 && mixed_bs) return k + 1;
@@ -796,14 +820,14 @@ struct PlanBatch {
         }
         KPAX_CUDA(cudaStreamSynchronize(stream));
         Ctl c1 = {};
-        if(fused) {
+        if(fused || fused_split) {
             KPAX_CUDA(cudaMemcpyAsync(&c1, d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, stream));
             KPAX_CUDA(cudaStreamSynchronize(stream));
         }
         for(uint32_t i = 0; i < n; ++i) {
             float a = 0, b = 0, d = 0, t = 0;
             cudaEvent_t* e = &tev[4 * (size_t)i];
-            if(fused && split) {  // phase times from the device clock, averaged over the n iterations
+            if((fused || fused_split) && split) {  // phase times from the device clock, averaged over the n iterations
                 a = (float)((c1.t_front_ns - c0[0].t_front_ns) * 1e-6 / n);
                 b = (float)((c1.t_expand_ns - c0[0].t_expand_ns) * 1e-6 / n);
                 d = (float)((c1.t_score_ns - c0[0].t_score_ns) * 1e-6 / n);

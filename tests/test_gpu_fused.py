@@ -16,10 +16,12 @@ pytestmark = pytest.mark.gpu
 GOLDEN = Path(__file__).parent / "golden"
 
 
-def run(torch, cfg, obs, s, g, kernels):
+def run(torch, cfg, obs, s, g, kernels, net=None):
     c = cfg.copy()
     c.iteration_kernels = kernels
     pl = kpax.KPAX(c)
+    if net is not None:
+        pl.set_proposal(net, 0.3)
     d = torch.from_numpy(np.ascontiguousarray(obs, np.float32)).cuda()
     l0 = kpax.kernel_launches()
     r = pl.plan(s, g, d.data_ptr(), obs.shape[0])
@@ -84,6 +86,29 @@ def test_fused_iteration_equals_per_stage_kernels(cuda, name):
     iters = fused["res"][4]
     assert fused["launches"] < staged["launches"], (fused["launches"], staged["launches"])
     assert fused["res"][3] > 1 and iters >= 1
+
+
+@pytest.mark.parametrize("block", [0, 128])
+def test_fused_parts_around_the_proposal_pass_equal_per_stage_kernels(cuda, block):
+    """With the learned proposal a single plan runs the fused iteration in two launches around the
+    tensor-core pass (frontier count and entry list; expansion and scores): the same plan, bit for
+    bit, as the per-stage kernels with the same pass between them, in three launches per
+    iteration instead of five."""
+    import torch
+
+    import kpax_learn as L
+
+    net = L.load_network(L.DEFAULT_WEIGHTS)
+    cfg = kpax.preset(kpax.PRESET_QUAD)
+    cfg.max_iter, cfg.max_tree_size, cfg.expansions_per_iter = 12, 1 << 18, 1 << 13
+    if block:
+        cfg.block_size = block
+    obs, s, g = E.quad_scene(n_total=300)
+    fused = run(torch, cfg, obs, s, g, 0, net)
+    staged = run(torch, cfg, obs, s, g, 1, net)
+    same(fused, staged)
+    iters = fused["res"][4]
+    assert iters >= 2 and fused["launches"] < staged["launches"], (iters, fused["launches"], staged["launches"])
 
 
 def test_fused_timed_iterations_report_phase_times(cuda):
