@@ -100,9 +100,10 @@ typedef struct kpax_config {
     float prune_goal_bias;          /* h_goalBias_ (0.7, PruneKPAX.cu:36) */
     float prune_exploration_bias;   /* h_explorationBias_ (0.3, PruneKPAX.cu:35) */
     float prune_progress_scale;     /* h_progressScale_ (10, PruneKPAX.cu:34) */
-    /* 0: a single plan without the learned proposal runs each iteration as one persistent launch
-     * (frontier passes, expansion and scores separated by bounded grid-wide barriers); 1: one launch
-     * per stage (as batches and the learned proposal always do).  Plans are identical either way. */
+    /* 0: a single plan runs each iteration as one persistent launch (frontier passes, expansion
+     * and scores separated by bounded grid-wide barriers), or with the learned proposal as two such
+     * launches around the tensor-core pass; 1: one launch per stage.  Batches always run their own
+     * persistent stages.  Plans are identical either way. */
     int32_t iteration_kernels;
     int32_t reserved[2];
 } kpax_config;
