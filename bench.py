@@ -48,9 +48,10 @@ METRIC = "valid expansions/s"
 UNIT = "expansions/s"
 # Algorithmic FP32 work per RK4 step (FMA = 2), counted from a CSE'd restatement of the models.
 FLOP_PER_STEP = {kpax.MODEL_DOUBLE_INTEGRATOR: 18, kpax.MODEL_DUBINS_AIRPLANE: 51, kpax.MODEL_QUADROTOR: 498}
-# dram__bytes_read.sum + dram__bytes_write.sum of one steady-state k_expand launch (2^16 children,
-# L2 flushed before the iteration) in an ncu capture of the default workload; none for the others
-EXPAND_DRAM_BYTES = {kpax.MODEL_QUADROTOR: 1535744 + 0}
+# dram__bytes_read.sum + dram__bytes_write.sum of one steady-state k_iterate launch (the fused
+# iteration, 2^16 children, L2 flushed before it) in an ncu capture of the default workload; none
+# for the others
+ITERATE_DRAM_BYTES = {kpax.MODEL_QUADROTOR: 2093824 + 0}
 # the same sum for the one-pass kernel (kpax_propagate_batch_noalloc) on 2^20 Dubins segments, L2
 # flushed before the step, per segment
 ONE_PASS_DRAM_BYTES_PER_SEGMENT = (25186304 + 48397824) / (1 << 20)
@@ -768,10 +769,11 @@ def run_ours(args) -> None:
     sm_mhz = peaks.get("sm_max_mhz", 1965.0)
     nominal = 148 * 128 * 2 * sm_mhz * 1e6 / 1e12
     roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                "traffic": EXPAND_DRAM_BYTES.get(cfg.model), "kernel": "k_expand",
-                "traffic_note": "DRAM bytes read + written by one steady-state 2^16-child k_expand launch of this "
-                                "workload in an ncu capture (summary under profiles/); the tree, regions and grid are "
-                                "L2-resident, so traffic is far below the bytes the kernel touches",
+                "traffic": ITERATE_DRAM_BYTES.get(cfg.model), "kernel": "k_iterate (its expansion phase)",
+                "traffic_note": "DRAM bytes read + written by one steady-state k_iterate launch of this workload (the "
+                                "whole fused iteration) in an ncu capture (summary under profiles/); after the L2 flush "
+                                "only the first touches of the tree's repeat bytes and region ids, the regions and the "
+                                "grid reach DRAM, the rest of what the kernel touches is L2-resident",
                 "peak_note": "measured: kpax_fp32_peak (8 independent FMA chains per thread, 2048 threads per SM, "
                              "CUDA events) on this GPU inside the clock-sampling window; MEASURED_PEAKS.json has no "
                              "FP32 figure",
