@@ -270,10 +270,10 @@ __device__ __forceinline__ int grid_coord(const Grid& g, float x)
 
 // isMotionValidSpatialHash (spatialHash.cu:145-194) with isBroadPhaseValid (collisionCheck.cu:3-10):
 // true when no obstacle overlaps the box strictly in all three dimensions.
-__device__ __forceinline__ bool box_free(const Grid& g, const float lo[3], const float hi[3])
+// The box's cells are x0..x1, y0..y1, z0..z1.
+__device__ __forceinline__ bool box_free_cells(const Grid& g, const float lo[3], const float hi[3], int x0, int y0, int z0,
+                                               int x1, int y1, int z1)
 {
-    const int x0 = grid_coord(g, lo[0]), y0 = grid_coord(g, lo[1]), z0 = grid_coord(g, lo[2]);
-    const int x1 = grid_coord(g, hi[0]), y1 = grid_coord(g, hi[1]), z1 = grid_coord(g, hi[2]);
     for(int gz = z0; gz <= z1; ++gz)
         for(int gy = y0; gy <= y1; ++gy)
             for(int gx = x0; gx <= x1; ++gx) {
@@ -288,7 +288,17 @@ __device__ __forceinline__ bool box_free(const Grid& g, const float lo[3], const
     return true;
 }
 
-__device__ __forceinline__ bool step_free(const Grid& g, const float p0[3], const float p1[3])
+__device__ __forceinline__ bool box_free(const Grid& g, const float lo[3], const float hi[3])
+{
+    return box_free_cells(g, lo, hi, grid_coord(g, lo[0]), grid_coord(g, lo[1]), grid_coord(g, lo[2]), grid_coord(g, hi[0]),
+                          grid_coord(g, hi[1]), grid_coord(g, hi[2]));
+}
+
+// The swept box of one step, p0 -> p1.  cells (optional): the cell coordinates of p0 on entry,
+// replaced by p1's — a step's end is the next step's start, and since the cell map is
+// non-decreasing the box's cell range is the range of its two corners' cells, so each step maps
+// one point instead of two.
+__device__ __forceinline__ bool step_free(const Grid& g, const float p0[3], const float p1[3], int* cells = nullptr)
 {
     float lo[3], hi[3];
 #pragma unroll
@@ -297,7 +307,12 @@ __device__ __forceinline__ bool step_free(const Grid& g, const float p0[3], cons
         lo[d] = sw ? p1[d] : p0[d];
         hi[d] = sw ? p0[d] : p1[d];
     }
-    return box_free(g, lo, hi);
+    if(!cells) return box_free(g, lo, hi);
+    const int c1[3] = {grid_coord(g, p1[0]), grid_coord(g, p1[1]), grid_coord(g, p1[2])};
+    const bool ok = box_free_cells(g, lo, hi, min(cells[0], c1[0]), min(cells[1], c1[1]), min(cells[2], c1[2]),
+                                   max(cells[0], c1[0]), max(cells[1], c1[1]), max(cells[2], c1[2]));
+    cells[0] = c1[0], cells[1] = c1[1], cells[2] = c1[2];
+    return ok;
 }
 
 __device__ __forceinline__ bool finite_all(const float* s, int n)
@@ -357,7 +372,7 @@ __device__ __forceinline__ DIConsts di_consts(const KParams& p, const float* c)
 
 // One step from s in place; false when the step fails a check (velocity box, workspace, finite,
 // collision).
-__device__ __forceinline__ bool step_di(const StepParams& p, const Grid& g, float* s, const DIConsts& k)
+__device__ __forceinline__ bool step_di(const StepParams& p, const Grid& g, float* s, const DIConsts& k, int* cells = nullptr)
 {
     const float h = p.h;
     const float p0[3] = {s[0], s[1], s[2]};
@@ -373,7 +388,7 @@ __device__ __forceinline__ bool step_di(const StepParams& p, const Grid& g, floa
     }
     if(s[3] < p.vmin || s[3] > p.vmax || s[4] < p.vmin || s[4] > p.vmax || s[5] < p.vmin || s[5] > p.vmax) return false;
     if(s[0] < p.ws_lo || s[0] > p.ws_hi || s[1] < p.ws_lo || s[1] > p.ws_hi || s[2] < p.ws_lo || s[2] > p.ws_hi) return false;
-    return finite_all(s, 6) && step_free(g, p0, s);
+    return finite_all(s, 6) && step_free(g, p0, s, cells);
 }
 
 // Dubins airplane, statePropagatorSpatialHash.cu:139-229; c = (a, yawRate, pitchRate).  One step
@@ -392,7 +407,8 @@ __device__ __forceinline__ DubinsShifts dubins_shifts(const KParams& p, const fl
             shift_coef(__fmul_rn(hh, yr)), shift_coef(__fmul_rn(h, pr)), shift_coef(__fmul_rn(h, yr))};
 }
 
-__device__ __forceinline__ bool step_dubins(const StepParams& p, const Grid& g, float* s, const float* c, const DubinsShifts& k)
+__device__ __forceinline__ bool step_dubins(const StepParams& p, const Grid& g, float* s, const float* c, const DubinsShifts& k,
+                                            int* cells = nullptr)
 {
     const float h = p.h, hh = p.hh, h6 = p.h6;
     const float a = c[0], yr = c[1], pr = c[2];
@@ -425,7 +441,7 @@ __device__ __forceinline__ bool step_dubins(const StepParams& p, const Grid& g, 
     s[5] = __fmaf_rn(h6, __fadd_rn(__fmaf_rn(2.0f, __fadd_rn(a, a), a), a), v);
     if(s[5] < p.vmin || s[5] > p.vmax || s[4] < p.pitch_lo || s[4] > p.pitch_hi) return false;
     if(s[0] < p.ws_lo || s[0] > p.ws_hi || s[1] < p.ws_lo || s[1] > p.ws_hi || s[2] < p.ws_lo || s[2] > p.ws_hi) return false;
-    return finite_all(s, 6) && step_free(g, p0, s);
+    return finite_all(s, 6) && step_free(g, p0, s, cells);
 }
 
 // Quadrotor right-hand side, statePropagator.cu:325-370, in its two halves: the kinematics
@@ -525,16 +541,17 @@ __device__ __forceinline__ bool quad_dyn_ok(const StepParams& p, const float* v)
            finite_all(v, 6);
 }
 
-__device__ __forceinline__ bool quad_kin_ok(const StepParams& p, const Grid& g, const float* p0, const float* x)
+__device__ __forceinline__ bool quad_kin_ok(const StepParams& p, const Grid& g, const float* p0, const float* x,
+                                            int* cells = nullptr)
 {
     if(x[0] < p.ws_lo || x[0] > p.ws_hi || x[1] < p.ws_lo || x[1] > p.ws_hi || x[2] < p.ws_lo || x[2] > p.ws_hi) return false;
-    return finite_all(x, 6) && step_free(g, p0, x);
+    return finite_all(x, 6) && step_free(g, p0, x, cells);
 }
 
 // Quadrotor RK4, statePropagatorSpatialHash.cu:234-308: four stages, the stage sum in the
 // reference's order ((k1 + 2k2) + 2k3) + k4.  One step from s in place; false when the step fails
 // a check (velocity box, workspace, finite, collision).
-__device__ __forceinline__ bool step_quad(const StepParams& p, const Grid& g, float* s, const float* c)
+__device__ __forceinline__ bool step_quad(const StepParams& p, const Grid& g, float* s, const float* c, int* cells = nullptr)
 {
     const float h = p.h, hh = p.hh, h6 = p.h6;
     const float p0[3] = {s[0], s[1], s[2]};
@@ -560,7 +577,7 @@ __device__ __forceinline__ bool step_quad(const StepParams& p, const Grid& g, fl
     }
 #pragma unroll
     for(int j = 0; j < 12; ++j) s[j] = __fmaf_rn(h6, acc[j], s[j]);
-    return quad_dyn_ok(p, s + 6) && quad_kin_ok(p, g, p0, s);
+    return quad_dyn_ok(p, s + 6) && quad_kin_ok(p, g, p0, s, cells);
 }
 
 // Per-segment constants of a model's step (the double integrator's acceleration terms, the Dubins
@@ -575,11 +592,12 @@ __device__ __forceinline__ auto segment_consts(const KParams& p, const float* c)
 }
 
 template <int M, class K>
-__device__ __forceinline__ bool model_step(const StepParams& p, const Grid& g, float* s, const float* c, const K& k)
+__device__ __forceinline__ bool model_step(const StepParams& p, const Grid& g, float* s, const float* c, const K& k,
+                                           int* cells = nullptr)
 {
-    if constexpr(M == KPAX_MODEL_DOUBLE_INTEGRATOR) return step_di(p, g, s, k);
-    else if constexpr(M == KPAX_MODEL_DUBINS_AIRPLANE) return step_dubins(p, g, s, c, k);
-    else return step_quad(p, g, s, c);
+    if constexpr(M == KPAX_MODEL_DOUBLE_INTEGRATOR) return step_di(p, g, s, k, cells);
+    else if constexpr(M == KPAX_MODEL_DUBINS_AIRPLANE) return step_dubins(p, g, s, c, k, cells);
+    else return step_quad(p, g, s, c, cells);
 }
 
 // Propagates `steps` steps from s (in place), checking every step like the reference, and
@@ -590,8 +608,9 @@ __device__ __forceinline__ bool propagate(const KParams& p, const Grid& g, float
     const auto k = segment_consts<M>(p, c);
     const StepParams sp = step_params(p);
     const Grid gl = g;  // register copy of the grid's pointers and cell map
+    int cells[3] = {grid_coord(gl, s[0]), grid_coord(gl, s[1]), grid_coord(gl, s[2])};  // of the current position
     for(int i = 0; i < steps; ++i) {
-        if(!model_step<M>(sp, gl, s, c, k)) {
+        if(!model_step<M>(sp, gl, s, c, k, cells)) {
             done = i + 1;
             return false;
         }
