@@ -271,7 +271,6 @@ __global__ void __launch_bounds__(kScoreBS) k_scores_all(const QueryDev* __restr
 {
     extern __shared__ uint32_t s_off[];
     __shared__ QueryDev sq;
-    __shared__ float s_part[kPartials];
     __shared__ uint32_t s_warp[kScoreBS / 32], s_last;
     wait_predecessor();
     release_successor();
@@ -302,7 +301,7 @@ __global__ void __launch_bounds__(kScoreBS) k_scores_all(const QueryDev* __restr
         if(s_last) {
             __threadfence();
             if(tid == 0) *sq.sarr = 0u;
-            score_finish(sq, s_part, active, true);
+            score_finish(sq, active, true);
         }
         __syncthreads();
     }

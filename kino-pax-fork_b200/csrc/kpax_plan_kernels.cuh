@@ -685,29 +685,43 @@ __device__ __forceinline__ void score_partials(const QueryDev& sq, uint32_t gtid
     }
 }
 
-// Total of the partials by one block (all threads; s_part holds kPartials floats), then the
-// iteration's bookkeeping by thread 0: tree size, fAccept (KPAX.cu:527-528), counters, stop flags.
-__device__ __forceinline__ void score_finish(const QueryDev& sq, float* s_part, uint32_t* __restrict__ active,
-                                             bool defer_finish = false)
+// Total of the partials by the block's first warp, then the iteration's bookkeeping by thread 0:
+// tree size, fAccept (KPAX.cu:527-528), counters, stop flags.  All threads call it.
+__device__ __forceinline__ void score_finish(const QueryDev& sq, uint32_t* __restrict__ active, bool defer_finish = false)
 {
+    constexpr int kRegs = kPartials / 32;  // partials per lane: lane l holds partials l + 32 m
     const KParams& p = sq.p;
     Ctl* ctl = sq.ctl;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31;
+    if(tid >= 32) return;
     const uint32_t ngroups = (p.num_r1 + 31) / 32;
     const int used = (int)min(ngroups, (uint32_t)kPartials);
-    // halving tree over the 1024 partials; the levels whose upper halves hold only the zero
-    // partials at and above `used` leave the lower entries unchanged (x + 0 = x), so the tree
-    // starts at the first power of two not below `used` and gives the same total
+    // halving tree over the partials (level s adds partial j + s into partial j, j < s); the levels
+    // whose upper halves hold only the zero partials at and above `used` leave the lower entries
+    // unchanged (x + 0 = x), so the tree starts at the first power of two not below `used` and
+    // gives the same total.  Levels s >= 32 pair partials of the same lane (registers m and
+    // m + s / 32), levels below 32 pair lanes (shuffles): the same additions in the same order.
     int half = 1;
     while(half < used) half <<= 1;
-    for(int j = tid; j < half; j += blockDim.x) s_part[j] = j < used ? ((volatile float*)sq.partials)[j] : 0.0f;
-    __syncthreads();
-    for(int s = half / 2; s > 0; s >>= 1) {
-        for(int j = tid; j < s; j += blockDim.x) s_part[j] = __fadd_rn(s_part[j], s_part[j + s]);
-        __syncthreads();
+    float v[kRegs];
+#pragma unroll
+    for(int m = 0; m < kRegs; ++m) {
+        const int j = lane + 32 * m;
+        v[m] = j < used ? ((volatile float*)sq.partials)[j] : 0.0f;
+    }
+#pragma unroll
+    for(int S = kRegs / 2; S >= 1; S >>= 1) {
+        if(32 * 2 * S <= half) {
+#pragma unroll
+            for(int m = 0; m < S; ++m) v[m] = __fadd_rn(v[m], v[m + S]);
+        }
+    }
+    for(int sh = min(half, 32) / 2; sh > 0; sh >>= 1) {
+        const float o = __shfl_down_sync(0xffffffffu, v[0], sh);
+        if(lane < sh) v[0] = __fadd_rn(v[0], o);
     }
     if(tid == 0) {
-        ctl->score_total = s_part[0];
+        ctl->score_total = v[0];
         ctl->scores_ready = 1u;
         // the block may hold the control block's line in L1 from earlier in a fused launch, while
         // other CTAs updated it since: volatile reads
@@ -733,7 +747,6 @@ __device__ __forceinline__ void score_finish(const QueryDev& sq, float* s_part, 
 __global__ void __launch_bounds__(kScoreBS) k_scores(const QueryDev* __restrict__ qs, uint32_t* __restrict__ active)
 {
     __shared__ QueryDev sq;
-    __shared__ float s_part[kPartials];
     __shared__ uint32_t s_last;
     load_query(qs, nullptr, sq);
     const int tid = threadIdx.x;
@@ -751,7 +764,7 @@ __global__ void __launch_bounds__(kScoreBS) k_scores(const QueryDev* __restrict_
         __threadfence();
         if(tid == 0) *sq.sarr = 0u;
     }
-    score_finish(sq, s_part, active);
+    score_finish(sq, active);
 }
 
 // ---------------------------------------------------------------- fused iteration (single query)
@@ -833,7 +846,6 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_iterate(c
     __shared__ ExpandSmem<NW> sm;
     __shared__ uint32_t s_flag, s_last;
     __shared__ uint32_t s_warp[NW], s_warp2[NW];
-    __shared__ float s_part[kPartials];
     __shared__ unsigned long long s_t[3];  // phase start times (thread 0)
     if(threadIdx.x == 0) asm volatile("prefetch.global.L2 [%0];" ::"l"(ctl_line));
     load_query(qs, nullptr, sq);
@@ -982,7 +994,7 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_iterate(c
     if(!s_last) return;
     __threadfence();
     if(tid == 0) *sq.sarr = 0u, sq.bar[0] = 0u;  // every CTA is past the last grid barrier
-    score_finish(sq, s_part, active);
+    score_finish(sq, active);
     if(tid == 0) {
         const unsigned long long t4 = globaltimer();
         if constexpr(PART == kIterWhole) ctl->t_front_ns += s_t[1] - s_t[0];
