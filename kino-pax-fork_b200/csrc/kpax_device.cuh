@@ -315,12 +315,15 @@ __device__ __forceinline__ bool step_free(const Grid& g, const float p0[3], cons
     return ok;
 }
 
+// x * 0 is +-0 for a finite x and NaN for an infinite or NaN one, so the sum of those products is
+// 0 exactly when every value is finite (two chains for a shorter dependency).
 __device__ __forceinline__ bool finite_all(const float* s, int n)
 {
-    bool ok = true;
+    float a = 0.0f, b = 0.0f;
 #pragma unroll
-    for(int i = 0; i < n; ++i) ok = ok && isfinite(s[i]);
-    return ok;
+    for(int i = 0; i + 1 < n; i += 2) a = __fmaf_rn(s[i], 0.0f, a), b = __fmaf_rn(s[i + 1], 0.0f, b);
+    if(n & 1) a = __fmaf_rn(s[n - 1], 0.0f, a);
+    return __fadd_rn(a, b) == 0.0f;
 }
 
 // ------------------------------------------------------------------ controls
@@ -535,16 +538,23 @@ __device__ __forceinline__ void quad_trig0(const float* a0, float* trig0)
 
 // The per-step checks of each half, in the reference's order (velocity box; workspace; then the
 // finite check and the swept box's collision query).
+// A box check of three values by their minimum and maximum: fminf / fmaxf pass over a NaN that the
+// six comparisons would let through as well, and the finite check rejects it either way, so the
+// verdict is the comparisons'.
+__device__ __forceinline__ bool in_box3(const float* v, float lo, float hi)
+{
+    return !(fminf(fminf(v[0], v[1]), v[2]) < lo || fmaxf(fmaxf(v[0], v[1]), v[2]) > hi);
+}
+
 __device__ __forceinline__ bool quad_dyn_ok(const StepParams& p, const float* v)
 {
-    return !(v[0] < p.vmin || v[0] > p.vmax || v[1] < p.vmin || v[1] > p.vmax || v[2] < p.vmin || v[2] > p.vmax) &&
-           finite_all(v, 6);
+    return in_box3(v, p.vmin, p.vmax) && finite_all(v, 6);
 }
 
 __device__ __forceinline__ bool quad_kin_ok(const StepParams& p, const Grid& g, const float* p0, const float* x,
                                             int* cells = nullptr)
 {
-    if(x[0] < p.ws_lo || x[0] > p.ws_hi || x[1] < p.ws_lo || x[1] > p.ws_hi || x[2] < p.ws_lo || x[2] > p.ws_hi) return false;
+    if(!in_box3(x, p.ws_lo, p.ws_hi)) return false;
     return finite_all(x, 6) && step_free(g, p0, x, cells);
 }
 
