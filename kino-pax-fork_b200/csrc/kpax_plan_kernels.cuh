@@ -444,6 +444,14 @@ __global__ void __launch_bounds__(kFrontierBS, kFrontierMinBlocks) k_frontier_co
     }
 }
 
+// ceil(a * E / R), the first of the E entries taken at or after virtual entry a (entry j is virtual
+// entry floor(j * R / E)); a <= R, so the product fits 64 bits.  A node's last bound is the next
+// node's first, so a run of nodes divides once per node, and not at all when every entry is taken.
+__device__ __forceinline__ uint64_t entry_ceil(uint64_t a, uint32_t E, uint64_t R)
+{
+    return E == R ? a : (a * E + R - 1) / R;
+}
+
 // Tile b of the entry list (kFrontierBS threads, kItems consecutive nodes each): node i owns virtual
 // entries [a, a + rep) with a from the tile scan.
 __device__ __forceinline__ void write_tile(const QueryDev& sq, uint32_t b, uint32_t tree, uint64_t R, uint32_t E,
@@ -470,14 +478,14 @@ __device__ __forceinline__ void write_tile(const QueryDev& sq, uint32_t b, uint3
     uint32_t wex = 0;
     for(int w = 0; w < warp; ++w) wex += s_warp[w];
     uint64_t a = (uint64_t)__ldcg(sq.tiles + b) + wex + x - sum;
+    uint64_t lo = sum ? entry_ceil(a, E, R) : 0;
 #pragma unroll
     for(int j = 0; j < kItems; ++j) {
         if(!cnt[j]) continue;
-        const uint64_t bnd = a + cnt[j];
-        const uint64_t lo = (a * E + R - 1) / R, hi = (bnd * E + R - 1) / R;
+        const uint64_t bnd = a + cnt[j], hi = entry_ceil(bnd, E, R);
         for(uint64_t e = lo; e < hi; ++e) sq.entries[e] = i0 + j;
         if(lo < hi) t.rep[i0 + j] = 0;
-        a = bnd;
+        a = bnd, lo = hi;
     }
     __syncthreads();
 }
@@ -952,14 +960,14 @@ __global__ void __launch_bounds__(BS, (512 / BS > 0 ? 512 / BS : 1)) k_iterate(c
         if(B == 0) return;  // every CTA decides alike
         if(E) {
             uint64_t a = (uint64_t)a_cta + thr_excl;  // node i owns virtual entries [a, a + rep)
+            uint64_t elo = sum ? entry_ceil(a, E, R) : 0;
             for(uint32_t i = lo; i < hi; ++i) {
                 const uint32_t cnt = t.rep[i];
                 if(!cnt) continue;
-                const uint64_t bnd = a + cnt;
-                const uint64_t elo = (a * E + R - 1) / R, ehi = (bnd * E + R - 1) / R;
+                const uint64_t bnd = a + cnt, ehi = entry_ceil(bnd, E, R);
                 for(uint64_t e = elo; e < ehi; ++e) sq.entries[e] = i;
                 if(elo < ehi) t.rep[i] = 0;
-                a = bnd;
+                a = bnd, elo = ehi;
             }
         }
         if constexpr(PART == kIterFront) {  // the proposal pass and kIterBack follow
